@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Multislice LSQ-ML throughput on B200 (positions x slices per second).
+
+Workload (one "step" = one full LSQ-ML iteration over the scan):
+  8 slices of 517x517 (the reference geometry for a 512^2-class field: scan
+  span + 2 * (N/2 + 5) px), probe 128x128 with 4 incoherent modes
+  (70/15/10/5 %, 25 mrad, 300 kV, 200 A defocus), 64x64 = 4096 positions at
+  6 px, mini-batches of 256, amplitude noise model, probe-position
+  correction (momentum), patterns at 1e6 e-/pattern -- seeded synthetic
+  data with those shapes (no datasets ship here).
+
+  value : pos*slice/s with patterns resident in HBM (device-timed, max over ranks)
+  e2e   : the same through the engine API with every step's patterns copied
+          from pinned host memory and the iteration status read back
+  roofline : the fused mini-batch kernel (k_group) timed live with CUDA events
+          around each launch; algorithmic bytes per pos*slice = N^2 (28 + 16 M) + 4 N^2 / S
+  cpu_baseline : the numpy oracle of the same step on the host cores
+          (bounded sample: mini-batches of 16 positions at the full shapes).
+
+  --impl reference : times the reference's CPU algorithm (the numpy port in
+          oracle/) on this host with all its threads, same metric and config.
+
+Multi-GPU (torchrun): every rank runs an independent reconstruction
+(replicas); value = total pos*slice/s over ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "multislice pos*slice/s (LSQ-ML iteration, 1 B200)"
+UNIT = "pos*slice/s"
+CONFIG = {"workload": "multislice LSQ-ML: 8 x 517^2 slices (2 nm), probe 128^2 x 4 modes, "
+                      "scan 64x64=4096 @ 6 px, batch 256, position correction on",
+          "N": 128, "modes": 4, "slices": 8, "object": [517, 517], "positions": 4096, "batch": 256,
+          "solver": "lsqml", "noise_model": "amplitude", "l2": "working set > L2 (1.07 GB psi scratch per batch)"}
+
+
+def algorithmic_bytes_per_pos_slice(N: int, M: int, S: int, pattern_bytes: int = 4) -> int:
+    """O cutout read fwd + adj (16 N^2), psi store + reload (16 M N^2), object-update
+    scatter (8 N^2), illumination scatter (4 N^2), pattern read amortised over S."""
+    return N * N * (28 + 16 * M) + pattern_bytes * N * N // S
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+def ncu_traffic_per_launch():
+    """dram bytes (read + write) per k_group launch from the committed ncu summary."""
+    path = os.path.join(ROOT, 'profiles', 'k_group_lsqml_c2.md')
+    try:
+        for line in open(path):
+            if line.strip().startswith('traffic_bytes_per_full_launch:'):
+                return float(line.split(':', 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.gpu}', f'--query-gpu={self.Q}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in getattr(self, 'lines', []):
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_dist():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    return world, rank, local
+
+
+def cpu_sample(ds, patterns_host, n_groups: int, batch: int, threads: int, seed: int = 5):
+    """Time the numpy oracle's LSQ-ML mini-batch step on `n_groups` batches of
+    `batch` positions (full shapes).  Returns (pos*slice/s, seconds, description)."""
+    from oracle import phaser_np as O
+    O.set_fft_workers(threads)
+    N = ds.probe.shape[-1]
+    S = ds.true_object.shape[0]
+    ky, kx = O.recip_grid((N, N), ds.probe_sampling, numpy.float32)
+    geom = O.Geometry(numpy.asarray(ds.obj_sampling.corner), numpy.asarray(ds.obj_sampling.sampling), ky, kx,
+                      ds.thicknesses)
+    props = O.make_propagators(ky, kx, ds.probe_sampling, ds.wavelength, ds.thicknesses)
+    rng = numpy.random.default_rng(seed)
+    flat = ds.scan.reshape(-1, 2)
+    obj = ds.init_object.copy()
+    probe = ds.probe.copy()
+    t_total = 0.0
+    for _ in range(n_groups):
+        idx = rng.choice(flat.shape[0], batch, replace=False)
+        t0 = time.perf_counter()
+        res = O.lsqml_group(geom, probe, obj, flat[idx], patterns_host(idx), ds.mask, props, None,
+                            O.NoiseModel(), O.LSQMLParams(), update_position=True)
+        t_total += time.perf_counter() - t0
+        obj, probe = res['object'], res['probe']
+    units = n_groups * batch * S
+    return units / t_total, t_total, f"{n_groups} LSQ-ML mini-batches of {batch} positions at the full shapes"
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the CPU (numpy) algorithm timed on this host."""
+    if rank != 0:
+        return
+    from phaser_b200.synthetic import lsqml_multislice_config
+    from oracle import phaser_np as O
+    threads = os.cpu_count() or 1
+    ds = lsqml_multislice_config(seed=0)
+    N = ds.probe.shape[-1]
+    ky, kx = O.recip_grid((N, N), ds.probe_sampling, numpy.float32)
+    geom = O.Geometry(numpy.asarray(ds.obj_sampling.corner), numpy.asarray(ds.obj_sampling.sampling), ky, kx,
+                      ds.thicknesses)
+    props = O.make_propagators(ky, kx, ds.probe_sampling, ds.wavelength, ds.thicknesses)
+    O.set_fft_workers(threads)
+    flat = ds.scan.reshape(-1, 2)
+    cache = {}
+
+    def pats(idx):   # simulated with the oracle forward model, Poisson at the configured dose
+        missing = [int(i) for i in idx if int(i) not in cache]
+        if missing:
+            psi0, cuts, _, _ = O.cutout_group(geom, ds.probe, ds.true_object, flat[missing])
+            psi = O._forward(psi0, cuts, O.tilt_propagators(ky, kx, ds.thicknesses, props, None))
+            inten = numpy.sum(O.abs2(O.fft2c(psi[-1] * cuts[:, -1, None])), axis=1)
+            inten *= ds.counts / inten.sum(axis=(1, 2), keepdims=True)
+            rng = numpy.random.default_rng(1234)
+            for i, im in zip(missing, rng.poisson(inten).astype(numpy.float32)):
+                cache[i] = im
+        return numpy.stack([cache[int(i)] for i in idx])
+
+    batch = 16
+    S = ds.true_object.shape[0]
+    for _ in range(args.warmup):
+        cpu_sample(ds, pats, 1, batch, threads, seed=_)
+    times = []
+    for k in range(args.steps):
+        rate, secs, desc = cpu_sample(ds, pats, 1, batch, threads, seed=100 + k)
+        times.append(secs)
+    t = float(numpy.mean(times))
+    value = batch * S / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference", "config": CONFIG,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"each step: one LSQ-ML mini-batch of {batch} positions at the full shapes "
+                                       f"(numpy oracle, scipy.fft with {threads} threads)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from phaser_b200 import _lib
+    from phaser_b200.synthetic import lsqml_multislice_config, simulate_patterns
+    from phaser_b200.engines.conventional import ConventionalEngine
+    from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
+    from phaser_b200.sampling import Sampling
+    from phaser_b200 import plan as PL
+
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    lib = _lib.load()
+
+    # CPU baseline first (rank 0, N == 1), before the device is busy
+    ds = lsqml_multislice_config(seed=rank)
+    pats = simulate_patterns(ds, seed=rank, device=dev)
+    pats_host = pats.cpu().pin_memory()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        host_np = pats_host.numpy()
+        rate, secs, desc = cpu_sample(ds, lambda idx: host_np[idx], 2, 16, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": desc + f" (numpy oracle, scipy.fft with {threads} threads), {secs:.1f} s"}
+
+    N, M, S = ds.probe.shape[-1], ds.probe.shape[0], ds.true_object.shape[0]
+    n_pos = int(numpy.prod(ds.scan.shape[:-1]))
+
+    def new_engine():
+        state = ReconsState(iter=IterState(), wavelength=ds.wavelength,
+                            probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
+                            object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
+                            scan=ds.scan.copy())
+        props = PL.ConventionalEnginePlan(
+            noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
+            position_solver={'type': 'momentum', 'step_size': 1e-3, 'max_step_size': 0.2, 'momentum': 0.9},
+            niter=10 ** 6, grouping=256, update_positions=True)
+        e = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
+                                'seed': 'bench', 'recons_name': 'bench'}, props, patterns_on_device=pats)
+        e.presolve()
+        return e
+
+    eng = new_engine()
+    stream = torch.cuda.current_stream()
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        eng.iteration(it)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---------------- device-resident timing
+    eng.fused_events = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.phb_kernel_launches()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            it += 1
+            eng.iteration(it, sync=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = lib.phb_kernel_launches() - launches0
+    eng.check(it)
+    barrier()
+    t_ms = ev0.elapsed_time(ev1)
+    fused = []
+    import ctypes
+    for a, b in eng.fused_events:
+        ms = ctypes.c_float()
+        _lib.call('phb_event_elapsed_ms', a, b, ctypes.byref(ms))
+        fused.append(ms.value)
+        _lib.call('phb_event_destroy', a)
+        _lib.call('phb_event_destroy', b)
+    eng.fused_events = None
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    units_per_step = n_pos * S
+    value = world * units_per_step * args.steps / (t_ms / 1e3)
+
+    # ---------------- end-to-end: host patterns -> device each step, status back each step
+    e2e_ms = []
+    barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        it += 1
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pats.copy_(pats_host, non_blocking=True)
+        eng.iteration(it, sync=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    barrier()
+    e2e_t = float(numpy.mean(e2e_ms))
+    if world > 1:
+        tt = torch.tensor([e2e_t], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e_value = world * units_per_step / (e2e_t / 1e3)
+
+    # ---------------- roofline of the fused kernel
+    peak, peak_kind = measured_peaks()
+    B = 256
+    bytes_launch = algorithmic_bytes_per_pos_slice(N, M, S) * B * S
+    avg_ms = float(numpy.mean(fused)) if fused else float('nan')
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = ncu_traffic_per_launch()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": "k_group<128> (fused LSQ-ML mini-batch)",
+            "launch_ms": avg_ms, "launches_timed": len(fused), "bytes_per_launch": bytes_launch,
+            "peak_source": f"{peak_kind} hbm_gbs", "share_of_step": sum(fused) / t_ms if t_ms else None}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pats_host.numel() * 4),
+                        "d2h_bytes_per_step": 32},
+                "gpu_launches": int(launches), "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    world, rank, local = setup_dist()
+    if args.impl == 'reference':
+        run_reference(args, world, rank)
+    else:
+        run_b200(args, world, rank, local)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,240 @@
+/*
+ * phaser_b200 -- C ABI of the B200 (sm_100a) multislice ptychography backend.
+ *
+ * Conventions for every entry point:
+ *   - all array arguments are DEVICE pointers owned by the caller; nothing
+ *     here allocates device memory (scratch comes in through `workspace`);
+ *   - complex arrays are interleaved float pairs (C99 `float _Complex`,
+ *     numpy complex64), row-major, C-contiguous;
+ *   - work is enqueued on `stream` (a cudaStream_t, passed as void*) and the
+ *     call returns without synchronising;
+ *   - the return value is a status code (PHB_OK == 0); no exception or abort
+ *     crosses this boundary.  `phb_status_string` names a code.
+ *
+ * The reference citations are paths inside the phaser source tree.
+ */
+#ifndef PHASER_B200_H
+#define PHASER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define PHB_OK                 0
+#define PHB_ERR_INVALID_ARG    1   /* null pointer, bad size, misaligned workspace */
+#define PHB_ERR_UNSUPPORTED    2   /* shape the kernels do not implement (e.g. N not 64/128) */
+#define PHB_ERR_CUDA           3   /* a CUDA launch or runtime call failed */
+#define PHB_ERR_NONFINITE      4   /* NaN/inf found in the object or probe */
+#define PHB_ERR_OUTSIDE        5   /* probe positions completely outside the object */
+
+const char *phb_status_string(int status);
+int phb_version(void);
+/* Last CUDA error text seen by this library on the calling thread ("" if none). */
+const char *phb_last_cuda_error(void);
+
+/* ------------------------------------------------------------- cutouts (a1-a4)
+ * Integer cutout starts and sub-pixel shifts for scan positions.
+ * Replaces ObjectSampling._pos_to_object_idx + numpy.round
+ * (phaser/utils/object.py:291-301, 493-495) and get_subpx_shifts (324-331).
+ * idx = (pos - corner)/sampling - (n - 1)/2 in float64, rounded half-to-even,
+ * bit-exact with the reference.  `group` (B) selects rows of `scan` (n_pos x 2,
+ * float32, (y, x)); pass NULL to take rows 0..B-1.  `subpx` may be NULL. */
+int phb_cutout_starts(const float *scan, const int64_t *group, int64_t B,
+                      double corner_y, double corner_x, double samp_y, double samp_x,
+                      int64_t cut_y, int64_t cut_x,
+                      int64_t *starts /* B x 2 */, float *subpx /* B x 2 or NULL */,
+                      void *stream);
+
+/* Gather cutouts of every slice: out[b, s, i, j] = obj[s, i + y0_b, j + x0_b],
+ * out-of-bounds pixels read `fill`.  Replaces ObjectCutout.get
+ * (phaser/utils/object.py:501-519; GPU form phaser/utils/_cuda_kernels.py:51-75). */
+int phb_cutout_get_c64(const void *obj, int64_t S, int64_t H, int64_t W,
+                       const int64_t *starts, int64_t B, int64_t cut_y, int64_t cut_x,
+                       float fill_re, float fill_im, void *out, void *stream);
+int phb_cutout_get_f32(const float *obj, int64_t S, int64_t H, int64_t W,
+                       const int64_t *starts, int64_t B, int64_t cut_y, int64_t cut_x,
+                       float fill, float *out, void *stream);
+
+/* Scatter-add views (B, S, cut_y, cut_x) into obj (S, H, W); out-of-bounds
+ * pixels are dropped.  fp32 atomics, so the summation order is not fixed.
+ * Replaces ObjectCutout.add (phaser/utils/object.py:540-557;
+ * phaser/utils/_cuda_kernels.py:78-107). */
+int phb_cutout_add_c64(void *obj, int64_t S, int64_t H, int64_t W,
+                       const int64_t *starts, int64_t B, int64_t cut_y, int64_t cut_x,
+                       const void *views, void *stream);
+int phb_cutout_add_f32(float *obj, int64_t S, int64_t H, int64_t W,
+                       const int64_t *starts, int64_t B, int64_t cut_y, int64_t cut_x,
+                       const float *views, void *stream);
+
+/* Overwrite cutouts (last writer wins where views overlap, as in the reference).
+ * Replaces ObjectCutout.set (phaser/utils/object.py:521-538). */
+int phb_cutout_set_c64(void *obj, int64_t S, int64_t H, int64_t W,
+                       const int64_t *starts, int64_t B, int64_t cut_y, int64_t cut_x,
+                       const void *views, void *stream);
+
+/* --------------------------------------------------------------------- FFT (a5)
+ * Batched 2D FFT with phaser's convention: centred real space, orthonormal.
+ * inverse == 0: out = fft2(in)  = fft2(ifftshift(in)) / N   (phaser/utils/num.py:460-468)
+ * inverse == 1: out = ifft2(in) = fftshift(ifft2(in)) / N   (phaser/utils/num.py:434-442)
+ * N in {64, 128}; `in` and `out` may alias. */
+int phb_fft2_c64(const void *in, void *out, int64_t batch, int64_t N, int inverse, void *stream);
+
+/* ------------------------------------------------------------- constraints (a17)
+ * In-place amplitude clamp: a *= min(|a|, amplitude) / |a|.
+ * Replaces clamp_amplitude (phaser/engines/common/regularizers.py:36-42). */
+int phb_clamp_amplitude_c64(void *arr, int64_t n, float amplitude, void *stream);
+
+/* In-place Fourier filter of `batch` N x N tiles: a = ifft2(fft2(a) * mask), mask
+ * (N, N) float32 with the zero frequency in the corner.  Replaces
+ * LimitProbeSupport.apply_iter (phaser/engines/common/regularizers.py:45-64). */
+int phb_fourier_mask_c64(void *arr, int64_t batch, int64_t N, const float *mask, void *stream);
+
+/* ------------------------------------------------------ the multislice engine
+ * The LSQ-ML / ePIE / gradient mini-batch step
+ * (phaser/engines/conventional/solvers.py:132-504,
+ *  phaser/engines/gradient/run.py:357-438).
+ *
+ * One `phb_engine` describes a reconstruction resident on the device; the
+ * caller fills it once (see phb_engine_workspace_bytes for the scratch) and
+ * passes it to the per-group / per-iteration calls. */
+
+#define PHB_SOLVER_LSQML 0
+#define PHB_SOLVER_EPIE  1
+#define PHB_SOLVER_GRAD  2      /* gradient-engine loss + adjoint */
+
+#define PHB_NOISE_AMPLITUDE 0   /* also 'anscombe' (offset 0.375) */
+#define PHB_NOISE_POISSON   1   /* loss/gradient only (no wave update, as in the reference) */
+
+#define PHB_FLAG_UPDATE_OBJECT   1
+#define PHB_FLAG_UPDATE_PROBE    2
+#define PHB_FLAG_UPDATE_POSITION 4
+#define PHB_FLAG_CALC_ERROR      8
+
+typedef struct phb_engine {
+    /* sizes */
+    int32_t N;            /* probe / detector side: 64 or 128 */
+    int32_t M;            /* incoherent probe modes, 1..8 */
+    int32_t S;            /* object slices */
+    int32_t B_max;        /* largest group the workspace was sized for */
+    int64_t H, W;         /* object slice shape */
+    int64_t n_pos;        /* scan positions */
+    /* geometry (float64, as the reference computes cutout indices) */
+    double corner_y, corner_x, samp_y, samp_x;
+    /* state, updated in place */
+    void  *object;        /* (S, H, W) complex64 */
+    void  *probe;         /* (M, N, N) complex64, real space, centred */
+    float *scan;          /* (n_pos, 2) float32 (y, x) */
+    const float *tilt;    /* (n_pos, 2) float32 mrad, or NULL */
+    /* data */
+    const float *patterns;    /* (n_pos, N, N) float32, zero frequency in the corner */
+    const float *pattern_mask;/* (N, N) float32 */
+    const void  *propagators; /* (S-1, N, N) complex64 (band-limited, untilted) or NULL when S == 1 */
+    const float *thicknesses; /* (S) slice thicknesses, used for tilt ramps; NULL if no tilt */
+    const float *ky, *kx;     /* (N) fftfreq of the probe sampling, float32 */
+    /* noise model */
+    int32_t noise;        /* PHB_NOISE_* */
+    float noise_eps, noise_offset, noise_var;
+    /* workspace: phb_engine_workspace_bytes() bytes, 256-byte aligned */
+    void *workspace;
+    size_t workspace_bytes;
+    /* solver bookkeeping outputs (accumulated over the iteration) */
+    float *new_obj_mag;   /* (N, N) float32 or NULL */
+    float *new_probe_mag; /* (S, H, W) float32 or NULL */
+} phb_engine;
+
+typedef struct phb_step {
+    int32_t solver;       /* PHB_SOLVER_* */
+    int32_t flags;        /* PHB_FLAG_* */
+    float beta_object, beta_probe;
+    float illum_reg_object, illum_reg_probe, gamma;
+    float *pos_update;    /* (n_pos, 2) float32: this group's rows are written; may be NULL */
+    float *errors;        /* (n_pos) float32: per-position error of this group; may be NULL */
+    float *loss;          /* (n_pos) float32: gradient-engine per-position loss; may be NULL */
+    void  *grad_object;   /* gradient solver: (S, H, W) complex64 accumulator, NULL otherwise */
+    void  *grad_probe;    /* gradient solver: (M, N, N) complex64 accumulator */
+    float *grad_pos;      /* gradient solver: (n_pos, 2) float32 dL/d(y, x) */
+    int32_t *status;      /* device int, sticky: first group index that produced NaN/inf (or -1) */
+    int32_t group_index;  /* index of this group within the iteration (for `status`) */
+    const float *group_patterns; /* optional (B, N, N): this group's patterns in group order, read
+                                    instead of patterns[group[b]] (host-streamed data) */
+    void *event_begin;    /* optional cudaEvent_t recorded just before / after the fused kernel */
+    void *event_end;
+} phb_step;
+
+/* Bytes of workspace the engine needs for groups of up to B_max positions. */
+size_t phb_engine_workspace_bytes(int32_t N, int32_t M, int32_t S, int32_t B_max,
+                                  int64_t H, int64_t W);
+
+/* Validate the descriptor and prepare derived tables in the workspace
+ * (K-ordered propagators, mask, twiddles, probe spectrum). */
+int phb_engine_init(const phb_engine *e, void *stream);
+
+/* Refresh the cached probe spectrum after the caller changed `probe`
+ * (e.g. by a constraint or by rescaling). */
+int phb_engine_probe_changed(const phb_engine *e, void *stream);
+
+/* Presolve pass of LSQ-ML / ePIE (solvers.py:132-167, 387-412) or the gradient
+ * engine (gradient/run.py:413-438) over one group: accumulates per-position
+ * measured/model intensity into rescale_num/rescale_den (B, float64, must be
+ * zeroed by the caller).  LSQ-ML also adds the group illumination into
+ * new_probe_mag and |prod O|^2 into new_obj_mag.  `gradient_form` != 0 selects
+ * the gradient engine's variant (last slice transmitted, unmasked patterns). */
+int phb_presolve_group(const phb_engine *e, const int64_t *group, int32_t B, int32_t solver,
+                       int32_t gradient_form, double *rescale_num, double *rescale_den,
+                       void *stream);
+
+/* Forward model of one group (the gradient engine's form, gradient/run.py:357-400:
+ * subpixel-shifted probe, multislice propagation, last slice transmitted, far field):
+ * writes sum over modes of |fft2(exit wave)|^2 into intensity (B, N, N) float32, zero
+ * frequency in the corner -- the layout of measured patterns. */
+int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, float *intensity, void *stream);
+
+/* One mini-batch of the chosen solver: LSQ-ML (solvers.py:171-290), ePIE
+ * (solvers.py:415-504) or the gradient engine's loss and adjoint
+ * (gradient/run.py:357-405 under jax.value_and_grad).  Updates object/probe in
+ * place (LSQ-ML, ePIE) or accumulates gradients (GRAD). */
+int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
+                     void *stream);
+
+/* Per-iteration position update (phaser/engines/conventional/run.py:95-110 with
+ * phaser/engines/common/position_correction.py): subtract mean, momentum or
+ * steepest-descent step with norm clipping, subtract mean, scan += update, and
+ * count positions completely outside the object (-> *n_outside, device int). */
+int phb_position_update(float *scan, float *pos_update, float *momentum_state, int64_t n_pos,
+                        int32_t use_momentum, float step_size, float max_step /* <= 0: none */,
+                        float momentum, double obj_min_y, double obj_min_x,
+                        double obj_max_y, double obj_max_x, int32_t *n_outside, void *stream);
+
+/* Start of an iteration: *status = -1, errors[0:n] = NaN. */
+int phb_iteration_reset(int32_t *status, float *errors, int64_t n, void *stream);
+
+/* End of an iteration: out[0] = *status, out[1] = *n_outside (or 0 if NULL),
+ * out[2] = nanmean(errors[0:n]) (NaN if none), out[3] = number of non-NaN errors;
+ * `out` is 4 float64 (device memory, or host memory the device can write). */
+int phb_iteration_report(const int32_t *status, const int32_t *n_outside, const float *errors, int64_t n,
+                         double *out, void *stream);
+
+/* Kernel launches issued by this library since it was loaded (all streams). */
+int64_t phb_kernel_launches(void);
+
+/* cudaEvent_t helpers for callers without a CUDA runtime binding. */
+int phb_event_create(void **event);
+int phb_event_destroy(void *event);
+int phb_event_record(void *event, void *stream);
+int phb_event_elapsed_ms(void *start, void *end, float *ms);   /* synchronises on `end` */
+
+/* nanmean of `values` (n float32) into *out (float64); count of non-NaN into *count. */
+int phb_nanmean(const float *values, int64_t n, double *out, int64_t *count, void *stream);
+
+/* isfinite over a complex64 array: sets *status to `code` if any element is NaN/inf. */
+int phb_check_finite_c64(const void *arr, int64_t n, int32_t *status, int32_t code, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHASER_B200_H */

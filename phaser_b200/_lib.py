@@ -1,0 +1,149 @@
+"""ctypes binding of libphaser_b200.so (the C ABI in include/phaser_b200.h).
+
+The library is built in-tree by `phaser_b200.build`.  There is no fallback:
+if the shared object is missing or a call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / 'libphaser_b200.so'
+
+PHB_OK = 0
+PHB_ERR_INVALID_ARG = 1
+PHB_ERR_UNSUPPORTED = 2
+PHB_ERR_CUDA = 3
+PHB_ERR_NONFINITE = 4
+PHB_ERR_OUTSIDE = 5
+
+PHB_SOLVER_LSQML = 0
+PHB_SOLVER_EPIE = 1
+PHB_SOLVER_GRAD = 2
+
+PHB_NOISE_AMPLITUDE = 0
+PHB_NOISE_POISSON = 1
+
+PHB_FLAG_UPDATE_OBJECT = 1
+PHB_FLAG_UPDATE_PROBE = 2
+PHB_FLAG_UPDATE_POSITION = 4
+PHB_FLAG_CALC_ERROR = 8
+
+c_void_p = ctypes.c_void_p
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_f32 = ctypes.c_float
+c_f64 = ctypes.c_double
+c_size = ctypes.c_size_t
+
+
+class PhbEngine(ctypes.Structure):
+    """Mirror of `phb_engine` (include/phaser_b200.h)."""
+    _fields_ = [
+        ('N', c_i32), ('M', c_i32), ('S', c_i32), ('B_max', c_i32),
+        ('H', c_i64), ('W', c_i64), ('n_pos', c_i64),
+        ('corner_y', c_f64), ('corner_x', c_f64), ('samp_y', c_f64), ('samp_x', c_f64),
+        ('object', c_void_p), ('probe', c_void_p), ('scan', c_void_p), ('tilt', c_void_p),
+        ('patterns', c_void_p), ('pattern_mask', c_void_p), ('propagators', c_void_p),
+        ('thicknesses', c_void_p), ('ky', c_void_p), ('kx', c_void_p),
+        ('noise', c_i32), ('noise_eps', c_f32), ('noise_offset', c_f32), ('noise_var', c_f32),
+        ('workspace', c_void_p), ('workspace_bytes', c_size),
+        ('new_obj_mag', c_void_p), ('new_probe_mag', c_void_p),
+    ]
+
+
+class PhbStep(ctypes.Structure):
+    """Mirror of `phb_step` (include/phaser_b200.h)."""
+    _fields_ = [
+        ('solver', c_i32), ('flags', c_i32),
+        ('beta_object', c_f32), ('beta_probe', c_f32),
+        ('illum_reg_object', c_f32), ('illum_reg_probe', c_f32), ('gamma', c_f32),
+        ('pos_update', c_void_p), ('errors', c_void_p), ('loss', c_void_p),
+        ('grad_object', c_void_p), ('grad_probe', c_void_p), ('grad_pos', c_void_p),
+        ('status', c_void_p), ('group_index', c_i32),
+        ('group_patterns', c_void_p), ('event_begin', c_void_p), ('event_end', c_void_p),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    'phb_status_string': (ctypes.c_char_p, [c_i32]),
+    'phb_version': (c_i32, []),
+    'phb_last_cuda_error': (ctypes.c_char_p, []),
+    'phb_cutout_starts': (c_i32, [c_void_p, c_void_p, c_i64, c_f64, c_f64, c_f64, c_f64, c_i64, c_i64,
+                                  c_void_p, c_void_p, c_void_p]),
+    'phb_cutout_get_c64': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64,
+                                   c_f32, c_f32, c_void_p, c_void_p]),
+    'phb_cutout_get_f32': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64,
+                                   c_f32, c_void_p, c_void_p]),
+    'phb_cutout_add_c64': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64,
+                                   c_void_p, c_void_p]),
+    'phb_cutout_add_f32': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64,
+                                   c_void_p, c_void_p]),
+    'phb_cutout_set_c64': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i64, c_i64, c_i64,
+                                   c_void_p, c_void_p]),
+    'phb_fft2_c64': (c_i32, [c_void_p, c_void_p, c_i64, c_i64, c_i32, c_void_p]),
+    'phb_clamp_amplitude_c64': (c_i32, [c_void_p, c_i64, c_f32, c_void_p]),
+    'phb_fourier_mask_c64': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p]),
+    'phb_engine_workspace_bytes': (c_size, [c_i32, c_i32, c_i32, c_i32, c_i64, c_i64]),
+    'phb_engine_init': (c_i32, [ctypes.POINTER(PhbEngine), c_void_p]),
+    'phb_engine_probe_changed': (c_i32, [ctypes.POINTER(PhbEngine), c_void_p]),
+    'phb_presolve_group': (c_i32, [ctypes.POINTER(PhbEngine), c_void_p, c_i32, c_i32, c_i32,
+                                   c_void_p, c_void_p, c_void_p]),
+    'phb_solver_group': (c_i32, [ctypes.POINTER(PhbEngine), ctypes.POINTER(PhbStep), c_void_p, c_i32,
+                                 c_void_p]),
+    'phb_simulate_group': (c_i32, [ctypes.POINTER(PhbEngine), c_void_p, c_i32, c_void_p, c_void_p]),
+    'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
+                                    c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
+    'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),
+    'phb_iteration_reset': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
+    'phb_iteration_report': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p, c_void_p]),
+    'phb_kernel_launches': (c_i64, []),
+    'phb_event_create': (c_i32, [ctypes.POINTER(c_void_p)]),
+    'phb_event_destroy': (c_i32, [c_void_p]),
+    'phb_event_record': (c_i32, [c_void_p, c_void_p]),
+    'phb_event_elapsed_ms': (c_i32, [c_void_p, c_void_p, ctypes.POINTER(c_f32)]),
+    'phb_check_finite_c64': (c_i32, [c_void_p, c_i64, c_void_p, c_i32, c_void_p]),
+}
+
+EXPORTED = tuple(_SIGNATURES)
+
+_lib = None
+
+
+class PhbError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        lib = _lib
+        msg = lib.phb_status_string(status).decode() if lib else str(status)
+        if status == PHB_ERR_CUDA and lib is not None:
+            msg += f" ({lib.phb_last_cuda_error().decode()})"
+        super().__init__(f"{where}: {msg}")
+        self.status = status
+
+
+def load(path: os.PathLike | None = None) -> ctypes.CDLL:
+    """Load the shared library (once).  Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m phaser_b200.build` "
+                          "(the B200 backend has no CPU fallback)")
+    lib = ctypes.CDLL(str(p))
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> None:
+    """Call an entry point that returns a status; raise PhbError unless PHB_OK."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != PHB_OK:
+        raise PhbError(rc, name)

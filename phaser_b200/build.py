@@ -1,0 +1,67 @@
+"""Build libphaser_b200.so in-tree with nvcc for sm_100a.
+
+    python -m phaser_b200.build          # or phaser_b200.build.build()
+
+The library is a plain C ABI (include/phaser_b200.h); nothing here depends on
+torch.  Objects are rebuilt when a source or header is newer than the .so.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / 'csrc'
+LIB = PKG / 'libphaser_b200.so'
+SOURCES = ['phb_runtime.cu', 'phb_ops.cu', 'phb_engine.cu']
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+
+
+def nvcc() -> str:
+    cand = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def _stale() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    deps = list(CSRC.glob('*.cu')) + list(CSRC.glob('*.cuh')) + list(CSRC.glob('*.h'))
+    deps.append(ROOT / 'include' / 'phaser_b200.h')
+    return any(p.stat().st_mtime > t for p in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not _stale():
+        return LIB
+    out_dir = PKG / '_build'
+    out_dir.mkdir(exist_ok=True)
+    flags = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC',
+             '-Xptxas', '-v' if verbose else '-O3', *ARCH, f'-I{ROOT / "include"}']
+    objs = []
+    for src in SOURCES:
+        obj = out_dir / (Path(src).stem + '.o')
+        cmd = [nvcc(), '-c', str(CSRC / src), '-o', str(obj), *flags]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{res.stderr}")
+        if verbose:
+            sys.stderr.write(res.stderr)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix('.so.tmp')
+    cmd = [nvcc(), '-shared', '-o', str(tmp), *objs, *ARCH, '-lcudart']
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed:\n{res.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    print(build(force='--force' in sys.argv, verbose='-v' in sys.argv))

@@ -1,0 +1,303 @@
+// Register-resident 2D FFT of one N x N complex64 tile per CTA (N = 64, 128).
+//
+// A CTA of 512 threads holds the whole tile in registers (16 or 8 complex
+// values per thread) and exchanges through ONE N*N complex shared-memory
+// buffer.  A 1D line FFT of length N = E * NT runs as
+//     radix-E DFT in registers (elements strided by NT)
+//     -> twiddle W_N^{jj*k1} -> shared-memory exchange among the NT threads
+//        of the line -> E/NT radix-NT DFTs in registers,
+// so a 2D transform is 3 exchanges (line, transpose, line).  The forward
+// transform leaves the spectrum in a fixed permuted register order
+// ("K layout"); the inverse consumes that order and returns natural order
+// ("R layout").  Pointwise work between the two (propagators, the detector
+// constraint, shift filters) is done in K layout with explicit (ky, kx)
+// indices, so no reorder pass is ever needed.
+//
+// Layouts (tid = threadIdx.x, rsel = tid / 8, jl = tid % 8, unit u):
+//   R layout: v[u][q]          = x[row = rsel + 64u][col = jl + 8q]
+//   K layout: v[u][p*NT + k2]  = X[ky = (jl*P + p) + E*k2][kx = rsel + 64u]
+// The transforms are unnormalised DFTs with exp(-2 pi i nk/N) forward.
+//
+// Shared-memory addresses are XOR-swizzled so that every 8-byte access of a
+// half-warp (two lines x 8 threads) hits 16 distinct 8-byte bank pairs.
+#pragma once
+
+#include "phb_common.cuh"
+
+namespace phb {
+
+constexpr int FFT_THREADS = 512;
+
+template <int N> struct FFTCfg;
+template <> struct FFTCfg<128> { static constexpr int E = 16, NT = 8, P = 2, U = 2; };
+template <> struct FFTCfg<64>  { static constexpr int E = 8,  NT = 8, P = 1, U = 1; };
+
+// ----------------------------------------------------------------- small DFTs
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3) {
+    float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = csub(a1, a3);
+    float2 r3 = INV ? make_float2(-t3.y, t3.x) : make_float2(t3.y, -t3.x);   // * (+-i)
+    a0 = cadd(t0, t2);
+    a2 = csub(t0, t2);
+    a1 = cadd(t1, r3);
+    a3 = csub(t1, r3);
+}
+
+// multiply by W^e for the 16-point twiddles (forward sign); INV conjugates.
+template <int EXP>
+struct Tw16 {   // exp(-2 pi i EXP / 16)
+    static constexpr float C1 = 0.92387953251128674f, S1 = 0.38268343236508978f, R = 0.70710678118654752f;
+    static constexpr float re = EXP == 1 ? C1 : EXP == 2 ? R : EXP == 3 ? S1 : EXP == 6 ? -R : EXP == 9 ? -C1 : 1.f;
+    static constexpr float im = EXP == 1 ? -S1 : EXP == 2 ? -R : EXP == 3 ? -C1 : EXP == 6 ? -R : EXP == 9 ? S1 : 0.f;
+    static_assert(EXP == 0 || EXP == 1 || EXP == 2 || EXP == 3 || EXP == 4 || EXP == 6 || EXP == 9,
+                  "unsupported twiddle");
+};
+
+template <bool INV, int EXP>
+__device__ __forceinline__ float2 tw16(float2 a) {
+    if constexpr (EXP == 0) {
+        return a;
+    } else if constexpr (EXP == 4) {
+        return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+    } else {
+        return cmul(a, make_float2(Tw16<EXP>::re, INV ? -Tw16<EXP>::im : Tw16<EXP>::im));
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(float2 *x) {
+    constexpr float R = 0.70710678118654752f;
+    float2 e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
+    float2 o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    // o_k *= W8^k
+    float2 w1 = INV ? make_float2(R * (o1.x - o1.y), R * (o1.x + o1.y))
+                    : make_float2(R * (o1.x + o1.y), R * (o1.y - o1.x));
+    float2 w2 = INV ? make_float2(-o2.y, o2.x) : make_float2(o2.y, -o2.x);
+    float2 w3 = INV ? make_float2(-R * (o3.x + o3.y), R * (o3.x - o3.y))
+                    : make_float2(R * (o3.y - o3.x), -R * (o3.x + o3.y));
+    x[0] = cadd(e0, o0); x[4] = csub(e0, o0);
+    x[1] = cadd(e1, w1); x[5] = csub(e1, w1);
+    x[2] = cadd(e2, w2); x[6] = csub(e2, w2);
+    x[3] = cadd(e3, w3); x[7] = csub(e3, w3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft16(float2 *x) {
+    // n = q0 + 4*n1, k = k1 + 4*k2
+#pragma unroll
+    for (int q0 = 0; q0 < 4; ++q0) dft4<INV>(x[q0], x[q0 + 4], x[q0 + 8], x[q0 + 12]);
+    // x[q0 + 4*k1] = A[q0][k1]; twiddle W16^{q0*k1}
+    x[5] = tw16<INV, 1>(x[5]);  x[9] = tw16<INV, 2>(x[9]);  x[13] = tw16<INV, 3>(x[13]);
+    x[6] = tw16<INV, 2>(x[6]);  x[10] = tw16<INV, 4>(x[10]); x[14] = tw16<INV, 6>(x[14]);
+    x[7] = tw16<INV, 3>(x[7]);  x[11] = tw16<INV, 6>(x[11]); x[15] = tw16<INV, 9>(x[15]);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<INV>(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3]);
+    // slot 4*k1 + k2 holds X[k1 + 4*k2]: transpose 4x4 to natural order
+    float2 t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) t[k1 + 4 * k2] = x[4 * k1 + k2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = t[i];
+}
+
+template <int L, bool INV>
+__device__ __forceinline__ void dftL(float2 *x) {
+    if constexpr (L == 16) dft16<INV>(x);
+    else if constexpr (L == 8) dft8<INV>(x);
+    else static_assert(L < 0, "unsupported radix");
+}
+
+// --------------------------------------------------------------- addressing
+template <int N>
+struct Lay {
+    using C = FFTCfg<N>;
+    static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
+    // exchange among the NT threads of one line (row or column) L
+    static __device__ __forceinline__ int line(int L, int jj, int k1) {
+        return L * N + (((k1 ^ (L & 1)) * NT) + (jj ^ (k1 / P)));
+    }
+    static __device__ __forceinline__ int g(int r) {
+        if constexpr (N == 128) return (2 * r + (r & 1)) & 15;
+        else return ((r & 1) << 3) | (r & 6);
+    }
+    // transpose tile
+    static __device__ __forceinline__ int tile(int r, int c) { return r * N + (c ^ g(r)); }
+};
+
+// twiddle table: twid[k1 * NT + jj] = exp(-2 pi i jj k1 / N), N entries
+template <int N>
+__device__ __forceinline__ void fft_init_twiddles(float2 *twid) {
+    using C = FFTCfg<N>;
+    for (int i = threadIdx.x; i < C::E * C::NT; i += blockDim.x) {
+        int k1 = i / C::NT, jj = i % C::NT;
+        float s, c;
+        sincospif(-2.0f * (float)(jj * k1) / (float)N, &s, &c);
+        twid[i] = make_float2(c, s);
+    }
+}
+
+// ----------------------------------------------------------------- line passes
+template <int N>
+__device__ __forceinline__ void line_pass_fwd(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
+                                              const float2 *twid) {
+    using Ly = Lay<N>;
+    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
+    const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        dftL<E, false>(v[u]);
+#pragma unroll
+        for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmul(v[u][k1], twid[k1 * NT + jl]);
+        const int L = rsel + 64 * u;
+#pragma unroll
+        for (int k1 = 0; k1 < E; ++k1) xb[Ly::line(L, jl, k1)] = v[u][k1];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int L = rsel + 64 * u;
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+            for (int jj = 0; jj < NT; ++jj) v[u][p * NT + jj] = xb[Ly::line(L, jj, jl * P + p)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int p = 0; p < P; ++p) dftL<NT, false>(&v[u][p * NT]);
+}
+
+template <int N>
+__device__ __forceinline__ void line_pass_inv(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
+                                              const float2 *twid) {
+    using Ly = Lay<N>;
+    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
+    const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int L = rsel + 64 * u;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            dftL<NT, true>(&v[u][p * NT]);
+#pragma unroll
+            for (int jj = 0; jj < NT; ++jj) xb[Ly::line(L, jj, jl * P + p)] = v[u][p * NT + jj];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int L = rsel + 64 * u;
+#pragma unroll
+        for (int k1 = 0; k1 < E; ++k1) v[u][k1] = xb[Ly::line(L, jl, k1)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+#pragma unroll
+        for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmulc(v[u][k1], twid[k1 * NT + jl]);
+        dftL<E, true>(v[u]);
+    }
+}
+
+// row-pass output (K form of rows) -> column-pass input (R form of columns)
+template <int N>
+__device__ __forceinline__ void transpose_rk(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
+    using Ly = Lay<N>;
+    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
+    const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+            for (int k2 = 0; k2 < NT; ++k2)
+                xb[Ly::tile(rsel + 64 * u, (jl * P + p) + E * k2)] = v[u][p * NT + k2];
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int q = 0; q < E; ++q) v[u][q] = xb[Ly::tile(jl + NT * q, rsel + 64 * u)];
+    __syncthreads();
+}
+
+// column-pass output (R form of columns) -> row-pass input (K form of rows)
+template <int N>
+__device__ __forceinline__ void transpose_kr(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
+    using Ly = Lay<N>;
+    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
+    const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int q = 0; q < E; ++q) xb[Ly::tile(jl + NT * q, rsel + 64 * u)] = v[u][q];
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+            for (int k2 = 0; k2 < NT; ++k2)
+                v[u][p * NT + k2] = xb[Ly::tile(rsel + 64 * u, (jl * P + p) + E * k2)];
+    __syncthreads();
+}
+
+// Forward 2D DFT: R layout in, K layout out.
+template <int N>
+__device__ __forceinline__ void fft2_r2k(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
+                                         const float2 *twid) {
+    line_pass_fwd<N>(v, xb, twid);
+    transpose_rk<N>(v, xb);
+    line_pass_fwd<N>(v, xb, twid);
+}
+
+// Inverse 2D DFT (unnormalised): K layout in, R layout out.
+template <int N>
+__device__ __forceinline__ void ifft2_k2r(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
+                                          const float2 *twid) {
+    line_pass_inv<N>(v, xb, twid);
+    transpose_kr<N>(v, xb);
+    line_pass_inv<N>(v, xb, twid);
+}
+
+// ------------------------------------------------------------- index helpers
+template <int N>
+struct Idx {
+    using C = FFTCfg<N>;
+    static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
+    // R layout
+    static __device__ __forceinline__ int row(int u) { return (threadIdx.x >> 3) + 64 * u; }
+    static __device__ __forceinline__ int col(int q) { return (threadIdx.x & 7) + NT * q; }
+    // K layout
+    static __device__ __forceinline__ int kx(int u) { return (threadIdx.x >> 3) + 64 * u; }
+    static __device__ __forceinline__ int ky(int e) {
+        return ((threadIdx.x & 7) * P + e / NT) + E * (e % NT);
+    }
+    // register-order flat index (coalesced per warp), used for scratch and packed tables
+    static __device__ __forceinline__ int flat(int u, int e) { return (u * E + e) * FFT_THREADS + threadIdx.x; }
+};
+
+// decode a register-order flat index (from any thread) to (row, col) in R layout
+template <int N>
+__device__ __forceinline__ void flat_to_rc(int f, int &r, int &c) {
+    using C = FFTCfg<N>;
+    const int t = f % FFT_THREADS, s = f / FFT_THREADS;   // s = u*E + q
+    const int u = s / C::E, q = s % C::E;
+    r = (t >> 3) + 64 * u;
+    c = (t & 7) + C::NT * q;
+}
+// ... and to (ky, kx) in K layout
+template <int N>
+__device__ __forceinline__ void flat_to_k(int f, int &ky, int &kx) {
+    using C = FFTCfg<N>;
+    const int t = f % FFT_THREADS, s = f / FFT_THREADS;
+    const int u = s / C::E, e = s % C::E;
+    kx = (t >> 3) + 64 * u;
+    ky = ((t & 7) * C::P + e / C::NT) + C::E * (e % C::NT);
+}
+
+}  // namespace phb

@@ -1,0 +1,233 @@
+"""Conventional (LSQ-ML / ePIE) engine on the B200 kernels.
+
+Drop-in for `phaser.engines.conventional.run:run_engine`
+(phaser/engines/conventional/run.py:15-123): same EngineArgs / plan inputs,
+same iteration structure (presolve rescale, per-iteration groupings, group
+steps, iteration constraints, position update, detector error), same
+exceptions.  Each mini-batch is one fused kernel launch plus small apply
+kernels (libphaser_b200, phb_solver_group); the host only builds the seeded
+groupings and reads back one status block per iteration.
+"""
+from __future__ import annotations
+
+import logging
+import typing as t
+
+import numpy
+import torch
+
+from .. import plan as P
+from .. import _lib
+from ..constraints import build_constraints
+from ..device import DeviceEngine, NoiseSpec
+from ..groups import GroupManager, mask_fraction_of_groups
+from ..sampling import ObjectSampling
+
+logger = logging.getLogger(__name__)
+
+
+def _object_sampling(s) -> ObjectSampling:
+    if isinstance(s, ObjectSampling):
+        return s
+    return ObjectSampling(tuple(s.shape), s.sampling, s.corner,
+                          getattr(s, 'region_min', None), getattr(s, 'region_max', None))
+
+
+def _noise(props) -> NoiseSpec:
+    kind, np_ = P.noise_model(P.get(props, 'noise_model'))
+    return NoiseSpec(kind, float(P.get(np_, 'eps', 1e-3)), float(P.get(np_, 'offset', 0.0)),
+                     float(P.get(np_, 'gaussian_variance', 0.1)))
+
+
+def _call(observer, name: str, *args, **kwargs) -> None:
+    f = getattr(observer, name, None) if observer is not None else None
+    if callable(f):
+        f(*args, **kwargs)
+
+
+class _SolverBase:
+    kind = ''
+
+    def __init__(self, engine_plan, props):
+        self.engine_plan = engine_plan
+        self.plan = props
+
+    @classmethod
+    def name(cls) -> str:
+        return cls.__name__.replace('Solver', '')
+
+    def schedules(self, fargs) -> t.Dict[str, float]:
+        out = {}
+        for key, default in (('beta_object', 1.0), ('beta_probe', 1.0), ('illum_reg_object', 1e-2),
+                             ('illum_reg_probe', 1e-2), ('gamma', 1e-4)):
+            out[key] = P.process_schedule(P.get(self.plan, key, default))(fargs)
+        return out
+
+
+class LSQMLSolver(_SolverBase):
+    """LSQ-ML (phaser/engines/conventional/solvers.py:18-128) on the fused kernel."""
+    kind = 'lsqml'
+
+
+class EPIESolver(_SolverBase):
+    """ePIE / 3PIE (phaser/engines/conventional/solvers.py:293-383) on the fused kernel."""
+    kind = 'epie'
+
+
+SOLVERS = {'lsqml': LSQMLSolver, 'epie': EPIESolver}
+
+
+class ConventionalEngine:
+    """One conventional-engine run on the device: construction uploads the
+    state, `presolve()` rescales the probe, `iteration(i)` runs one full
+    iteration (all mini-batches, constraints, position update, error), and
+    `finish()` writes the result back into the host state."""
+
+    def __init__(self, args: t.Mapping[str, t.Any], props: t.Any, *,
+                 patterns_on_device: t.Optional[torch.Tensor] = None):
+        state = args['state']
+        data = args['data']
+        self.state = state
+        self.observer = args.get('observer', None)
+        dtype = numpy.dtype(args.get('dtype', numpy.float32))
+        if dtype != numpy.float32:
+            raise NotImplementedError("the B200 backend computes in float32/complex64 (plan dtype 'float32')")
+        self.noise = _noise(props)
+        if self.noise.kind == 'poisson':
+            # the reference's Poisson model has no wave update (noise_models.py:104-112)
+            raise NotImplementedError("the Poisson noise model has no wave update; use 'amplitude' or 'anscombe'")
+        self.solver_kind, solver_props = P.solver(P.get(props, 'solver'))
+        self.solver = SOLVERS[self.solver_kind](props, solver_props)
+        self.pos_solver = P.position_solver(P.get(props, 'position_solver'))
+        self.niter = int(P.get(props, 'niter', 10))
+        grouping = int(P.get(props, 'grouping', None) or 64)
+        self.compact = bool(P.get(props, 'compact', False))
+        self.update_probe = P.process_flag(P.get(props, 'update_probe', True))
+        self.update_object = P.process_flag(P.get(props, 'update_object', True))
+        self.update_positions = P.process_flag(P.get(props, 'update_positions', False))
+        self.calc_error = P.process_flag(P.get(props, 'calc_error', P.Flag(every=1)))
+        self.shuffle_groups = P.process_flag(P.get(props, 'shuffle_groups', None) or not self.compact)
+
+        probe0 = numpy.asarray(state.probe.data)
+        obj0 = numpy.asarray(state.object.data)
+        self.scan0 = numpy.asarray(state.scan)
+        if probe0.dtype != numpy.complex64 or obj0.dtype != numpy.complex64:
+            raise TypeError("object and probe must be complex64")
+        osamp = _object_sampling(state.object.sampling)
+        thick = numpy.asarray(state.object.thicknesses)
+        self.eng = eng = DeviceEngine(
+            probe=probe0, obj=obj0, scan=self.scan0,
+            patterns=None if patterns_on_device is not None else numpy.asarray(data.patterns),
+            mask=numpy.asarray(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
+            obj_sampling=osamp, thicknesses=thick, wavelength=float(state.wavelength),
+            tilt=None if state.tilt is None else numpy.asarray(state.tilt), noise=self.noise,
+            bwlim_frac=P.get(props, 'bwlim_frac', 2 / 3), group_max=grouping,
+            patterns_on_device=patterns_on_device)
+        self.group_cons = build_constraints(P.get(props, 'group_constraints', []) or [], eng, state, per_group=True)
+        self.iter_cons = build_constraints(P.get(props, 'iter_constraints', []) or [], eng, state, per_group=False)
+        self.groups = GroupManager(self.scan0.shape[:-1], grouping, self.compact, seed=args.get('seed', None))
+        self.calc_error_mask = mask_fraction_of_groups(len(self.groups),
+                                                       float(P.get(props, 'calc_error_fraction', 0.1)))
+        self.mom_state = None
+        if self.pos_solver is not None and self.pos_solver[0] == 'momentum':
+            self.mom_state = torch.zeros_like(eng.scan)
+        self.start_i = int(state.iter.total_iter)
+        self.status_host = torch.empty((4,), dtype=torch.float64).pin_memory()
+        self.fused_events: t.Optional[t.List[t.Tuple[int, int]]] = None
+        _call(self.observer, 'init_engine', state, recons_name=args.get('recons_name', ''), plan=props,
+              noise_model=self.noise.kind)
+
+    def presolve(self) -> float:
+        """Probe intensity rescale (solvers.py:36-63, 306-329)."""
+        first = self.groups.iter(self.scan0 if self.compact else None, 0)
+        gt, sizes = self.eng.group_tensor([self.groups.flat(g) for g in first])
+        rescale = self.eng.presolve(gt, sizes, self.solver_kind)
+        logger.info(f"Rescaling initial probe intensity by {rescale:.2e}")
+        self.eng.probe.mul_(float(numpy.sqrt(rescale)))
+        self.eng.probe_changed()
+        _call(self.observer, 'start_engine', self.state)
+        return rescale
+
+    def iteration(self, i: int, *, sync: bool = True) -> t.Optional[float]:
+        """Run iteration i (1-based).  With sync=True, wait for the device, raise
+        on NaN / positions outside the object, record and return the error."""
+        eng, state = self.eng, self.state
+        state.iter.engine_iter = i
+        state.iter.total_iter = self.start_i + i
+        fargs = {'state': state, 'niter': self.niter}
+        it_pos = self.update_positions(fargs)
+        it_err = self.calc_error(fargs)
+        flags = ((_lib.PHB_FLAG_UPDATE_OBJECT if self.update_object(fargs) else 0)
+                 | (_lib.PHB_FLAG_UPDATE_PROBE if self.update_probe(fargs) else 0)
+                 | (_lib.PHB_FLAG_UPDATE_POSITION if it_pos else 0))
+        sched = self.solver.schedules(fargs)
+        scan_host = eng.scan.cpu().numpy().reshape(self.scan0.shape) if self.compact else None
+        glist = self.groups.iter(scan_host, i, self.shuffle_groups(fargs))
+        gt, sizes = eng.group_tensor([self.groups.flat(g) for g in glist])
+        eng.iteration_reset()
+        for gi, B in enumerate(sizes):
+            f = flags | (_lib.PHB_FLAG_CALC_ERROR if (it_err and self.calc_error_mask[gi]) else 0)
+            ev = None
+            if self.fused_events is not None:
+                ev = _new_event_pair()
+                self.fused_events.append(ev)
+            eng.step(self.solver_kind, gt[gi], B, flags=f, group_index=gi, events=ev, **sched)
+            for con in self.group_cons:
+                con.apply_group()
+        for con in self.iter_cons:
+            con.apply_iter()
+        if it_pos:
+            if self.pos_solver is None:
+                raise ValueError("Updating positions with no PositionSolver specified")
+            kind, pp = self.pos_solver
+            step = float(P.get(pp, 'step_size', 1e-2))
+            # the reference's steepest-descent solver clips at step_size (position_correction.py:16)
+            maxs = P.get(pp, 'max_step_size', None) if kind == 'momentum' else step
+            eng.position_update(self.mom_state, step, maxs, float(P.get(pp, 'momentum', 0.9)))
+        # one device->host status block per iteration
+        eng.iteration_report(eng.report)
+        self.status_host.copy_(eng.report, non_blocking=True)
+        if not sync:
+            return None
+        torch.cuda.current_stream().synchronize()
+        return self.check(i, it_pos, it_err)
+
+    def check(self, i: int, it_pos: bool = True, it_err: bool = True) -> t.Optional[float]:
+        state, eng = self.state, self.eng
+        bad_group, n_out, err = int(self.status_host[0]), int(self.status_host[1]), float(self.status_host[2])
+        if bad_group >= 0:
+            raise ValueError(f"NaN or inf encountered in object or probe, group {bad_group}")
+        if it_pos and n_out > 0:
+            raise ValueError(f"{n_out}/{eng.n_pos} probe positions completely outside object")
+        error = err if it_err else None
+        if error is not None:
+            state.progress.iters = numpy.concatenate([state.progress.iters, [i + self.start_i]])
+            state.progress.detector_errors = numpy.concatenate([state.progress.detector_errors, [error]])
+        _call(self.observer, 'update_iteration', state, i, self.niter, error)
+        return error
+
+    def finish(self):
+        probe, obj, scan = self.eng.host_state()
+        self.state.probe.data = probe
+        self.state.object.data = obj
+        self.state.scan = scan.astype(self.scan0.dtype)
+        _call(self.observer, 'finish_engine', self.state)
+        return self.state
+
+
+def _new_event_pair() -> t.Tuple[int, int]:
+    import ctypes
+    a, b = ctypes.c_void_p(), ctypes.c_void_p()
+    _lib.call('phb_event_create', ctypes.byref(a))
+    _lib.call('phb_event_create', ctypes.byref(b))
+    return a.value, b.value
+
+
+def run_engine(args: t.Mapping[str, t.Any], props: t.Any) -> t.Any:
+    """Run a conventional engine; returns the (updated) ReconsState.
+    Signature of phaser.engines.conventional.run:run_engine (run.py:15)."""
+    eng = ConventionalEngine(args, props)
+    eng.presolve()
+    for i in range(1, eng.niter + 1):
+        eng.iteration(i)
+    return eng.finish()

@@ -1,0 +1,178 @@
+"""Engine plan types for the B200 backend, field-compatible with phaser's.
+
+phaser's own plan classes (phaser/plan.py:43-160, phaser/hooks/solver.py:80-99)
+are `pane` dataclasses and its hooks are `Hook(ref, props, type)` objects.
+The B200 engines accept those directly (duck-typed), plain dicts of the same
+shape (what a plan YAML becomes), or the small dataclasses defined here,
+which carry the same field names and defaults.
+"""
+from __future__ import annotations
+
+import dataclasses
+import typing as t
+
+
+@dataclasses.dataclass(eq=False)
+class Flag:
+    """Iteration flag (phaser/types.py:125-145): true when after < i, (i-after) % every == 0, i < before."""
+    after: int = 0
+    every: int = 1
+    before: t.Optional[int] = None
+
+    def __call__(self, args) -> bool:
+        i = args['state'].iter.engine_iter
+        return (self.before is None or i < self.before) and i > self.after and (i - self.after) % self.every == 0
+
+
+@dataclasses.dataclass(eq=False)
+class AmplitudeNoisePlan:
+    gaussian_variance: float = 0.1
+    eps: float = 1.0e-3
+    offset: float = 0.0
+
+
+@dataclasses.dataclass(eq=False)
+class AnscombeNoisePlan(AmplitudeNoisePlan):
+    offset: float = 0.375
+
+
+@dataclasses.dataclass(eq=False)
+class PoissonNoisePlan(AmplitudeNoisePlan):
+    eps: float = 1.0e-3
+
+
+@dataclasses.dataclass(eq=False)
+class LSQMLSolverPlan:
+    stochastic: bool = True
+    beta_object: t.Any = 1.0
+    beta_probe: t.Any = 1.0
+    illum_reg_object: t.Any = 1e-2
+    illum_reg_probe: t.Any = 1e-2
+    gamma: t.Any = 1e-4
+
+
+@dataclasses.dataclass(eq=False)
+class EPIESolverPlan:
+    beta_object: t.Any = 1.0
+    beta_probe: t.Any = 1.0
+
+
+@dataclasses.dataclass(eq=False)
+class SteepestDescentPositionSolverProps:
+    step_size: float = 1e-2
+    max_step_size: t.Optional[float] = None
+
+
+@dataclasses.dataclass(eq=False)
+class MomentumPositionSolverProps:
+    step_size: float = 1e-2
+    max_step_size: t.Optional[float] = None
+    momentum: float = 0.9
+
+
+@dataclasses.dataclass(eq=False)
+class HookSpec:
+    """A resolved hook: `type` is the registry name ('lsqml', 'amplitude', ...)."""
+    type: str
+    props: t.Any = None
+
+
+@dataclasses.dataclass(eq=False)
+class ConventionalEnginePlan:
+    """Fields of phaser's ConventionalEnginePlan that the engine reads."""
+    noise_model: t.Any = dataclasses.field(default_factory=lambda: HookSpec('amplitude', AmplitudeNoisePlan()))
+    solver: t.Any = dataclasses.field(default_factory=lambda: HookSpec('lsqml', LSQMLSolverPlan()))
+    position_solver: t.Any = None
+    group_constraints: t.List[t.Any] = dataclasses.field(default_factory=list)
+    iter_constraints: t.List[t.Any] = dataclasses.field(default_factory=list)
+    niter: int = 10
+    grouping: t.Optional[int] = None
+    compact: bool = False
+    shuffle_groups: t.Any = None
+    buffer_n_groups: int = 2
+    update_probe: t.Any = True
+    update_object: t.Any = True
+    update_positions: t.Any = False
+    update_tilt: t.Any = False
+    calc_error: t.Any = dataclasses.field(default_factory=lambda: Flag(every=1))
+    calc_error_fraction: float = 0.1
+    bwlim_frac: t.Optional[float] = 2 / 3
+    send_every_group: bool = False
+
+
+_NOISE_DEFAULTS = {'amplitude': AmplitudeNoisePlan, 'anscombe': AnscombeNoisePlan, 'poisson': PoissonNoisePlan}
+_SOLVER_DEFAULTS = {'lsqml': LSQMLSolverPlan, 'epie': EPIESolverPlan}
+_POS_DEFAULTS = {'momentum': MomentumPositionSolverProps, 'steepest_descent': SteepestDescentPositionSolverProps}
+_REF_CLASS_NAMES = {
+    'AmplitudeNoiseModel': 'amplitude', 'AnscombeNoiseModel': 'anscombe', 'PoissonNoiseModel': 'poisson',
+    'LSQMLSolver': 'lsqml', 'EPIESolver': 'epie',
+    'MomentumPositionSolver': 'momentum', 'SteepestDescentPositionSolver': 'steepest_descent',
+    'ClampObjectAmplitude': 'clamp_object_amplitude', 'LimitProbeSupport': 'limit_probe_support',
+}
+
+
+def resolve_hook(hook: t.Any, defaults: t.Mapping[str, type]) -> t.Tuple[str, t.Any]:
+    """(registry name, props) for a phaser Hook, a dict, a string, or a HookSpec."""
+    if hook is None:
+        raise ValueError("missing hook")
+    if isinstance(hook, str):
+        name, props = hook, None
+    elif isinstance(hook, dict):
+        hook = dict(hook)
+        name = str(hook.pop('type'))
+        props = hook
+    else:
+        name = getattr(hook, 'type', None) or getattr(hook, 'ref', None)
+        props = getattr(hook, 'props', None)
+    if name is None:
+        raise ValueError(f"can't resolve hook {hook!r}")
+    name = str(name)
+    if ':' in name:   # 'module:Class' reference to a known reference implementation
+        name = _REF_CLASS_NAMES.get(name.rsplit(':', 1)[1], name)
+    name = name.lower()
+    base = defaults.get(name)
+    if base is None:
+        raise NotImplementedError(f"hook '{name}' is not implemented by the B200 backend")
+    if props is None or props == {}:
+        props = base()
+    elif isinstance(props, dict):
+        props = base(**props)
+    return name, props
+
+
+def noise_model(hook) -> t.Tuple[str, t.Any]:
+    return resolve_hook(hook, _NOISE_DEFAULTS)
+
+
+def solver(hook) -> t.Tuple[str, t.Any]:
+    return resolve_hook(hook, _SOLVER_DEFAULTS)
+
+
+def position_solver(hook) -> t.Optional[t.Tuple[str, t.Any]]:
+    return None if hook is None else resolve_hook(hook, _POS_DEFAULTS)
+
+
+def process_flag(flag: t.Any) -> t.Callable[[t.Mapping[str, t.Any]], bool]:
+    """bool or callable Flag -> predicate of {'state', 'niter'} (phaser/types.py:157-161)."""
+    if isinstance(flag, bool) or flag is None:
+        val = bool(flag)
+        return lambda args: val
+    if isinstance(flag, dict):
+        flag = Flag(**flag)
+    return flag
+
+
+def process_schedule(sched: t.Any) -> t.Callable[[t.Mapping[str, t.Any]], float]:
+    """float or callable schedule -> value for this iteration (phaser/hooks/schedule.py)."""
+    if isinstance(sched, (int, float)):
+        val = float(sched)
+        return lambda args: val
+    if callable(sched):
+        return lambda args: float(sched(args))
+    raise TypeError(f"unsupported schedule {sched!r}")
+
+
+def get(props: t.Any, name: str, default: t.Any = None) -> t.Any:
+    if isinstance(props, dict):
+        return props.get(name, default)
+    return getattr(props, name, default)

@@ -1,0 +1,188 @@
+"""GPU parity of the fused multislice engine against the numpy oracle
+(itself pinned to the reference by test_oracle_golden.py).
+
+Tolerances (complex64 arithmetic, float64 step-size sums on the GPU, float32
+sums in the oracle): forward model within 1e-5 relative L2; one mini-batch
+step's object / probe within 1e-5 relative L2 of the oracle (their UPDATES
+within 1e-3); per-position errors within 1e-4; position steps within 2e-3
+(a ratio of two float32-accumulated sums in the oracle)."""
+import numpy
+import pytest
+import torch
+
+from oracle import phaser_np as P
+from phaser_b200 import _lib
+from phaser_b200.device import DeviceEngine, NoiseSpec
+from phaser_b200.engines.conventional import run_engine
+from phaser_b200 import plan as PL
+from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
+from phaser_b200.sampling import Sampling
+
+from .cases import make_case
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = numpy.asarray(a, numpy.complex128)
+    b = numpy.asarray(b, numpy.complex128)
+    return float(numpy.linalg.norm(a - b) / numpy.linalg.norm(b))
+
+
+def engine_for(c, group_max, noise=NoiseSpec()):
+    return DeviceEngine(probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+                        probe_sampling=c.probe_sampling, obj_sampling=c.osamp, thicknesses=c.thick,
+                        wavelength=c.wavelength, tilt=c.tilt, noise=noise, group_max=group_max)
+
+
+CONFIGS = [
+    dict(seed=1, N=64, M=1, S=1),
+    dict(seed=2, N=64, M=2, S=3),
+    dict(seed=3, N=128, M=4, S=2),
+    dict(seed=4, N=64, M=3, S=2, tilt=True),
+    dict(seed=5, N=128, M=1, S=3, scan_shape=(3, 3)),
+]
+
+
+@pytest.mark.parametrize('cfg', CONFIGS, ids=lambda c: f"N{c['N']}M{c['M']}S{c['S']}{'t' if c.get('tilt') else ''}")
+def test_forward_model_matches_oracle(cfg):
+    c = make_case(**cfg)
+    n = c.scan.shape[0] * c.scan.shape[1]
+    eng = engine_for(c, n)
+    idx = numpy.arange(n, dtype=numpy.int64)
+    gt, sizes = eng.group_tensor([idx])
+    sim = eng.simulate(gt[0], sizes[0]).cpu().numpy()
+    g = c.geom()
+    flat = c.scan.reshape(-1, 2)
+    psi0, cuts, _, _ = P.cutout_group(g, c.probe, c.obj, flat)
+    pt = P.tilt_propagators(g.ky, g.kx, c.thick, c.props(), None if c.tilt is None else c.tilt.reshape(-1, 2))
+    psi = P._forward(psi0, cuts, pt)
+    ref = numpy.sum(P.abs2(P.fft2c(psi[-1] * cuts[:, -1, None])), axis=1)
+    assert rel_l2(sim, ref) < 1e-5
+
+
+def run_group(c, solver, flags_kw, params, noise=P.NoiseModel()):
+    n = c.scan.shape[0] * c.scan.shape[1]
+    rng = numpy.random.default_rng(99)
+    idx = rng.permutation(n)[: max(2, (2 * n) // 3)].astype(numpy.int64)
+    spec = NoiseSpec('anscombe' if noise.offset else 'amplitude', noise.eps, noise.offset, noise.gaussian_variance)
+    eng = engine_for(c, len(idx), spec)
+    gt, sizes = eng.group_tensor([idx])
+    flags = (_lib.PHB_FLAG_CALC_ERROR
+             | (_lib.PHB_FLAG_UPDATE_OBJECT if flags_kw.get('update_object', True) else 0)
+             | (_lib.PHB_FLAG_UPDATE_PROBE if flags_kw.get('update_probe', True) else 0)
+             | (_lib.PHB_FLAG_UPDATE_POSITION if flags_kw.get('update_position', True) else 0))
+    eng.status.fill_(-1)
+    if solver == 'lsqml':
+        eng.step('lsqml', gt[0], sizes[0], flags=flags, beta_object=params.beta_object,
+                 beta_probe=params.beta_probe, illum_reg_object=params.illum_reg_object,
+                 illum_reg_probe=params.illum_reg_probe, gamma=params.gamma)
+    else:
+        eng.step('epie', gt[0], sizes[0], flags=flags, beta_object=params.beta_object,
+                 beta_probe=params.beta_probe)
+    probe, obj, _ = eng.host_state()
+    errors = eng.errors.cpu().numpy()[idx]
+    pos = eng.pos_update.cpu().numpy()[idx]
+    assert int(eng.status.cpu()[0]) == -1
+    g = c.geom()
+    tl = None if c.tilt is None else c.tilt.reshape(-1, 2)[idx]
+    fn = P.lsqml_group if solver == 'lsqml' else P.epie_group
+    ref = fn(g, c.probe, c.obj, c.scan.reshape(-1, 2)[idx], c.patterns.reshape(-1, *c.probe.shape[-2:])[idx],
+             c.mask, c.props(), tl, noise, params, **flags_kw)
+    return dict(obj=obj, probe=probe, errors=errors, pos=pos), ref
+
+
+GROUP_CONFIGS = [
+    ('lsqml', dict(seed=21, N=64, M=2, S=3), {}),
+    ('lsqml', dict(seed=22, N=128, M=4, S=2), {}),
+    ('lsqml', dict(seed=23, N=64, M=1, S=1), {}),
+    ('lsqml', dict(seed=24, N=64, M=2, S=2, tilt=True), {}),
+    ('lsqml', dict(seed=25, N=128, M=2, S=2), dict(update_probe=False)),
+    ('epie', dict(seed=26, N=64, M=2, S=3), {}),
+    ('epie', dict(seed=27, N=128, M=1, S=2), {}),
+]
+
+
+@pytest.mark.parametrize('solver,cfg,flags', GROUP_CONFIGS,
+                         ids=[f"{s}-N{c['N']}M{c['M']}S{c['S']}-{i}" for i, (s, c, f) in enumerate(GROUP_CONFIGS)])
+def test_group_step_matches_oracle(solver, cfg, flags):
+    c = make_case(**cfg)
+    params = (P.LSQMLParams(0.9, 0.8, 1e-2, 1e-2, 1e-4) if solver == 'lsqml' else P.EPIEParams(0.7, 0.6))
+    got, ref = run_group(c, solver, dict(flags, update_position=True), params)
+    d_obj = rel_l2(got['obj'] - c.obj, ref['object'] - c.obj)
+    d_probe = rel_l2(got['probe'] - c.probe, ref['probe'] - c.probe) if flags.get('update_probe', True) else 0.0
+    assert rel_l2(got['obj'], ref['object']) < 1e-5, d_obj
+    assert rel_l2(got['probe'], ref['probe']) < 1e-5, d_probe
+    assert d_obj < 1e-3
+    assert d_probe < 1e-3
+    assert numpy.allclose(got['errors'], ref['errors'], rtol=1e-4)
+    assert rel_l2(got['pos'], ref['pos_update']) < 2e-3
+
+
+def test_presolve_rescale_matches_oracle():
+    c = make_case(seed=31, N=64, M=2, S=3)
+    n = c.scan.shape[0] * c.scan.shape[1]
+    eng = engine_for(c, 8)
+    flat = numpy.arange(n, dtype=numpy.int64)
+    chunks = [flat[i:i + 8] for i in range(0, n, 8)]
+    gt, sizes = eng.group_tensor(chunks)
+    r = eng.presolve(gt, sizes, 'lsqml')
+    g = c.geom()
+    ref = []
+    for ch in chunks:
+        ref.append(P.epie_dry_run(g, c.probe, c.obj, c.scan.reshape(-1, 2)[ch],
+                                  c.patterns.reshape(-1, 64, 64)[ch], c.mask, c.props(), None))
+    assert r == pytest.approx(float(numpy.mean(numpy.concatenate(ref))), rel=1e-5)
+
+
+def make_state(c):
+    N = c.probe.shape[-1]
+    return ReconsState(iter=IterState(), wavelength=c.wavelength,
+                       probe=ProbeState(Sampling((N, N), sampling=c.probe_sampling), c.probe.copy()),
+                       object=ObjectState(c.osamp, c.obj.copy(), c.thick.copy()),
+                       scan=c.scan.copy(), tilt=None)
+
+
+@pytest.mark.parametrize('solver', ['lsqml', 'epie'])
+def test_run_engine_matches_oracle(solver):
+    c = make_case(seed=41, N=64, M=2, S=2, scan_shape=(5, 5))
+    props = PL.ConventionalEnginePlan(
+        noise_model={'type': 'amplitude', 'eps': 1e-2},
+        solver={'type': solver, 'beta_object': 0.9, 'beta_probe': 0.8, 'gamma': 1e-3},
+        position_solver={'type': 'momentum', 'step_size': 1e-2, 'max_step_size': 0.2, 'momentum': 0.9},
+        niter=3, grouping=10, update_positions=True, calc_error_fraction=0.5)
+    state = run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                        'seed': 'engine-seed', 'recons_name': 't'}, props)
+    run = P.ConventionalRun(solver=solver, niter=3, grouping=10, seed='engine-seed', noise=P.NoiseModel(eps=1e-2),
+                            lsqml=P.LSQMLParams(0.9, 0.8, 1e-2, 1e-2, 1e-3), epie=P.EPIEParams(0.9, 0.8),
+                            update_positions=True, position_solver='momentum', pos_step_size=1e-2,
+                            pos_max_step=0.2, pos_momentum=0.9, calc_error_fraction=0.5)
+    probe, obj, scan, errors = P.run_conventional(
+        run, probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+        probe_sampling=c.probe_sampling, corner=c.osamp.corner, obj_sampling=c.osamp.sampling,
+        thicknesses=c.thick, wavelength=c.wavelength)
+    assert rel_l2(state.object.data, obj) < 1e-4
+    assert rel_l2(state.probe.data, probe) < 1e-4
+    assert numpy.max(numpy.abs(state.scan - scan)) < 1e-4
+    assert numpy.allclose(state.progress.detector_errors, errors, rtol=1e-3)
+
+
+def test_nonfinite_pattern_raises_value_error():
+    c = make_case(seed=51, N=64, M=1, S=1, scan_shape=(4, 4))
+    c.patterns[1, 2, 5, 5] = numpy.inf
+    props = PL.ConventionalEnginePlan(niter=1, grouping=8)
+    with pytest.raises(ValueError, match="NaN or inf encountered in object or probe, group"):
+        run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                    'seed': 1, 'recons_name': 't'}, props)
+
+
+def test_unsupported_shapes_fail_loudly():
+    c = make_case(seed=52, N=64, M=1, S=1, scan_shape=(2, 2))
+    with pytest.raises(NotImplementedError):
+        DeviceEngine(probe=numpy.zeros((1, 96, 96), numpy.complex64), obj=c.obj, scan=c.scan,
+                     patterns=numpy.zeros((4, 96, 96), numpy.float32), mask=numpy.ones((96, 96), numpy.float32),
+                     probe_sampling=c.probe_sampling, obj_sampling=c.osamp, thicknesses=c.thick,
+                     wavelength=c.wavelength)
+    eng = engine_for(c, 2)
+    with pytest.raises(ValueError):
+        eng.group_tensor([numpy.arange(4)])

@@ -1,0 +1,93 @@
+"""Host-side logic of the backend against the reference fixtures (CPU only)."""
+import json
+import os
+
+import numpy
+import pytest
+from numpy.testing import assert_array_equal, assert_allclose
+
+from phaser_b200 import groups as G
+from phaser_b200 import plan as P
+from phaser_b200 import optics
+from phaser_b200.sampling import ObjectSampling, Sampling
+
+from .conftest import GOLDEN
+
+
+def load(name):
+    return dict(numpy.load(os.path.join(GOLDEN, name), allow_pickle=False))
+
+
+def test_groupings_bit_exact_with_reference():
+    g = json.load(open(os.path.join(GOLDEN, 'groupings.json')))
+    assert [a.tolist() for a in G.create_sparse_groupings(32, 8, 'seed1')] == g['sparse_32_8']
+    assert [a.tolist() for a in G.create_sparse_groupings(33, 8, 'seed1')] == g['sparse_33_8']
+    assert [a.tolist() for a in G.create_sparse_groupings((6, 7), 10, 'abc', i=3)] == g['sparse_6x7_10_i3']
+    assert [int(v) for v in G.shuffled(list(range(5)), seed='abc', i=2)] == g['shuffle_5_i2']
+    assert G.mask_fraction_of_groups(17, 0.1).tolist() == g['mask_17_0.1']
+    assert G.mask_fraction_of_groups(3, 0.5).tolist() == g['mask_3_0.5']
+    scan = numpy.stack(numpy.meshgrid(numpy.linspace(0., 20., 8), numpy.linspace(0., 20., 8),
+                                      indexing='ij'), axis=-1).reshape(-1, 2)
+    assert [a.tolist() for a in G.create_compact_groupings(scan, 16, 'seed1')] == g['compact_64_16']
+
+
+def test_group_manager_iteration_semantics():
+    gm = G.GroupManager((5, 6), 7, seed='s')
+    first = gm.iter(None, 0)
+    assert sum(g.shape[1] for g in first) == 30 and len(first) == len(gm) == 5
+    again = gm.iter(None, 2, shuffle_groups=False)      # same groups, shuffled order
+    assert sorted(map(lambda a: tuple(a.ravel()), again)) == sorted(map(lambda a: tuple(a.ravel()), first))
+    fresh = gm.iter(None, 2, shuffle_groups=True)       # regenerated with entropy groupings_2
+    assert [a.tolist() for a in fresh] == [a.tolist() for a in G.create_sparse_groupings((5, 6), 7, 's', 2)]
+    flat = gm.flat(fresh[0])
+    assert flat.dtype == numpy.int64 and flat.tolist() == (fresh[0][0] * 6 + fresh[0][1]).tolist()
+
+
+def test_object_sampling_indices_bit_exact():
+    g = load('cutouts.npz')
+    osamp = ObjectSampling((60, 70), g['sampling'], g['corner'])
+    shape = tuple(g['shape'])
+    assert_array_equal(osamp.pos_to_object_idx(g['pos'], shape), g['idx'])
+    assert_array_equal(osamp.cutout_starts(g['pos'], shape), g['starts'])
+    assert_array_equal(osamp.get_subpx_shifts(g['pos'], shape), g['subpx'])
+
+
+def test_propagators_match_reference():
+    g = load('numerics.npz')
+    samp = Sampling((32, 32), sampling=g['psamp'])
+    ky, kx = samp.recip_grid(dtype=numpy.float32)
+    props = optics.make_propagators(ky, kx, g['psamp'], float(g['wavelength']), g['thick'])
+    assert_array_equal(props, g['props'])     # same float32 ops, same values
+    probe = optics.make_focused_probe(ky, kx, float(g['wavelength']), 25., defocus=200.)
+    assert numpy.linalg.norm(probe - g['probe']) / numpy.linalg.norm(g['probe']) < 1e-6
+    modes = optics.make_hermite_modes(probe, 4, 0.7, [0.5, 1 / 3, 1 / 6])
+    assert numpy.linalg.norm(modes - g['modes']) / numpy.linalg.norm(g['modes']) < 1e-5
+    assert optics.electron_wavelength(200e3) == pytest.approx(0.02507934741, rel=1e-10)
+
+
+def test_plan_hook_resolution():
+    assert P.solver({'type': 'lsqml', 'beta_object': 0.5})[1].beta_object == 0.5
+    assert P.solver('epie')[0] == 'epie'
+    kind, props = P.noise_model({'type': 'anscombe'})
+    assert kind == 'anscombe' and props.offset == 0.375
+    assert P.position_solver({'type': 'momentum', 'step_size': 1e-3}) [1].momentum == 0.9
+
+    class RefHook:   # the shape of phaser's Hook objects (phaser/hooks/hook.py:15-30)
+        ref = 'phaser.engines.conventional.solvers:LSQMLSolver'
+        type = 'lsqml'
+        props = P.LSQMLSolverPlan(gamma=1e-3)
+    assert P.solver(RefHook())[1].gamma == 1e-3
+    with pytest.raises(NotImplementedError):
+        P.solver('something_else')
+
+
+def test_flags_and_schedules():
+    class S:
+        class iter:
+            engine_iter = 6
+    args = {'state': S, 'niter': 10}
+    assert P.process_flag(True)(args) and not P.process_flag(False)(args)
+    assert P.process_flag({'after': 5})(args)
+    assert not P.process_flag(P.Flag(after=5, every=2))(args)
+    assert not P.process_flag(P.Flag(before=6))(args)
+    assert P.process_schedule(0.25)(args) == 0.25
