@@ -225,8 +225,13 @@ def run_b200(args, world, rank, local):
     lib = _lib.load()
 
     # CPU baseline first (rank 0, N == 1), before the device is busy
-    ds = lsqml_multislice_config(seed=rank)
+    ds = lsqml_multislice_config(seed=rank, scan=args.scan)
     pats = simulate_patterns(ds, seed=rank, device=dev)
+    config = dict(CONFIG)
+    if args.scan != 64 or args.batch != 256:   # reduced case (profiling); not the benchmark line
+        config.update(workload=f"reduced multislice LSQ-ML (scan {args.scan}x{args.scan}, batch {args.batch})",
+                      positions=args.scan * args.scan, batch=args.batch,
+                      object=[int(v) for v in ds.obj_sampling.shape])
     pats_host = pats.cpu().pin_memory()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -247,7 +252,7 @@ def run_b200(args, world, rank, local):
         props = PL.ConventionalEnginePlan(
             noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
             position_solver={'type': 'momentum', 'step_size': 1e-3, 'max_step_size': 0.2, 'momentum': 0.9},
-            niter=10 ** 6, grouping=256, update_positions=True)
+            niter=10 ** 6, grouping=args.batch, update_positions=True)
         e = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
                                 'seed': 'bench', 'recons_name': 'bench'}, props, patterns_on_device=pats)
         e.presolve()
@@ -301,7 +306,7 @@ def run_b200(args, world, rank, local):
     e2e_ms = []
     barrier()
     torch.cuda.synchronize()
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         it += 1
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -311,7 +316,7 @@ def run_b200(args, world, rank, local):
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     barrier()
-    e2e_t = float(numpy.mean(e2e_ms))
+    e2e_t = float(numpy.mean(e2e_ms)) if e2e_ms else float('nan')
     if world > 1:
         tt = torch.tensor([e2e_t], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -320,7 +325,7 @@ def run_b200(args, world, rank, local):
 
     # ---------------- roofline of the fused kernel
     peak, peak_kind = measured_peaks()
-    B = 256
+    B = args.batch
     bytes_launch = algorithmic_bytes_per_pos_slice(N, M, S) * B * S
     avg_ms = float(numpy.mean(fused)) if fused else float('nan')
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
@@ -334,7 +339,7 @@ def run_b200(args, world, rank, local):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-                "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+                "config": dict(config, parallelism=f"replicas x{world}"),
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pats_host.numel() * 4),
                         "d2h_bytes_per_step": 32},
@@ -351,6 +356,9 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--scan', type=int, default=64, help='scan side (64 = the benchmark configuration)')
+    ap.add_argument('--batch', type=int, default=256, help='mini-batch size (256 = the benchmark configuration)')
     args = ap.parse_args()
     world, rank, local = setup_dist()
     if args.impl == 'reference':

@@ -141,7 +141,34 @@ __device__ __forceinline__ void tilt_tables(const GroupArgs &a, int64_t pos, int
     }
 }
 
+// Per-thread view of one position's cutout in R layout: row base offsets and a
+// validity bit per register slot (identical for every slice).
 template <int N>
+struct CutView {
+    int64_t base[FFTCfg<N>::U];   // (y0 + row(u)) * W + x0 + jl
+    uint32_t valid;               // bit u*E + q: pixel (row(u), col(q)) inside the object
+    __device__ __forceinline__ void init(const CutoutIndex &ci, int64_t H, int64_t W) {
+        using I = Idx<N>;
+        valid = 0u;
+#pragma unroll
+        for (int u = 0; u < I::U; ++u) {
+            const int64_t y = ci.y0 + I::row(u);
+            base[u] = y * W + ci.x0 + (threadIdx.x & 7);
+            const bool rowok = y >= 0 && y < H;
+#pragma unroll
+            for (int q = 0; q < I::E; ++q) {
+                const int64_t x = ci.x0 + I::col(q);
+                if (rowok && x >= 0 && x < W) valid |= 1u << (u * I::E + q);
+            }
+        }
+    }
+    __device__ __forceinline__ float2 at(const float2 *Os, int u, int q) const {
+        return (valid >> (u * FFTCfg<N>::E + q)) & 1u ? __ldg(Os + base[u] + FFTCfg<N>::NT * q)
+                                                      : make_float2(1.f, 0.f);
+    }
+};
+
+template <int N, int MODE>
 __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     using I = Idx<N>;
     constexpr int U = I::U, E = I::E, NN = N * N, SLOTS = U * E;
@@ -153,15 +180,15 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
-    float2 *twid = xb + NN;
+    float2 *twid = xb + Lay<N>::BUF;
     float2 *hy = twid + N, *hx = hy + N;
     float2 *ry = hx + N, *rx = ry + N;
     double *dred = reinterpret_cast<double *>(rx + N);
     float *fred = reinterpret_cast<float *>(dred + 64);   // [0..31] block scratch, [32] cluster slot
 
-    const int mode = a.mode;
-    const bool presolve = mode >= MODE_PRE_LSQML;
-    const bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
+    constexpr int mode = MODE;
+    constexpr bool presolve = mode >= MODE_PRE_LSQML;
+    constexpr bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
     const bool upd_obj = !presolve && (a.flags & PHB_FLAG_UPDATE_OBJECT);
     const bool upd_probe = !presolve && (a.flags & PHB_FLAG_UPDATE_PROBE);
     const bool upd_pos = !presolve && (a.flags & PHB_FLAG_UPDATE_POSITION);
@@ -173,6 +200,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 
     const int64_t pos = a.group[b];
     const CutoutIndex ci = cutout_index(a.scan, pos, a.cy, a.cx, a.sy, a.sx, N, N);
+    CutView<N> cv;
+    cv.init(ci, a.H, a.W);
 
     fft_init_twiddles<N>(twid);
     for (int k = tid; k < N; k += blockDim.x) {
@@ -263,7 +292,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int q = 0; q < E; ++q) v[u][q] = cmul(v[u][q], obj_px<N>(Os, ci, a.H, a.W, I::row(u), I::col(q)));
+            for (int q = 0; q < E; ++q) v[u][q] = cmul(v[u][q], cv.at(Os, u, q));
         if (last && mode == MODE_PRE_GRAD) {
             double t[2] = {0.0, 0.0};
 #pragma unroll
@@ -391,7 +420,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int q = 0; q < E; ++q) {
                     const int f = I::flat(u, q);
                     const float2 c = v[u][q];
-                    const float2 o = obj_px<N>(Os, ci, a.H, a.W, I::row(u), I::col(q));
+                    const float2 o = cv.at(Os, u, q);
                     const float c2 = cabs2(c);
                     if (upd_obj) {
                         const float2 p = ps[f];
@@ -446,7 +475,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int q = 0; q < E; ++q) {
-                    const float2 o = obj_px<N>(Os, ci, a.H, a.W, I::row(u), I::col(q));
+                    const float2 o = cv.at(Os, u, q);
                     omax = fmaxf(omax, cabs2(o));
                     if (upd_obj) xf[I::flat(u, q)] = cabs2(ps[I::flat(u, q)]);
                 }
@@ -491,7 +520,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int q = 0; q < E; ++q) {
                     const float2 c = v[u][q];
                     if (s == 0 && upd_pos) ps[I::flat(u, q)] = c;
-                    const float2 o = obj_px<N>(Os, ci, a.H, a.W, I::row(u), I::col(q));
+                    const float2 o = cv.at(Os, u, q);
                     v[u][q] = cscale(cmulc(c, o), inv);
                 }
         }
@@ -547,7 +576,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int q = 0; q < E; ++q) {
-                    const float2 o = obj_px<N>(a.object, ci, a.H, a.W, I::row(u), I::col(q));
+                    const float2 o = cv.at(a.object, u, q);
                     const float2 c = ps0[I::flat(u, q)];
                     const float2 pr = cmul(v[u][q], o);
                     t[0] += (double)(c.x * pr.x + c.y * pr.y);
@@ -716,7 +745,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
     constexpr int U = I::U, E = I::E, NN = N * N;
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
-    float2 *twid = xb + NN;
+    float2 *twid = xb + Lay<N>::BUF;
     float *fred = reinterpret_cast<float *>(twid + N);
     fft_init_twiddles<N>(twid);
     __syncthreads();
@@ -925,11 +954,11 @@ __global__ void k_check_finite(const float2 *v, int64_t n, int32_t *status, int3
 // ---------------------------------------------------------------- host glue
 template <int N>
 static size_t group_smem_bytes() {
-    return (size_t)N * N * sizeof(float2) + 5 * N * sizeof(float2) + 64 * sizeof(double) + 64 * sizeof(float);
+    return (size_t)Lay<N>::BUF * sizeof(float2) + 5 * N * sizeof(float2) + 64 * sizeof(double) + 64 * sizeof(float);
 }
 template <int N>
 static size_t fft_smem_bytes() {
-    return (size_t)N * N * sizeof(float2) + N * sizeof(float2) + 64 * sizeof(float);
+    return (size_t)Lay<N>::BUF * sizeof(float2) + N * sizeof(float2) + 64 * sizeof(float);
 }
 
 template <int N>
@@ -937,9 +966,7 @@ static int configure_kernels() {
     static int done = -1;
     if (done >= 0) return done;
     int rc = PHB_OK;
-    if (cudaFuncSetAttribute(k_group<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem_bytes<N>()) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_probe_apply<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_probe_apply<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)fft_smem_bytes<N>()) != cudaSuccess)
         rc = record_cuda(cudaGetLastError());
     done = rc;
@@ -1001,8 +1028,15 @@ static GroupArgs make_args(const phb_engine *e, const Workspace &w, int mode, in
     return a;
 }
 
-template <int N>
-static int launch_group(const GroupArgs &a, cudaStream_t st) {
+template <int N, int MODE>
+static int launch_group_mode(const GroupArgs &a, cudaStream_t st) {
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(k_group<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)group_smem_bytes<N>()) != cudaSuccess)
+            return record_cuda(cudaGetLastError());
+        configured = true;
+    }
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)(a.B * a.M), 1, 1);
     cfg.blockDim = dim3(FFT_THREADS, 1, 1);
@@ -1015,9 +1049,23 @@ static int launch_group(const GroupArgs &a, cudaStream_t st) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const int rc = record_cuda(cudaLaunchKernelEx(&cfg, k_group<N>, a));
+    const int rc = record_cuda(cudaLaunchKernelEx(&cfg, k_group<N, MODE>, a));
     if (rc == PHB_OK) count_launch();
     return rc;
+}
+
+template <int N>
+static int launch_group(const GroupArgs &a, cudaStream_t st) {
+    switch (a.mode) {
+        case MODE_LSQML: return launch_group_mode<N, MODE_LSQML>(a, st);
+        case MODE_EPIE: return launch_group_mode<N, MODE_EPIE>(a, st);
+        case MODE_GRAD: return launch_group_mode<N, MODE_GRAD>(a, st);
+        case MODE_PRE_LSQML: return launch_group_mode<N, MODE_PRE_LSQML>(a, st);
+        case MODE_PRE_EPIE: return launch_group_mode<N, MODE_PRE_EPIE>(a, st);
+        case MODE_PRE_GRAD: return launch_group_mode<N, MODE_PRE_GRAD>(a, st);
+        case MODE_SIM: return launch_group_mode<N, MODE_SIM>(a, st);
+        default: return PHB_ERR_INVALID_ARG;
+    }
 }
 
 template <int N>

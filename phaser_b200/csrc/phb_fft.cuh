@@ -18,8 +18,9 @@
 //   K layout: v[u][p*NT + k2]  = X[ky = (jl*P + p) + E*k2][kx = rsel + 64u]
 // The transforms are unnormalised DFTs with exp(-2 pi i nk/N) forward.
 //
-// Shared-memory addresses are XOR-swizzled so that every 8-byte access of a
-// half-warp (two lines x 8 threads) hits 16 distinct 8-byte bank pairs.
+// Shared-memory addresses are padded / XOR-swizzled so that every 8-byte
+// access of a half-warp (two lines x 8 threads) hits 16 distinct 8-byte bank
+// pairs.  The exchange buffer holds Lay<N>::BUF complex values.
 #pragma once
 
 #include "phb_common.cuh"
@@ -112,20 +113,27 @@ __device__ __forceinline__ void dftL(float2 *x) {
 }
 
 // --------------------------------------------------------------- addressing
+// Every shared-memory access below is (per-thread base) + (compile-time
+// offset), so the compiler keeps a handful of base registers instead of one
+// address per element.
+//
+// Line exchange (the NT threads of one row / column): line L starts at L*LS
+// with LS = N + 8 complex, so the two lines a half-warp touches sit in
+// opposite 64-byte halves of the bank space; inside a line, element
+// (thread jj, k1) lives at k1*NT + (jj ^ k1/P).
+//
+// Transpose tile: (r, c) at r*N + (c ^ g(r)); for every access pattern used
+// here g(r) depends only on per-thread bits, so the XOR folds into the base.
 template <int N>
 struct Lay {
     using C = FFTCfg<N>;
     static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
-    // exchange among the NT threads of one line (row or column) L
-    static __device__ __forceinline__ int line(int L, int jj, int k1) {
-        return L * N + (((k1 ^ (L & 1)) * NT) + (jj ^ (k1 / P)));
-    }
+    static constexpr int LS = N + 8;                    // padded line stride
+    static constexpr int BUF = N * LS;                  // complex elements of the exchange buffer
     static __device__ __forceinline__ int g(int r) {
         if constexpr (N == 128) return (2 * r + (r & 1)) & 15;
         else return ((r & 1) << 3) | (r & 6);
     }
-    // transpose tile
-    static __device__ __forceinline__ int tile(int r, int c) { return r * N + (c ^ g(r)); }
 };
 
 // twiddle table: twid[k1 * NT + jj] = exp(-2 pi i jj k1 / N), N entries
@@ -145,26 +153,26 @@ template <int N>
 __device__ __forceinline__ void line_pass_fwd(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
                                               const float2 *twid) {
     using Ly = Lay<N>;
-    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
+    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U, LS = Ly::LS;
     const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+    const float2 *tw = twid + jl;
+    float2 *lb = xb + rsel * LS;
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         dftL<E, false>(v[u]);
 #pragma unroll
-        for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmul(v[u][k1], twid[k1 * NT + jl]);
-        const int L = rsel + 64 * u;
+        for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmul(v[u][k1], tw[k1 * NT]);
 #pragma unroll
-        for (int k1 = 0; k1 < E; ++k1) xb[Ly::line(L, jl, k1)] = v[u][k1];
+        for (int k1 = 0; k1 < E; ++k1) lb[64 * u * LS + k1 * NT + (jl ^ (k1 / P))] = v[u][k1];
     }
     __syncthreads();
+    const float2 *rb = xb + rsel * LS + jl * P * NT;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const int L = rsel + 64 * u;
+    for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int p = 0; p < P; ++p)
 #pragma unroll
-            for (int jj = 0; jj < NT; ++jj) v[u][p * NT + jj] = xb[Ly::line(L, jj, jl * P + p)];
-    }
+            for (int jj = 0; jj < NT; ++jj) v[u][p * NT + jj] = rb[64 * u * LS + p * NT + (jj ^ jl)];
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -176,74 +184,101 @@ template <int N>
 __device__ __forceinline__ void line_pass_inv(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
                                               const float2 *twid) {
     using Ly = Lay<N>;
-    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
+    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U, LS = Ly::LS;
     const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+    float2 *wb = xb + rsel * LS + jl * P * NT;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const int L = rsel + 64 * u;
+    for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             dftL<NT, true>(&v[u][p * NT]);
 #pragma unroll
-            for (int jj = 0; jj < NT; ++jj) xb[Ly::line(L, jj, jl * P + p)] = v[u][p * NT + jj];
+            for (int jj = 0; jj < NT; ++jj) wb[64 * u * LS + p * NT + (jj ^ jl)] = v[u][p * NT + jj];
         }
-    }
     __syncthreads();
+    const float2 *lb = xb + rsel * LS;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int k1 = 0; k1 < E; ++k1) v[u][k1] = lb[64 * u * LS + k1 * NT + (jl ^ (k1 / P))];
+    __syncthreads();
+    const float2 *tw = twid + jl;
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int L = rsel + 64 * u;
 #pragma unroll
-        for (int k1 = 0; k1 < E; ++k1) v[u][k1] = xb[Ly::line(L, jl, k1)];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-#pragma unroll
-        for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmulc(v[u][k1], twid[k1 * NT + jl]);
+        for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmulc(v[u][k1], tw[k1 * NT]);
         dftL<E, true>(v[u]);
     }
 }
 
-// row-pass output (K form of rows) -> column-pass input (R form of columns)
-template <int N>
-__device__ __forceinline__ void transpose_rk(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
+// row-pass output (K form of rows) -> column-pass input (R form of columns), and back.
+// Row r = rsel + 64u holds kx = (jl*P + p) + E*k2; column c = rsel + 64u holds rows jl + NT*q.
+// tile(r, c) = r*N + (c ^ g(r)); g(rsel + 64u) == g(rsel) and g(jl + NT*q) == g(jl).
+template <int N, bool TO_COLUMNS>
+__device__ __forceinline__ void transpose(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
     using Ly = Lay<N>;
     constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
     const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
+    // row side: element (u, p, k2) at rsel*N + 64u*N + (((jl*P + p) + E*k2) ^ gr)
+    const int gr = Ly::g(rsel);
+    // column side: element (u, q) at jl*N + NT*q*N + ((rsel + 64u) ^ gc)
+    const int gc = Ly::g(jl);
+    float2 *rowb = xb + rsel * N;
+    float2 *colb = xb + jl * N + (rsel ^ gc);           // gc < 64, so (rsel + 64u) ^ gc = (rsel ^ gc) + 64u
+    if constexpr (TO_COLUMNS) {
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+        for (int u = 0; u < U; ++u)
 #pragma unroll
-        for (int p = 0; p < P; ++p)
+            for (int p = 0; p < P; ++p) {
+                if constexpr (N == 128) {   // gr < E: the XOR stays inside the low 4 bits
+                    float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ gr);
 #pragma unroll
-            for (int k2 = 0; k2 < NT; ++k2)
-                xb[Ly::tile(rsel + 64 * u, (jl * P + p) + E * k2)] = v[u][p * NT + k2];
-    __syncthreads();
+                    for (int k2 = 0; k2 < NT; ++k2) b[E * k2] = v[u][p * NT + k2];
+                } else {                    // E == 8: bit 3 of gr flips bit 0 of k2
+                    const int hb = gr >> 3;
+                    float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ (gr & 7));
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+                    for (int k2 = 0; k2 < NT; ++k2) b[E * (k2 ^ hb)] = v[u][p * NT + k2];
+                }
+            }
+        __syncthreads();
 #pragma unroll
-        for (int q = 0; q < E; ++q) v[u][q] = xb[Ly::tile(jl + NT * q, rsel + 64 * u)];
-    __syncthreads();
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < E; ++q) v[u][q] = colb[NT * q * N + 64 * u];
+        __syncthreads();
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < E; ++q) colb[NT * q * N + 64 * u] = v[u][q];
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                if constexpr (N == 128) {
+                    const float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ gr);
+#pragma unroll
+                    for (int k2 = 0; k2 < NT; ++k2) v[u][p * NT + k2] = b[E * k2];
+                } else {
+                    const int hb = gr >> 3;
+                    const float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ (gr & 7));
+#pragma unroll
+                    for (int k2 = 0; k2 < NT; ++k2) v[u][p * NT + k2] = b[E * (k2 ^ hb)];
+                }
+            }
+        __syncthreads();
+    }
 }
 
-// column-pass output (R form of columns) -> row-pass input (K form of rows)
+template <int N>
+__device__ __forceinline__ void transpose_rk(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
+    transpose<N, true>(v, xb);
+}
 template <int N>
 __device__ __forceinline__ void transpose_kr(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
-    using Ly = Lay<N>;
-    constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
-    const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-        for (int q = 0; q < E; ++q) xb[Ly::tile(jl + NT * q, rsel + 64 * u)] = v[u][q];
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-        for (int p = 0; p < P; ++p)
-#pragma unroll
-            for (int k2 = 0; k2 < NT; ++k2)
-                v[u][p * NT + k2] = xb[Ly::tile(rsel + 64 * u, (jl * P + p) + E * k2)];
-    __syncthreads();
+    transpose<N, false>(v, xb);
 }
 
 // Forward 2D DFT: R layout in, K layout out.

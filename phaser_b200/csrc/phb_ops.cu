@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
     constexpr int U = I::U, E = I::E;
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
-    float2 *twid = xb + N * N;
+    float2 *twid = xb + Lay<N>::BUF;
     fft_init_twiddles<N>(twid);
     const float2 *src = in + (size_t)blockIdx.x * N * N;
     float2 *dst = out + (size_t)blockIdx.x * N * N;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
 
 template <int N>
 static int launch_fft2(const float2 *in, float2 *out, int64_t batch, int inverse, cudaStream_t st) {
-    const size_t smem = (size_t)N * N * sizeof(float2) + N * sizeof(float2);
+    const size_t smem = (size_t)Lay<N>::BUF * sizeof(float2) + N * sizeof(float2);
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(k_fft2_centred<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
     constexpr int U = I::U, E = I::E;
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
-    float2 *twid = xb + N * N;
+    float2 *twid = xb + Lay<N>::BUF;
     fft_init_twiddles<N>(twid);
     float2 *t = a + (size_t)blockIdx.x * N * N;
     float2 v[U][E];
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
 
 template <int N>
 static int launch_fourier_mask(float2 *a, const float *mask, int64_t batch, cudaStream_t st) {
-    const size_t smem = (size_t)N * N * sizeof(float2) + N * sizeof(float2);
+    const size_t smem = (size_t)Lay<N>::BUF * sizeof(float2) + N * sizeof(float2);
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(k_fourier_mask<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

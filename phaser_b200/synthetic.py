@@ -99,8 +99,8 @@ def make_dataset(*, N: int, M: int, S: int, scan_shape: t.Tuple[int, int], step_
 
 
 # the multislice LSQ-ML benchmark configuration (8 x 2 nm slices, 128^2 probe, 4 modes, 64^2 scan)
-def lsqml_multislice_config(seed: int = 0) -> Dataset:
-    return make_dataset(N=128, M=4, S=8, scan_shape=(64, 64), step_px=6.0, sampling=0.2, kv=300e3,
+def lsqml_multislice_config(seed: int = 0, scan: int = 64) -> Dataset:
+    return make_dataset(N=128, M=4, S=8, scan_shape=(scan, scan), step_px=6.0, sampling=0.2, kv=300e3,
                         conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
                         peak_rad=0.2, counts=1e6, mode_powers=(0.70, 0.15, 0.10, 0.05), seed=seed)
 

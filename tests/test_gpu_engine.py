@@ -148,7 +148,8 @@ def test_run_engine_matches_oracle(solver):
     c = make_case(seed=41, N=64, M=2, S=2, scan_shape=(5, 5))
     props = PL.ConventionalEnginePlan(
         noise_model={'type': 'amplitude', 'eps': 1e-2},
-        solver={'type': solver, 'beta_object': 0.9, 'beta_probe': 0.8, 'gamma': 1e-3},
+        solver=({'type': 'lsqml', 'beta_object': 0.9, 'beta_probe': 0.8, 'gamma': 1e-3} if solver == 'lsqml'
+                else {'type': 'epie', 'beta_object': 0.9, 'beta_probe': 0.8}),
         position_solver={'type': 'momentum', 'step_size': 1e-2, 'max_step_size': 0.2, 'momentum': 0.9},
         niter=3, grouping=10, update_positions=True, calc_error_fraction=0.5)
     state = run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
