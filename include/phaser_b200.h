@@ -114,6 +114,8 @@ int phb_fourier_mask_c64(void *arr, int64_t batch, int64_t N, const float *mask,
 #define PHB_FLAG_UPDATE_POSITION 4
 #define PHB_FLAG_CALC_ERROR      8
 
+#define PHB_STATUS_INTERNAL (1 << 30)   /* flag bit in phb_step.status: kernel aborted its program */
+
 typedef struct phb_engine {
     /* sizes */
     int32_t N;            /* probe / detector side: 64 or 128 */
@@ -157,7 +159,8 @@ typedef struct phb_step {
     void  *grad_object;   /* gradient solver: (S, H, W) complex64 accumulator, NULL otherwise */
     void  *grad_probe;    /* gradient solver: (M, N, N) complex64 accumulator */
     float *grad_pos;      /* gradient solver: (n_pos, 2) float32 dL/d(y, x) */
-    int32_t *status;      /* device int, sticky: first group index that produced NaN/inf (or -1) */
+    int32_t *status;      /* device int, sticky, -1 = fine: the first group index that produced NaN/inf,
+                             or PHB_STATUS_INTERNAL | group index if a kernel aborted (internal error) */
     int32_t group_index;  /* index of this group within the iteration (for `status`) */
     const float *group_patterns; /* optional (B, N, N): this group's patterns in group order, read
                                     instead of patterns[group[b]] (host-streamed data) */

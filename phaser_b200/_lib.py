@@ -30,6 +30,7 @@ PHB_FLAG_UPDATE_OBJECT = 1
 PHB_FLAG_UPDATE_PROBE = 2
 PHB_FLAG_UPDATE_POSITION = 4
 PHB_FLAG_CALC_ERROR = 8
+PHB_STATUS_INTERNAL = 1 << 30
 
 c_void_p = ctypes.c_void_p
 c_i32 = ctypes.c_int32

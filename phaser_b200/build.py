@@ -44,16 +44,15 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     out_dir.mkdir(exist_ok=True)
     flags = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC',
              '-Xptxas', '-v' if verbose else '-O3', *ARCH, f'-I{ROOT / "include"}']
-    objs = []
-    for src in SOURCES:
-        obj = out_dir / (Path(src).stem + '.o')
-        cmd = [nvcc(), '-c', str(CSRC / src), '-o', str(obj), *flags]
-        res = subprocess.run(cmd, capture_output=True, text=True)
-        if res.returncode != 0:
-            raise RuntimeError(f"nvcc failed for {src}:\n{res.stderr}")
+    objs = [str(out_dir / (Path(src).stem + '.o')) for src in SOURCES]
+    procs = [subprocess.Popen([nvcc(), '-c', str(CSRC / src), '-o', obj, *flags], stdout=subprocess.PIPE,
+                              stderr=subprocess.PIPE, text=True) for src, obj in zip(SOURCES, objs)]
+    for src, proc in zip(SOURCES, procs):   # the translation units compile in parallel
+        _, err = proc.communicate()
+        if proc.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{err}")
         if verbose:
-            sys.stderr.write(res.stderr)
-        objs.append(str(obj))
+            sys.stderr.write(err)
     tmp = LIB.with_suffix('.so.tmp')
     cmd = [nvcc(), '-shared', '-o', str(tmp), *objs, *ARCH, '-lcudart']
     res = subprocess.run(cmd, capture_output=True, text=True)

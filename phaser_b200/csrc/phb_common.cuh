@@ -110,6 +110,13 @@ __device__ __forceinline__ float block_max_float(float v, float *smem) {
     return r;
 }
 
+// Warp-level float64 sum; lane 0 adds it to *dst.  Call from uniform code (all 32 lanes).
+__device__ __forceinline__ void warp_atomic_sum(double *dst, double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(dst, v);
+}
+
 // Vector fp32 atomics (sm_90+): one red per complex value.
 __device__ __forceinline__ void atomic_add_c(float2 *addr, float2 v) {
     atomicAdd(addr, v);

@@ -30,6 +30,22 @@ namespace cg = cooperative_groups;
 
 namespace phb {
 
+// Optional per-phase cycle accounting of the fused kernel (off unless the
+// library is built with -DPHB_PHASE_TIMING; then phb_debug_phase_cycles reads it).
+#ifdef PHB_PHASE_TIMING
+__device__ unsigned long long g_phase_cycles[16];
+#define PHB_T_BEGIN() long long phb_t0_ = clock64()
+#define PHB_T_MARK(k)                                                                               \
+    do {                                                                                            \
+        const long long phb_t1_ = clock64();                                                        \
+        if (threadIdx.x == 0) atomicAdd(&g_phase_cycles[(k)], (unsigned long long)(phb_t1_ - phb_t0_)); \
+        phb_t0_ = phb_t1_;                                                                          \
+    } while (0)
+#else
+#define PHB_T_BEGIN() (void)0
+#define PHB_T_MARK(k) (void)0
+#endif
+
 enum Mode : int {
     MODE_LSQML = 0,
     MODE_EPIE = 1,
@@ -48,8 +64,10 @@ struct Workspace {
     float2 *acc_probe;  // M*N*N (K order): sum_b FFT(dP) conj(H)
     float *gom;         // N*N : group_obj_mag
     float2 *probe_k;    // M*N*N (K order): DFT(probe) / N^2
-    float2 *prop_k;     // max(S-1,1)*N*N (K order)
+    float2 *prop1d;     // max(S-1,1) * 2N: per slice gap, propagator factors p(ky) then p(kx)
+    uint32_t *band;     // N*N/32 band-limit bits (propagator support)
     float *mask_k;      // N*N (K order)
+    int32_t *info;      // [0] pattern mask is all ones, [1] propagators separable, [2] max deviation (float bits)
     double *sums;       // float64 accumulators, see SumIdx
     double *coef;       // S + M step coefficients
     size_t bytes;
@@ -88,8 +106,10 @@ static Workspace carve(void *base, int N, int M, int S, int B, int64_t H, int64_
     w.acc_probe = (float2 *)take((size_t)M * NN * sizeof(float2));
     w.gom = (float *)take(NN * sizeof(float));
     w.probe_k = (float2 *)take((size_t)M * NN * sizeof(float2));
-    w.prop_k = (float2 *)take((size_t)(S > 1 ? S - 1 : 1) * NN * sizeof(float2));
+    w.prop1d = (float2 *)take((size_t)(S > 1 ? S - 1 : 1) * 2 * N * sizeof(float2));
+    w.band = (uint32_t *)take(NN / 32 * sizeof(uint32_t));
     w.mask_k = (float *)take(NN * sizeof(float));
+    w.info = (int32_t *)take(4 * sizeof(int32_t));
     w.sums = (double *)take((size_t)SumIdx(B, S, M).total * sizeof(double));
     w.coef = (double *)take((size_t)(S + M + 4) * sizeof(double));
     w.bytes = off;
@@ -106,7 +126,14 @@ struct GroupArgs {
     const float *scan, *tilt, *thick;
     const int64_t *group;
     const float *patterns, *mask_k;
-    const float2 *prop_k, *probe_k;
+    const float2 *prop1d, *probe_k;
+    const uint32_t *band;
+    const int32_t *info;   // device: [0] mask is all ones
+    int32_t *err_word;     // device: set to 1 if a kernel ran past its bounded program
+    int32_t *status;       // optional sticky status of the step (see phb_step.status)
+    int32_t group_index;
+    // float64 accumulator offsets (SumIdx for B_max), precomputed on the host
+    int64_t o_numO, o_denO, o_numP, o_denP, o_pnum, o_pden, o_pnorm, o_loss;
     const float *fy, *fx;
     float2 *psi, *acc_obj, *acc_probe;
     float *illum;
@@ -124,56 +151,66 @@ __device__ __forceinline__ float2 obj_px(const float2 *Os, const CutoutIndex &ci
     return (y >= 0 && y < H && x >= 0 && x < W) ? __ldg(Os + y * W + x) : make_float2(1.f, 0.f);
 }
 
-// tilt ramps of slice gap s: exp(2 pi i dz tan(t*1e-3) k) (simulation.py:193-222), separable in (ky, kx)
-template <int N>
-__device__ __forceinline__ void tilt_tables(const GroupArgs &a, int64_t pos, int s, float2 *ry, float2 *rx) {
-    const float dz = a.thick[s];
-    const float ty = tanf(a.tilt[2 * pos] * 1e-3f), tx = tanf(a.tilt[2 * pos + 1] * 1e-3f);
-    for (int k = threadIdx.x; k < 2 * N; k += blockDim.x) {
-        float sn, cs;
-        if (k < N) {
-            sincospif(2.0f * (dz * (ty * a.fy[k])), &sn, &cs);
-            ry[k] = make_float2(cs, sn);
-        } else {
-            sincospif(2.0f * (dz * (tx * a.fx[k - N])), &sn, &cs);
-            rx[k - N] = make_float2(cs, sn);
-        }
-    }
-}
-
 // Per-thread view of one position's cutout in R layout: row base offsets and a
 // validity bit per register slot (identical for every slice).
 template <int N>
 struct CutView {
-    int64_t base[FFTCfg<N>::U];   // (y0 + row(u)) * W + x0 + jl
-    uint32_t valid;               // bit u*E + q: pixel (row(u), col(q)) inside the object
+    int32_t base[FFTCfg<N>::U];   // (y0 + row(u)) * W + x0 + jl, inside one slice (H*W < 2^31)
+    uint64_t valid;               // bit u*E + q: pixel (row(u), col(q)) inside the object
+    static_assert(FFTCfg<N>::U * FFTCfg<N>::E <= 64, "per-thread slot bits must fit 64 bits");
     __device__ __forceinline__ void init(const CutoutIndex &ci, int64_t H, int64_t W) {
         using I = Idx<N>;
-        valid = 0u;
+        valid = 0ull;
 #pragma unroll
         for (int u = 0; u < I::U; ++u) {
             const int64_t y = ci.y0 + I::row(u);
-            base[u] = y * W + ci.x0 + (threadIdx.x & 7);
+            base[u] = (int32_t)(y * W + ci.x0 + (threadIdx.x & 7));
             const bool rowok = y >= 0 && y < H;
 #pragma unroll
             for (int q = 0; q < I::E; ++q) {
                 const int64_t x = ci.x0 + I::col(q);
-                if (rowok && x >= 0 && x < W) valid |= 1u << (u * I::E + q);
+                if (rowok && x >= 0 && x < W) valid |= 1ull << (u * I::E + q);
             }
         }
     }
+    __device__ __forceinline__ bool ok(int u, int q) const { return (valid >> (u * FFTCfg<N>::E + q)) & 1ull; }
+    // offset of pixel (row(u), col(q)) inside one object slice (valid only if ok(u, q))
+    __device__ __forceinline__ int32_t off(int u, int q) const { return base[u] + FFTCfg<N>::NT * q; }
     __device__ __forceinline__ float2 at(const float2 *Os, int u, int q) const {
-        return (valid >> (u * FFTCfg<N>::E + q)) & 1u ? __ldg(Os + base[u] + FFTCfg<N>::NT * q)
+        return (valid >> (u * FFTCfg<N>::E + q)) & 1ull ? __ldg(Os + base[u] + FFTCfg<N>::NT * q)
                                                       : make_float2(1.f, 0.f);
     }
 };
 
-template <int N, int MODE>
+// Phases of the fused mini-batch program.  Each is the elementwise work that
+// follows one transform (R = real-space layout after an inverse transform,
+// K = Fourier layout after a forward transform).  The kernel body contains
+// exactly one forward and one inverse 2D FFT, so the instruction footprint
+// stays small however many slices the program walks through.
+enum Phase : int {
+    PH_START = 0,   // R: incident wave of slice s: store, illuminate, transmit
+    PH_PROP = 1,    // K: propagate to slice s+1
+    PH_FAR = 2,     // K: detector plane, constraint / loss gradient
+    PH_BACK = 3,    // R: adjoint of slice s (object/probe update terms)
+    PH_BPROP = 4,   // K: adjoint propagation to slice s-1
+    PH_PROBE = 5,   // K: probe-update accumulation
+    PH_POS = 6,     // R: position-gradient dot products (direction `dir`)
+};
+
+// MC > 0: the number of probe modes (cluster size) is the compile-time constant MC,
+// so every cross-mode loop unrolls and its remote loads issue back to back;
+// MC == 0 handles any M at run time.
+template <int N, int MODE, int MC>
 __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     using I = Idx<N>;
     constexpr int U = I::U, E = I::E, NN = N * N, SLOTS = U * E;
+    constexpr int mode = MODE;
+    constexpr int MR = MC > 0 ? MC : 8;   // capacity of the remote-pointer arrays
+    constexpr bool presolve = mode >= MODE_PRE_LSQML;
+    constexpr bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
     cg::cluster_group cl = cg::this_cluster();
-    const int M = a.M, S = a.S;
+    const int M = MC > 0 ? MC : a.M;
+    const int S = a.S;
     const int m = (int)cl.block_rank();
     const int b = blockIdx.x / M;
     const int tid = threadIdx.x;
@@ -181,27 +218,41 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
     float2 *twid = xb + Lay<N>::BUF;
-    float2 *hy = twid + N, *hx = hy + N;
-    float2 *ry = hx + N, *rx = ry + N;
-    double *dred = reinterpret_cast<double *>(rx + N);
-    float *fred = reinterpret_cast<float *>(dred + 64);   // [0..31] block scratch, [32] cluster slot
+    float2 *hy = twid + N, *hx = hy + N;           // sub-pixel shift filter factors
+    float2 *py = hx + N, *px = py + N;             // propagator factors of the current slice gap
+    double *dred = reinterpret_cast<double *>(px + N);
+    float *fred = reinterpret_cast<float *>(dred + 64);              // [0..31] block scratch, [32] cluster slot
+    uint32_t *band = reinterpret_cast<uint32_t *>(fred + 64);        // N*N/32 band-limit bits
+    // per-thread cutout view and band bits live in shared memory between phases,
+    // leaving the registers to the wavefield while the transforms run
+    uint64_t *s_bits = reinterpret_cast<uint64_t *>(band + NN / 32);   // [valid | kband][FFT_THREADS]
+    int32_t *s_base = reinterpret_cast<int32_t *>(s_bits + 2 * FFT_THREADS);   // [U][FFT_THREADS]
 
-    constexpr int mode = MODE;
-    constexpr bool presolve = mode >= MODE_PRE_LSQML;
-    constexpr bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
     const bool upd_obj = !presolve && (a.flags & PHB_FLAG_UPDATE_OBJECT);
     const bool upd_probe = !presolve && (a.flags & PHB_FLAG_UPDATE_PROBE);
     const bool upd_pos = !presolve && (a.flags & PHB_FLAG_UPDATE_POSITION);
     const bool calc_err = !presolve && !grad && (a.flags & PHB_FLAG_CALC_ERROR) && a.errors;
     const bool do_illum = a.illum && (mode == MODE_LSQML || mode == MODE_PRE_LSQML);
     const bool tilted = a.tilt != nullptr;
-    const SumIdx SI(a.B_max, S, M);
+    const bool mask_ones = __ldg(a.info) != 0;
     double *sums = a.sums;
 
     const int64_t pos = a.group[b];
     const CutoutIndex ci = cutout_index(a.scan, pos, a.cy, a.cx, a.sy, a.sx, N, N);
-    CutView<N> cv;
-    cv.init(ci, a.H, a.W);
+    {
+        CutView<N> c0;
+        c0.init(ci, a.H, a.W);
+        s_bits[tid] = c0.valid;
+#pragma unroll
+        for (int u = 0; u < U; ++u) s_base[u * FFT_THREADS + tid] = c0.base[u];
+    }
+    auto load_cv = [&]() {
+        CutView<N> c;
+        c.valid = s_bits[tid];
+#pragma unroll
+        for (int u = 0; u < U; ++u) c.base[u] = s_base[u * FFT_THREADS + tid];
+        return c;
+    };
 
     fft_init_twiddles<N>(twid);
     for (int k = tid; k < N; k += blockDim.x) {
@@ -211,135 +262,191 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
         sincospif(-2.0f * (ci.sx * a.fx[k]), &sn, &cs);
         hx[k] = make_float2(cs, sn);
     }
+    for (int k = tid; k < NN / 32; k += blockDim.x) band[k] = a.band[k];
     __syncthreads();
 
     float2 *psi_b = a.psi + (size_t)(b * M + m) * S * NN;
     const int slot0 = (m * SLOTS) / M, slot1 = ((m + 1) * SLOTS) / M;
+    const float inv_n = 1.0f / (float)N, inv_nn = 1.0f / (float)NN;
 
-    // ---------------------------------------------------------- psi_0 = IFFT(FFT(P_m) H_b)
     float2 v[U][E];
-    {
-        const float2 *pk = a.probe_k + (size_t)m * NN;
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int e = 0; e < E; ++e)
-                v[u][e] = cmul(__ldg(pk + I::flat(u, e)), cmul(hy[I::ky(e)], hx[I::kx(u)]));
-        ifft2_k2r<N>(v, xb, twid);
-    }
-    if (upd_pos) {
-        double n0 = 0.0;
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int q = 0; q < E; ++q) n0 += (double)cabs2(v[u][q]);
-        block_sum_doubles<FFT_THREADS>(&n0, 1, dred);
-        if (tid == 0) atomicAdd(sums + SI.pnorm + b, n0);
-    }
-
-    // ---------------------------------------------------------- forward multislice
-    for (int s = 0; s < S; ++s) {
-        const float2 *Os = a.object + (size_t)s * a.H * a.W;
-        const bool last = (s == S - 1);
-        if (upd_obj) {
-            float2 *dst = psi_b + (size_t)s * NN;
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) dst[I::flat(u, q)] = v[u][q];
-        }
-        if (do_illum) {   // group_probe_mag[s] += scatter(sum_m |psi_s|^2)
-            float *xf = reinterpret_cast<float *>(xb);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) xf[I::flat(u, q)] = cabs2(v[u][q]);
-            cl.sync();
-            float *dst = a.illum + (size_t)s * a.H * a.W;
-            for (int sl = slot0; sl < slot1; ++sl) {
-                const int f = sl * FFT_THREADS + tid;
-                float acc = 0.f;
-                for (int r = 0; r < M; ++r) acc += cl.map_shared_rank(xf, r)[f];
-                int rr, cc;
-                flat_to_rc<N>(f, rr, cc);
-                const int64_t y = ci.y0 + rr, x = ci.x0 + cc;
-                if (y >= 0 && y < a.H && x >= 0 && x < a.W) atomicAdd(dst + y * a.W + x, acc);
-            }
-            cl.sync();
-        }
-        if (last && (mode == MODE_PRE_LSQML || mode == MODE_PRE_EPIE)) {
-            // rescale: sum(I_exp * mask) / sum |fft2(psi_last)|^2 (Parseval), psi before transmission
-            double t[2] = {0.0, 0.0};
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
-            if (m == 0) {
-                const float *pat = a.patterns + pos * NN;
-                for (int f = tid; f < NN; f += FFT_THREADS) {
-                    int ky, kx;
-                    flat_to_k<N>(f, ky, kx);
-                    t[1] += (double)(__ldg(pat + ky * N + kx) * __ldg(a.mask_k + f));
-                }
-            }
-            block_sum_doubles<FFT_THREADS>(t, 2, dred);
-            if (tid == 0) {
-                atomicAdd(a.pre_den + b, t[0]);
-                if (m == 0) atomicAdd(a.pre_num + b, t[1]);
-            }
-            return;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int q = 0; q < E; ++q) v[u][q] = cmul(v[u][q], cv.at(Os, u, q));
-        if (last && mode == MODE_PRE_GRAD) {
-            double t[2] = {0.0, 0.0};
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
-            if (m == 0) {
-                const float *pat = a.patterns + pos * NN;
-                for (int f = tid; f < NN; f += FFT_THREADS) t[1] += (double)__ldg(pat + f);
-            }
-            block_sum_doubles<FFT_THREADS>(t, 2, dred);
-            if (tid == 0) {
-                atomicAdd(a.pre_den + b, t[0]);
-                if (m == 0) atomicAdd(a.pre_num + b, t[1]);
-            }
-            return;
-        }
-        fft2_r2k<N>(v, xb, twid);
-        if (!last) {
+    // propagator of slice gap g (and this position's tilt ramp) into py/px
+    auto load_prop = [&](int g) {
+        const float2 *src = a.prop1d + (size_t)g * 2 * N;
+        for (int k = tid; k < 2 * N; k += blockDim.x) {
+            float2 p = src[k];
             if (tilted) {
-                tilt_tables<N>(a, pos, s, ry, rx);
-                __syncthreads();
+                const float dz = a.thick[g];
+                const float t = tanf(a.tilt[2 * pos + (k < N ? 0 : 1)] * 1e-3f);
+                const float f = k < N ? a.fy[k] : a.fx[k - N];
+                float sn, cs;
+                sincospif(2.0f * (dz * (t * f)), &sn, &cs);
+                p = cmul(p, make_float2(cs, sn));
             }
-            const float2 *pr = a.prop_k + (size_t)s * NN;
-            const float sc = 1.0f / (float)NN;
+            py[k] = p;   // py[0..N) then px[0..N): contiguous
+        }
+        __syncthreads();
+    };
+    // band-limit bits of this thread's K-layout elements (same for every slice gap)
+    {
+        uint64_t kb = 0ull;
+        static_assert(U * E <= 64, "per-thread slot bits must fit 64 bits");
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int f = I::ky(e) * N + I::kx(u);
+                if ((band[f >> 5] >> (f & 31)) & 1u) kb |= 1ull << (u * E + e);
+            }
+        s_bits[FFT_THREADS + tid] = kb;
+    }
+    // v (K layout) = DFT(P_m)/N^2 * H_b [* (-2 pi i k_dir)]
+    auto load_probe_spectrum = [&](int dir) {
+        const float2 *pk = a.probe_k + (size_t)m * NN;
+        const float twopi = 6.283185307179586f;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int ky = I::ky(e), kx = I::kx(u);
+                float2 g = cmul(__ldg(pk + I::flat(u, e)), cmul(hy[ky], hx[kx]));
+                if (dir >= 0) {
+                    const float w = twopi * (dir == 0 ? a.fy[ky] : a.fx[kx]);
+                    g = make_float2(w * g.y, -w * g.x);
+                }
+                v[u][e] = g;
+            }
+    };
+
+    load_probe_spectrum(-1);
+    int phase = PH_START, s = 0, dir = 0;
+    bool fwd = false;
+
+    // The program is 4 S + 2 transforms at most (forward, adjoint, probe, two
+    // position directions); the bound turns a logic error into a recorded error
+    // (info[3] and the step's status word) instead of a kernel that never ends.
+    const int max_steps = 4 * S + 8;
+    PHB_T_BEGIN();
+    for (int step = 0;; ++step) {
+        if (step >= max_steps) {
+            if (tid == 0) {
+                atomicExch(a.err_word, 1);
+                if (a.status) atomicCAS(a.status, -1, PHB_STATUS_INTERNAL | a.group_index);
+            }
+            return;
+        }
+        if (fwd) fft2_r2k<N>(v, xb, twid);
+        else ifft2_k2r<N>(v, xb, twid);
+        PHB_T_MARK(fwd ? 0 : 1);
+        const int timed_phase = phase;
+
+        if (phase == PH_START) {
+            // ------------------------------------------- incident wave of slice s (R layout)
+            const CutView<N> cv = load_cv();
+            const float2 *Os = a.object + (size_t)s * a.H * a.W;
+            if (s == 0 && upd_pos) {
+                float n0 = 0.f;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int q = 0; q < E; ++q) n0 += cabs2(v[u][q]);
+                warp_atomic_sum(sums + a.o_pnorm + b, (double)n0);
+            }
+            if (upd_obj) {
+                float2 *dst = psi_b + (size_t)s * NN;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int q = 0; q < E; ++q) dst[I::flat(u, q)] = v[u][q];
+            }
+            if (do_illum) {   // group_probe_mag[s] += scatter(|psi_s,m|^2): one red per pixel and mode
+                float *dst = a.illum + (size_t)s * a.H * a.W;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int q = 0; q < E; ++q)
+                        if (cv.ok(u, q)) atomicAdd(dst + cv.off(u, q), cabs2(v[u][q]));
+            }
+            const bool last = s == S - 1;
+            if constexpr (mode == MODE_PRE_LSQML || mode == MODE_PRE_EPIE) {
+                if (last) {   // rescale: sum(I_exp*mask) / sum|psi_last|^2 (Parseval), before transmission
+                    double t[2] = {0.0, 0.0};
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
+                    if (m == 0) {
+                        const float *pat = a.patterns + pos * NN;
+                        for (int f = tid; f < NN; f += FFT_THREADS) {
+                            int ky, kx;
+                            flat_to_k<N>(f, ky, kx);
+                            t[1] += (double)(__ldg(pat + ky * N + kx) * __ldg(a.mask_k + f));
+                        }
+                    }
+                    block_sum_doubles<FFT_THREADS>(t, 2, dred);
+                    if (tid == 0) {
+                        atomicAdd(a.pre_den + b, t[0]);
+                        if (m == 0) atomicAdd(a.pre_num + b, t[1]);
+                    }
+                    return;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int q = 0; q < E; ++q) v[u][q] = cmul(v[u][q], cv.at(Os, u, q));
+            if constexpr (mode == MODE_PRE_GRAD) {
+                if (last) {
+                    double t[2] = {0.0, 0.0};
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
+                    if (m == 0) {
+                        const float *pat = a.patterns + pos * NN;
+                        for (int f = tid; f < NN; f += FFT_THREADS) t[1] += (double)__ldg(pat + f);
+                    }
+                    block_sum_doubles<FFT_THREADS>(t, 2, dred);
+                    if (tid == 0) {
+                        atomicAdd(a.pre_den + b, t[0]);
+                        if (m == 0) atomicAdd(a.pre_num + b, t[1]);
+                    }
+                    return;
+                }
+            }
+            if (!last) load_prop(s);
+            fwd = true;
+            phase = last ? PH_FAR : PH_PROP;
+        } else if (phase == PH_PROP) {
+            // ------------------------------------------- propagate (K layout)
+            const uint64_t kband = s_bits[FFT_THREADS + tid];
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    float2 p = __ldg(pr + I::flat(u, e));
-                    if (tilted) p = cmul(p, cmul(ry[I::ky(e)], rx[I::kx(u)]));
-                    v[u][e] = cscale(cmul(v[u][e], p), sc);
+                    const int ky = I::ky(e), kx = I::kx(u);
+                    const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
+                    v[u][e] = cscale(cmul(v[u][e], p), inv_nn);
                 }
-            ifft2_k2r<N>(v, xb, twid);
-        } else {
-            // ------------------------------------------------ detector: Psi = fft2(exit), constraint
-            const float sc = 1.0f / (float)N;
+            fwd = false;
+            phase = PH_START;
+            ++s;
+        } else if (phase == PH_FAR) {
+            // ------------------------------------------- detector: Psi = fft2(exit), constraint
             float *xf = reinterpret_cast<float *>(xb);
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    v[u][e] = cscale(v[u][e], sc);
+                    v[u][e] = cscale(v[u][e], inv_n);
                     xf[I::flat(u, e)] = cabs2(v[u][e]);
                 }
             cl.sync();
-            if (mode == MODE_SIM) {
+            // the exchange buffer of every CTA of the cluster (distributed shared memory)
+            const float *rxf[MR];
+#pragma unroll
+            for (int r = 0; r < MR; ++r) rxf[r] = r < M ? cl.map_shared_rank(xf, r) : xf;
+            if constexpr (mode == MODE_SIM) {
                 if (m == 0) {
 #pragma unroll
                     for (int u = 0; u < U; ++u)
@@ -347,247 +454,237 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         for (int e = 0; e < E; ++e) {
                             const int f = I::flat(u, e);
                             float inten = 0.f;
-                            for (int r = 0; r < M; ++r) inten += cl.map_shared_rank(xf, r)[f];
+                            for (int r = 0; r < MR; ++r)
+                                if (r < M) inten += rxf[r][f];
                             a.sim_out[(size_t)b * NN + I::ky(e) * N + I::kx(u)] = inten;
                         }
                 }
                 cl.sync();
                 return;
-            }
-            const float *pat = a.group_patterns ? a.group_patterns + (size_t)b * NN : a.patterns + pos * NN;
-            double e2 = 0.0, loss = 0.0;
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const int f = I::flat(u, e);
-                    float inten = 0.f;
-                    for (int r = 0; r < M; ++r) inten += cl.map_shared_rank(xf, r)[f];
-                    const float pv = __ldg(pat + I::ky(e) * N + I::kx(u));
-                    const float mk = __ldg(a.mask_k + f);
-                    if (calc_err && m == 0) {
-                        const float d = inten - pv;
-                        if (d == d) e2 += (double)d * (double)d;
-                    }
-                    const float pm = np_max0(pv);
-                    float fac;
-                    if (!grad) {
-                        // amplitude / anscombe wave update (noise_models.py:47-64)
-                        fac = (sqrtf(pm + a.offset) / (sqrtf(inten + a.offset) + a.eps) - 1.0f) * mk;
-                    } else if (a.noise == PHB_NOISE_POISSON) {
-                        // d/dI of mask*(I + eps + p*(log(p+eps) - log(I+eps) - 1)) (noise_models.py:86-102)
-                        if (m == 0)
-                            loss += (double)(mk * (inten + a.eps +
-                                                   pm * (logf(pm + a.eps) - logf(inten + a.eps) - 1.0f)));
-                        fac = 2.0f * mk * (1.0f - pm / (inten + a.eps));
-                    } else {
-                        // d/dI of 2 mask (sqrt(p+c) - sqrt(I+c) - eps)^2 / var (noise_models.py:29-45)
-                        const float sI = sqrtf(inten + a.offset);
-                        const float dlt = sqrtf(pm + a.offset) - sI - a.eps;
-                        if (m == 0) loss += (double)(2.0f * mk * dlt * dlt / a.var);
-                        fac = 2.0f * (-2.0f * mk * dlt / (a.var * sI));
-                    }
-                    v[u][e] = cscale(v[u][e], fac);
-                }
-            cl.sync();
-            if (m == 0 && (calc_err || grad)) {
-                double t[2] = {e2, loss};
-                block_sum_doubles<FFT_THREADS>(t, 2, dred);
-                if (tid == 0) {
-                    if (calc_err) a.errors[pos] = (float)sqrt(t[0]);
-                    if (grad) sums[SI.loss + b] = t[1];
-                }
-            }
-            ifft2_k2r<N>(v, xb, twid);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) v[u][q] = cscale(v[u][q], sc);
-        }
-    }
-
-    // ---------------------------------------------------------- adjoint, slice by slice
-    for (int s = S - 1; s >= 0; --s) {
-        const float2 *Os = a.object + (size_t)s * a.H * a.W;
-        float2 *ps = psi_b + (size_t)s * NN;
-        if (!epie) {
-            // LSQ-ML: dO = chi conj(psi), dP = chi conj(O) (solvers.py:242-271); gradient: same adjoint
-            double t[4] = {0.0, 0.0, 0.0, 0.0};
-            float2 *xc = xb;
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const int f = I::flat(u, q);
-                    const float2 c = v[u][q];
-                    const float2 o = cv.at(Os, u, q);
-                    const float c2 = cabs2(c);
-                    if (upd_obj) {
-                        const float2 p = ps[f];
-                        xc[f] = cmulc(c, p);
-                        const float p2 = cabs2(p);
-                        t[0] += (double)(c2 * p2);
-                        t[1] += (double)(c2 * p2) * (double)p2;
-                    }
-                    if (s == 0) {
-                        if (lsqml && upd_probe) {
-                            const float o2 = cabs2(o);
-                            t[2] += (double)(c2 * o2);
-                            t[3] += (double)(c2 * o2) * (double)o2;
-                        }
-                        if (upd_pos) ps[f] = c;   // exit-wave update of slice 0 for the position step
-                    }
-                    v[u][q] = cmulc(c, o);
-                }
-            if (upd_obj) {
-                cl.sync();
-                float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
-                for (int sl = slot0; sl < slot1; ++sl) {
-                    const int f = sl * FFT_THREADS + tid;
-                    float2 acc = make_float2(0.f, 0.f);
-                    for (int r = 0; r < M; ++r) acc = cadd(acc, cl.map_shared_rank(xc, r)[f]);
-                    int rr, cc;
-                    flat_to_rc<N>(f, rr, cc);
-                    const int64_t y = ci.y0 + rr, x = ci.x0 + cc;
-                    if (y >= 0 && y < a.H && x >= 0 && x < a.W) atomic_add_c(dst + y * a.W + x, acc);
-                }
-                cl.sync();
-            }
-            if (lsqml && (upd_obj || (s == 0 && upd_probe))) {
-                block_sum_doubles<FFT_THREADS>(t, 4, dred);
-                if (tid == 0) {
-                    if (upd_obj) {
-                        atomicAdd(sums + SI.numO + (int64_t)b * S + s, t[0]);
-                        atomicAdd(sums + SI.denO + s, t[1]);
-                    }
-                    if (s == 0 && upd_probe) {
-                        atomicAdd(sums + SI.numP + (int64_t)b * M + m, t[2]);
-                        atomicAdd(sums + SI.denP, t[3]);
-                    }
-                }
-            }
-        } else {
-            // ePIE: dP = conj(O) chi / max|O|^2; O += beta/S sum_m conj(psi) chi / max sum_m |psi|^2
-            // (solvers.py:459-486)
-            float omax = 0.f;
-            float *xf = reinterpret_cast<float *>(xb);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const float2 o = cv.at(Os, u, q);
-                    omax = fmaxf(omax, cabs2(o));
-                    if (upd_obj) xf[I::flat(u, q)] = cabs2(ps[I::flat(u, q)]);
-                }
-            omax = block_max_float<FFT_THREADS>(omax, fred);
-            if (upd_obj) {
-                cl.sync();
-                float lmax = 0.f;
-                for (int sl = slot0; sl < slot1; ++sl) {
-                    const int f = sl * FFT_THREADS + tid;
-                    float w = 0.f;
-                    for (int r = 0; r < M; ++r) w += cl.map_shared_rank(xf, r)[f];
-                    lmax = fmaxf(lmax, w);
-                }
-                lmax = block_max_float<FFT_THREADS>(lmax, fred);
-                if (tid == 0) fred[32] = lmax;
-                cl.sync();
-                float wmax = 0.f;
-                for (int r = 0; r < M; ++r) wmax = fmaxf(wmax, cl.map_shared_rank(fred, r)[32]);
-                float2 *xc = xb;
+            } else {
+                const float *pat = a.group_patterns ? a.group_patterns + (size_t)b * NN : a.patterns + pos * NN;
+                double e2 = 0.0, loss = 0.0;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int q = 0; q < E; ++q) xc[I::flat(u, q)] = cmulc(v[u][q], ps[I::flat(u, q)]);
+                    for (int e = 0; e < E; ++e) {
+                        const int f = I::flat(u, e);
+                        float inten = 0.f;
+                        for (int r = 0; r < MR; ++r)
+                                if (r < M) inten += rxf[r][f];
+                        const float pv = __ldg(pat + I::ky(e) * N + I::kx(u));
+                        const float mk = mask_ones ? 1.0f : __ldg(a.mask_k + f);
+                        if (calc_err && m == 0) {
+                            const float d = inten - pv;
+                            if (d == d) e2 += (double)d * (double)d;
+                        }
+                        const float pm = np_max0(pv);
+                        float fac;
+                        if constexpr (!grad) {
+                            // amplitude / anscombe wave update (noise_models.py:47-64)
+                            fac = (sqrtf(pm + a.offset) / (sqrtf(inten + a.offset) + a.eps) - 1.0f) * mk;
+                        } else {
+                            if (a.noise == PHB_NOISE_POISSON) {
+                                // d/dI of mask*(I + eps + p*(log(p+eps) - log(I+eps) - 1)) (noise_models.py:86-102)
+                                if (m == 0)
+                                    loss += (double)(mk * (inten + a.eps +
+                                                           pm * (logf(pm + a.eps) - logf(inten + a.eps) - 1.0f)));
+                                fac = 2.0f * mk * (1.0f - pm / (inten + a.eps));
+                            } else {
+                                // d/dI of 2 mask (sqrt(p+c) - sqrt(I+c) - eps)^2 / var (noise_models.py:29-45)
+                                const float sI = sqrtf(inten + a.offset);
+                                const float dlt = sqrtf(pm + a.offset) - sI - a.eps;
+                                if (m == 0) loss += (double)(2.0f * mk * dlt * dlt / a.var);
+                                fac = 2.0f * (-2.0f * mk * dlt / (a.var * sI));
+                            }
+                        }
+                        v[u][e] = cscale(v[u][e], fac);
+                    }
                 cl.sync();
-                const float scl = a.beta_object / (float)S / wmax;
-                float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
-                for (int sl = slot0; sl < slot1; ++sl) {
-                    const int f = sl * FFT_THREADS + tid;
-                    float2 acc = make_float2(0.f, 0.f);
-                    for (int r = 0; r < M; ++r) acc = cadd(acc, cl.map_shared_rank(xc, r)[f]);
-                    int rr, cc;
-                    flat_to_rc<N>(f, rr, cc);
-                    const int64_t y = ci.y0 + rr, x = ci.x0 + cc;
-                    if (y >= 0 && y < a.H && x >= 0 && x < a.W) atomic_add_c(dst + y * a.W + x, cscale(acc, scl));
+                if (m == 0 && (calc_err || grad)) {
+                    double t[2] = {e2, loss};
+                    block_sum_doubles<FFT_THREADS>(t, 2, dred);
+                    if (tid == 0) {
+                        if (calc_err) a.errors[pos] = (float)sqrt(t[0]);
+                        if (grad) sums[a.o_loss + b] = t[1];
+                    }
                 }
-                cl.sync();
+                fwd = false;
+                phase = PH_BACK;
+                s = S - 1;
             }
-            const float inv = 1.0f / omax;
+        } else if (phase == PH_BACK) {
+            // ------------------------------------------- adjoint of slice s (R layout)
+            const CutView<N> cv = load_cv();
+            if (s == S - 1) {
 #pragma unroll
-            for (int u = 0; u < U; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const float2 c = v[u][q];
-                    if (s == 0 && upd_pos) ps[I::flat(u, q)] = c;
-                    const float2 o = cv.at(Os, u, q);
-                    v[u][q] = cscale(cmulc(c, o), inv);
+                    for (int q = 0; q < E; ++q) v[u][q] = cscale(v[u][q], inv_n);   // chi = ifft2(.)
+            }
+            const float2 *Os = a.object + (size_t)s * a.H * a.W;
+            float2 *ps = psi_b + (size_t)s * NN;
+            if constexpr (!epie) {
+                // LSQ-ML: dO = chi conj(psi), dP = chi conj(O) (solvers.py:242-271); gradient: same adjoint.
+                // Each mode scatters its own dO (the sum over modes is linear).
+                float t4[4] = {0.f, 0.f, 0.f, 0.f};   // per-thread partials, reduced in float64
+                float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int q = 0; q < E; ++q) {
+                        const int f = I::flat(u, q);
+                        const float2 c = v[u][q];
+                        const float2 o = cv.at(Os, u, q);
+                        const float c2 = cabs2(c);
+                        if (upd_obj) {
+                            const float2 p = ps[f];
+                            if (cv.ok(u, q)) atomic_add_c(dst + cv.off(u, q), cmulc(c, p));
+                            if (lsqml) {
+                                const float p2 = cabs2(p);
+                                t4[0] += c2 * p2;
+                                t4[1] += (c2 * p2) * p2;
+                            }
+                        }
+                        if (s == 0) {
+                            if (lsqml && upd_probe) {
+                                const float o2 = cabs2(o);
+                                t4[2] += c2 * o2;
+                                t4[3] += (c2 * o2) * o2;
+                            }
+                            if (upd_pos) ps[f] = c;   // exit-wave update of slice 0 for the position step
+                        }
+                        v[u][q] = cmulc(c, o);
+                    }
+                if (lsqml) {
+                    if (upd_obj) {
+                        warp_atomic_sum(sums + a.o_numO + (int64_t)b * S + s, (double)t4[0]);
+                        warp_atomic_sum(sums + a.o_denO + s, (double)t4[1]);
+                    }
+                    if (s == 0 && upd_probe) {
+                        warp_atomic_sum(sums + a.o_numP + (int64_t)b * M + m, (double)t4[2]);
+                        warp_atomic_sum(sums + a.o_denP, (double)t4[3]);
+                    }
                 }
-        }
-
-        if (s > 0) {
-            if (tilted) tilt_tables<N>(a, pos, s - 1, ry, rx);   // read after the FFT's barriers
-            fft2_r2k<N>(v, xb, twid);
-            const float2 *pr = a.prop_k + (size_t)(s - 1) * NN;
-            const float sc = 1.0f / (float)NN;
+            } else {
+                // ePIE: dP = conj(O) chi / max|O|^2; O += beta/S sum_m conj(psi) chi / max sum_m |psi|^2
+                // (solvers.py:459-486)
+                float omax = 0.f;
+                float *xf = reinterpret_cast<float *>(xb);
 #pragma unroll
-            for (int u = 0; u < U; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    float2 p = __ldg(pr + I::flat(u, e));
-                    if (tilted) p = cmul(p, cmul(ry[I::ky(e)], rx[I::kx(u)]));
-                    v[u][e] = cscale(cmulc(v[u][e], p), sc);
+                    for (int q = 0; q < E; ++q) {
+                        omax = fmaxf(omax, cabs2(cv.at(Os, u, q)));
+                        if (upd_obj) xf[I::flat(u, q)] = cabs2(ps[I::flat(u, q)]);
+                    }
+                omax = block_max_float<FFT_THREADS>(omax, fred);
+                if (upd_obj) {
+                    cl.sync();
+                    float lmax = 0.f;
+                    for (int sl = slot0; sl < slot1; ++sl) {
+                        const int f = sl * FFT_THREADS + tid;
+                        float w = 0.f;
+                        for (int r = 0; r < MR; ++r)
+                            if (r < M) w += cl.map_shared_rank(xf, r)[f];
+                        lmax = fmaxf(lmax, w);
+                    }
+                    lmax = block_max_float<FFT_THREADS>(lmax, fred);
+                    // slot by slice parity: a rank may write the next slice's maximum while
+                    // others still read this one (the exchange barrier orders slice s-2's reads)
+                    const int slot = 32 + (s & 1);
+                    if (tid == 0) fred[slot] = lmax;
+                    cl.sync();
+                    float wmax = 0.f;
+                    for (int r = 0; r < M; ++r) wmax = fmaxf(wmax, cl.map_shared_rank(fred, r)[slot]);
+                    // last remote access of the program: no rank may leave (and release its
+                    // shared memory) before every rank has read the slice-0 maxima
+                    if (s == 0) cl.sync();
+                    const float scl = a.beta_object / (float)S / wmax;
+                    float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int q = 0; q < E; ++q)
+                            if (cv.ok(u, q))
+                                atomic_add_c(dst + cv.off(u, q), cscale(cmulc(v[u][q], ps[I::flat(u, q)]), scl));
                 }
-            ifft2_k2r<N>(v, xb, twid);
-        } else if (upd_probe) {
-            // sum_b fft2(dP) conj(H_b): accumulated per mode in K order (solvers.py:265, 484)
-            fft2_r2k<N>(v, xb, twid);
-            float2 *ap = a.acc_probe + (size_t)m * NN;
-            const float sc = 1.0f / (float)N;
+                const float inv = 1.0f / omax;
 #pragma unroll
-            for (int u = 0; u < U; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const float2 h = cmul(hy[I::ky(e)], hx[I::kx(u)]);
-                    atomic_add_c(ap + I::flat(u, e), cscale(cmulc(v[u][e], h), sc));
-                }
-        }
-    }
-
-    // ---------------------------------------------------------- position step (solvers.py:275-288)
-    if (upd_pos) {
-        const float2 *pk = a.probe_k + (size_t)m * NN;
-        const float2 *ps0 = psi_b;
-        const float twopi = 6.283185307179586f;
-        for (int dir = 0; dir < 2; ++dir) {
+                    for (int q = 0; q < E; ++q) {
+                        const float2 c = v[u][q];
+                        if (s == 0 && upd_pos) ps[I::flat(u, q)] = c;
+                        v[u][q] = cscale(cmulc(c, cv.at(Os, u, q)), inv);
+                    }
+            }
+            if (s > 0) {
+                load_prop(s - 1);
+                fwd = true;
+                phase = PH_BPROP;
+            } else if (upd_probe) {
+                fwd = true;
+                phase = PH_PROBE;
+            } else if (upd_pos) {
+                load_probe_spectrum(0);
+                fwd = false;
+                phase = PH_POS;
+                dir = 0;
+            } else {
+                return;
+            }
+        } else if (phase == PH_BPROP) {
+            // ------------------------------------------- adjoint propagation (K layout)
+            const uint64_t kband = s_bits[FFT_THREADS + tid];
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     const int ky = I::ky(e), kx = I::kx(u);
-                    const float k = dir == 0 ? a.fy[ky] : a.fx[kx];
-                    const float2 g = cmul(__ldg(pk + I::flat(u, e)), cmul(hy[ky], hx[kx]));
-                    const float w = twopi * k;
-                    v[u][e] = make_float2(w * g.y, -w * g.x);   // g * (-2 pi i k)
+                    const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
+                    v[u][e] = cscale(cmulc(v[u][e], p), inv_nn);
                 }
-            ifft2_k2r<N>(v, xb, twid);
-            double t[2] = {0.0, 0.0};
+            fwd = false;
+            phase = PH_BACK;
+            --s;
+        } else if (phase == PH_PROBE) {
+            // ------------------------------------------- sum_b fft2(dP) conj(H_b) (solvers.py:265, 484)
+            float2 *ap = a.acc_probe + (size_t)m * NN;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const float2 h = cmul(hy[I::ky(e)], hx[I::kx(u)]);
+                    atomic_add_c(ap + I::flat(u, e), cscale(cmulc(v[u][e], h), inv_n));
+                }
+            if (!upd_pos) return;
+            load_probe_spectrum(0);
+            fwd = false;
+            phase = PH_POS;
+            dir = 0;
+        } else {
+            // ------------------------------------------- position step (solvers.py:275-288), R layout
+            const CutView<N> cv = load_cv();
+            const float2 *ps0 = psi_b;   // slot 0 holds the slice-0 exit-wave update
+            float t2[2] = {0.f, 0.f};
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int q = 0; q < E; ++q) {
-                    const float2 o = cv.at(a.object, u, q);
                     const float2 c = ps0[I::flat(u, q)];
-                    const float2 pr = cmul(v[u][q], o);
-                    t[0] += (double)(c.x * pr.x + c.y * pr.y);
-                    t[1] += (double)cabs2(pr);
+                    const float2 pr = cmul(v[u][q], cv.at(a.object, u, q));
+                    t2[0] += c.x * pr.x + c.y * pr.y;
+                    t2[1] += cabs2(pr);
                 }
-            block_sum_doubles<FFT_THREADS>(t, 2, dred);
-            if (tid == 0) {
-                atomicAdd(sums + SI.pnum + 2 * b + dir, t[0]);
-                atomicAdd(sums + SI.pden + 2 * b + dir, t[1]);
-            }
+            warp_atomic_sum(sums + a.o_pnum + 2 * b + dir, (double)t2[0]);
+            warp_atomic_sum(sums + a.o_pden + 2 * b + dir, (double)t2[1]);
+            if (dir == 1) return;
+            dir = 1;
+            load_probe_spectrum(1);
+            fwd = false;
         }
+        PHB_T_MARK(2 + timed_phase);
     }
 }
 
@@ -809,6 +906,55 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
     (void)fred;
 }
 
+// ---------------------------------------------------------------- propagator factors
+// phaser's propagators (simulation.py:160-190) are band-limited Fresnel kernels,
+// exp(-i pi dz lambda (ky^2 + kx^2)) * band, i.e. p(ky) p(kx) inside the band with
+// p(0) = 1.  Extract p(ky) = P[ky, 0] and p(kx) = P[0, kx], the band bits (P != 0), and
+// check |P - band p(ky) p(kx)| <= 1e-5 max|P| (the reference's own float32 rounding is
+// ~1e-6); info[0] = pattern mask is all ones, info[1] = separable.
+template <int N>
+__global__ void __launch_bounds__(1024) k_prop_init(const float2 *props, int G, const float *mask, float2 *prop1d,
+                                                   uint32_t *band, int32_t *info) {
+    __shared__ int ok_mask, ok_sep;
+    if (threadIdx.x == 0) {
+        ok_mask = 1;
+        ok_sep = 1;
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < N * N; f += blockDim.x)
+        if (mask[f] != 1.0f) ok_mask = 0;
+    if (G <= 0) {
+        for (int k = threadIdx.x; k < N * N / 32; k += blockDim.x) band[k] = 0xffffffffu;
+    } else {
+        for (int k = threadIdx.x; k < N * N / 32; k += blockDim.x) {
+            uint32_t bits = 0;
+            for (int j = 0; j < 32; ++j) {
+                const float2 p = props[k * 32 + j];
+                if (p.x != 0.f || p.y != 0.f) bits |= 1u << j;
+            }
+            band[k] = bits;
+        }
+        for (int i = threadIdx.x; i < G * 2 * N; i += blockDim.x) {
+            const int g = i / (2 * N), k = i % (2 * N);
+            prop1d[i] = k < N ? props[(size_t)g * N * N + (size_t)k * N] : props[(size_t)g * N * N + (k - N)];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < G * N * N; i += blockDim.x) {
+            const int g = i / (N * N), f = i % (N * N), ky = f / N, kx = f % N;
+            const float2 p = props[i];
+            const bool in = (band[f >> 5] >> (f & 31)) & 1u;
+            const float2 q = in ? cmul(prop1d[g * 2 * N + ky], prop1d[g * 2 * N + N + kx]) : make_float2(0.f, 0.f);
+            const float d = fabsf(p.x - q.x) + fabsf(p.y - q.y);
+            if (!(d <= 1e-5f * fmaxf(1.0f, sqrtf(cabs2(p))))) ok_sep = 0;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        info[0] = ok_mask;
+        info[1] = ok_sep;
+    }
+}
+
 // ---------------------------------------------------------------- K-order packing
 template <int N>
 __global__ void k_pack_c64(const float2 *src, float2 *dst) {
@@ -954,7 +1100,9 @@ __global__ void k_check_finite(const float2 *v, int64_t n, int32_t *status, int3
 // ---------------------------------------------------------------- host glue
 template <int N>
 static size_t group_smem_bytes() {
-    return (size_t)Lay<N>::BUF * sizeof(float2) + 5 * N * sizeof(float2) + 64 * sizeof(double) + 64 * sizeof(float);
+    return (size_t)Lay<N>::BUF * sizeof(float2) + 5 * N * sizeof(float2) + 64 * sizeof(double) + 64 * sizeof(float) +
+           (size_t)N * N / 32 * sizeof(uint32_t) + 2 * FFT_THREADS * sizeof(uint64_t) +
+           (size_t)FFTCfg<N>::U * FFT_THREADS * sizeof(int32_t);
 }
 template <int N>
 static size_t fft_smem_bytes() {
@@ -1016,7 +1164,19 @@ static GroupArgs make_args(const phb_engine *e, const Workspace &w, int mode, in
     a.group = group;
     a.patterns = e->patterns;
     a.mask_k = w.mask_k;
-    a.prop_k = w.prop_k;
+    a.prop1d = w.prop1d;
+    a.band = w.band;
+    a.info = w.info;
+    a.err_word = w.info + 3;
+    const SumIdx SI(e->B_max, e->S, e->M);
+    a.o_numO = SI.numO;
+    a.o_denO = SI.denO;
+    a.o_numP = SI.numP;
+    a.o_denP = SI.denP;
+    a.o_pnum = SI.pnum;
+    a.o_pden = SI.pden;
+    a.o_pnorm = SI.pnorm;
+    a.o_loss = SI.loss;
     a.probe_k = w.probe_k;
     a.fy = e->ky;
     a.fx = e->kx;
@@ -1028,11 +1188,11 @@ static GroupArgs make_args(const phb_engine *e, const Workspace &w, int mode, in
     return a;
 }
 
-template <int N, int MODE>
+template <int N, int MODE, int MC>
 static int launch_group_mode(const GroupArgs &a, cudaStream_t st) {
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(k_group<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_group<N, MODE, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)group_smem_bytes<N>()) != cudaSuccess)
             return record_cuda(cudaGetLastError());
         configured = true;
@@ -1049,21 +1209,32 @@ static int launch_group_mode(const GroupArgs &a, cudaStream_t st) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const int rc = record_cuda(cudaLaunchKernelEx(&cfg, k_group<N, MODE>, a));
+    const int rc = record_cuda(cudaLaunchKernelEx(&cfg, k_group<N, MODE, MC>, a));
     if (rc == PHB_OK) count_launch();
     return rc;
+}
+
+template <int N, int MODE>
+static int launch_group_m(const GroupArgs &a, cudaStream_t st) {
+    switch (a.M) {
+        case 1: return launch_group_mode<N, MODE, 1>(a, st);
+        case 2: return launch_group_mode<N, MODE, 2>(a, st);
+        case 4: return launch_group_mode<N, MODE, 4>(a, st);
+        case 8: return launch_group_mode<N, MODE, 8>(a, st);
+        default: return launch_group_mode<N, MODE, 0>(a, st);
+    }
 }
 
 template <int N>
 static int launch_group(const GroupArgs &a, cudaStream_t st) {
     switch (a.mode) {
-        case MODE_LSQML: return launch_group_mode<N, MODE_LSQML>(a, st);
-        case MODE_EPIE: return launch_group_mode<N, MODE_EPIE>(a, st);
-        case MODE_GRAD: return launch_group_mode<N, MODE_GRAD>(a, st);
-        case MODE_PRE_LSQML: return launch_group_mode<N, MODE_PRE_LSQML>(a, st);
-        case MODE_PRE_EPIE: return launch_group_mode<N, MODE_PRE_EPIE>(a, st);
-        case MODE_PRE_GRAD: return launch_group_mode<N, MODE_PRE_GRAD>(a, st);
-        case MODE_SIM: return launch_group_mode<N, MODE_SIM>(a, st);
+        case MODE_LSQML: return launch_group_m<N, MODE_LSQML>(a, st);
+        case MODE_EPIE: return launch_group_m<N, MODE_EPIE>(a, st);
+        case MODE_GRAD: return launch_group_m<N, MODE_GRAD>(a, st);
+        case MODE_PRE_LSQML: return launch_group_mode<N, MODE_PRE_LSQML, 0>(a, st);
+        case MODE_PRE_EPIE: return launch_group_mode<N, MODE_PRE_EPIE, 0>(a, st);
+        case MODE_PRE_GRAD: return launch_group_mode<N, MODE_PRE_GRAD, 0>(a, st);
+        case MODE_SIM: return launch_group_m<N, MODE_SIM>(a, st);
         default: return PHB_ERR_INVALID_ARG;
     }
 }
@@ -1093,13 +1264,18 @@ static int engine_init(const phb_engine *e, cudaStream_t st) {
     if (!rc)
         rc = record_cuda(cudaMemsetAsync(w.sums, 0, (size_t)SumIdx(e->B_max, e->S, e->M).total * sizeof(double), st));
     if (rc) return rc;
-    if (e->S > 1) {
-        k_pack_c64<N><<<e->S - 1, FFT_THREADS, 0, st>>>((const float2 *)e->propagators, w.prop_k);
-        if ((rc = check_launch())) return rc;
-    }
+    k_prop_init<N><<<1, 1024, 0, st>>>((const float2 *)e->propagators, e->S - 1, e->pattern_mask, w.prop1d, w.band,
+                                        w.info);
+    if ((rc = check_launch())) return rc;
     k_pack_f32<N><<<1, FFT_THREADS, 0, st>>>(e->pattern_mask, w.mask_k);
     if ((rc = check_launch())) return rc;
-    return probe_spectrum<N>(e, w, st);
+    if ((rc = probe_spectrum<N>(e, w, st))) return rc;
+    // the propagator check is the only result the host needs from init
+    int32_t info[4];
+    if ((rc = record_cuda(cudaMemcpyAsync(info, w.info, sizeof(info), cudaMemcpyDeviceToHost, st)))) return rc;
+    if ((rc = record_cuda(cudaStreamSynchronize(st)))) return rc;
+    if (e->S > 1 && !info[1]) return PHB_ERR_UNSUPPORTED;   // not a separable (Fresnel) propagator
+    return PHB_OK;
 }
 
 template <int N>
@@ -1154,6 +1330,8 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     }
     if (mode == MODE_GRAD) a.acc_obj = (float2 *)sp->grad_object;
     a.group_patterns = sp->group_patterns;
+    a.status = sp->status;
+    a.group_index = sp->group_index;
     if (sp->event_begin && (rc = record_cuda(cudaEventRecord((cudaEvent_t)sp->event_begin, st)))) return rc;
     if ((rc = launch_group<N>(a, st))) return rc;
     if (sp->event_end && (rc = record_cuda(cudaEventRecord((cudaEvent_t)sp->event_end, st)))) return rc;
@@ -1227,6 +1405,17 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
 }  // namespace phb
 
 using namespace phb;
+
+#ifdef PHB_PHASE_TIMING
+extern "C" int phb_debug_phase_cycles(unsigned long long *out16, int reset) {
+    int rc = phb::record_cuda(cudaMemcpyFromSymbol(out16, phb::g_phase_cycles, 16 * sizeof(unsigned long long)));
+    if (!rc && reset) {
+        unsigned long long z[16] = {0};
+        rc = phb::record_cuda(cudaMemcpyToSymbol(phb::g_phase_cycles, z, sizeof(z)));
+    }
+    return rc;
+}
+#endif
 
 extern "C" {
 

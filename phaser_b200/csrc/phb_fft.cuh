@@ -1,6 +1,6 @@
 // Register-resident 2D FFT of one N x N complex64 tile per CTA (N = 64, 128).
 //
-// A CTA of 512 threads holds the whole tile in registers (16 or 8 complex
+// A CTA of 256 threads holds the whole tile in registers (64 or 16 complex
 // values per thread) and exchanges through ONE N*N complex shared-memory
 // buffer.  A 1D line FFT of length N = E * NT runs as
 //     radix-E DFT in registers (elements strided by NT)
@@ -13,9 +13,9 @@
 // constraint, shift filters) is done in K layout with explicit (ky, kx)
 // indices, so no reorder pass is ever needed.
 //
-// Layouts (tid = threadIdx.x, rsel = tid / 8, jl = tid % 8, unit u):
-//   R layout: v[u][q]          = x[row = rsel + 64u][col = jl + 8q]
-//   K layout: v[u][p*NT + k2]  = X[ky = (jl*P + p) + E*k2][kx = rsel + 64u]
+// Layouts (tid = threadIdx.x, rsel = tid / 8, jl = tid % 8, unit u, RPP = threads / 8):
+//   R layout: v[u][q]          = x[row = rsel + RPP*u][col = jl + 8q]
+//   K layout: v[u][p*NT + k2]  = X[ky = (jl*P + p) + E*k2][kx = rsel + RPP*u]
 // The transforms are unnormalised DFTs with exp(-2 pi i nk/N) forward.
 //
 // Shared-memory addresses are padded / XOR-swizzled so that every 8-byte
@@ -27,11 +27,15 @@
 
 namespace phb {
 
-constexpr int FFT_THREADS = 512;
+#ifndef PHB_FFT_THREADS
+#define PHB_FFT_THREADS 512
+#endif
+constexpr int FFT_THREADS = PHB_FFT_THREADS;  // threads per tile (256: 4 lines each; 512: 2)
+constexpr int RPP = FFT_THREADS / 8;          // rows (lines) handled per pass: 8 threads per line
 
 template <int N> struct FFTCfg;
-template <> struct FFTCfg<128> { static constexpr int E = 16, NT = 8, P = 2, U = 2; };
-template <> struct FFTCfg<64>  { static constexpr int E = 8,  NT = 8, P = 1, U = 1; };
+template <> struct FFTCfg<128> { static constexpr int E = 16, NT = 8, P = 2, U = 128 / RPP; };
+template <> struct FFTCfg<64>  { static constexpr int E = 8,  NT = 8, P = 1, U = 64 / RPP; };
 
 // ----------------------------------------------------------------- small DFTs
 template <bool INV>
@@ -163,7 +167,7 @@ __device__ __forceinline__ void line_pass_fwd(float2 (&v)[FFTCfg<N>::U][FFTCfg<N
 #pragma unroll
         for (int k1 = 1; k1 < E; ++k1) v[u][k1] = cmul(v[u][k1], tw[k1 * NT]);
 #pragma unroll
-        for (int k1 = 0; k1 < E; ++k1) lb[64 * u * LS + k1 * NT + (jl ^ (k1 / P))] = v[u][k1];
+        for (int k1 = 0; k1 < E; ++k1) lb[RPP * u * LS + k1 * NT + (jl ^ (k1 / P))] = v[u][k1];
     }
     __syncthreads();
     const float2 *rb = xb + rsel * LS + jl * P * NT;
@@ -172,7 +176,7 @@ __device__ __forceinline__ void line_pass_fwd(float2 (&v)[FFTCfg<N>::U][FFTCfg<N
 #pragma unroll
         for (int p = 0; p < P; ++p)
 #pragma unroll
-            for (int jj = 0; jj < NT; ++jj) v[u][p * NT + jj] = rb[64 * u * LS + p * NT + (jj ^ jl)];
+            for (int jj = 0; jj < NT; ++jj) v[u][p * NT + jj] = rb[RPP * u * LS + p * NT + (jj ^ jl)];
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -193,14 +197,14 @@ __device__ __forceinline__ void line_pass_inv(float2 (&v)[FFTCfg<N>::U][FFTCfg<N
         for (int p = 0; p < P; ++p) {
             dftL<NT, true>(&v[u][p * NT]);
 #pragma unroll
-            for (int jj = 0; jj < NT; ++jj) wb[64 * u * LS + p * NT + (jj ^ jl)] = v[u][p * NT + jj];
+            for (int jj = 0; jj < NT; ++jj) wb[RPP * u * LS + p * NT + (jj ^ jl)] = v[u][p * NT + jj];
         }
     __syncthreads();
     const float2 *lb = xb + rsel * LS;
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-        for (int k1 = 0; k1 < E; ++k1) v[u][k1] = lb[64 * u * LS + k1 * NT + (jl ^ (k1 / P))];
+        for (int k1 = 0; k1 < E; ++k1) v[u][k1] = lb[RPP * u * LS + k1 * NT + (jl ^ (k1 / P))];
     __syncthreads();
     const float2 *tw = twid + jl;
 #pragma unroll
@@ -212,31 +216,31 @@ __device__ __forceinline__ void line_pass_inv(float2 (&v)[FFTCfg<N>::U][FFTCfg<N
 }
 
 // row-pass output (K form of rows) -> column-pass input (R form of columns), and back.
-// Row r = rsel + 64u holds kx = (jl*P + p) + E*k2; column c = rsel + 64u holds rows jl + NT*q.
-// tile(r, c) = r*N + (c ^ g(r)); g(rsel + 64u) == g(rsel) and g(jl + NT*q) == g(jl).
+// Row r = rsel + RPP*u holds kx = (jl*P + p) + E*k2; column c = rsel + RPP*u holds rows jl + NT*q.
+// tile(r, c) = r*N + (c ^ g(r)); g(rsel + RPP*u) == g(rsel) and g(jl + NT*q) == g(jl).
 template <int N, bool TO_COLUMNS>
 __device__ __forceinline__ void transpose(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb) {
     using Ly = Lay<N>;
     constexpr int E = Ly::E, NT = Ly::NT, P = Ly::P, U = Ly::U;
     const int rsel = threadIdx.x >> 3, jl = threadIdx.x & 7;
-    // row side: element (u, p, k2) at rsel*N + 64u*N + (((jl*P + p) + E*k2) ^ gr)
+    // row side: element (u, p, k2) at rsel*N + RPP*u*N + (((jl*P + p) + E*k2) ^ gr)
     const int gr = Ly::g(rsel);
-    // column side: element (u, q) at jl*N + NT*q*N + ((rsel + 64u) ^ gc)
+    // column side: element (u, q) at jl*N + NT*q*N + ((rsel + RPP*u) ^ gc)
     const int gc = Ly::g(jl);
     float2 *rowb = xb + rsel * N;
-    float2 *colb = xb + jl * N + (rsel ^ gc);           // gc < 64, so (rsel + 64u) ^ gc = (rsel ^ gc) + 64u
+    float2 *colb = xb + jl * N + (rsel ^ gc);           // gc < 16 <= RPP: (rsel + RPP*u) ^ gc = (rsel ^ gc) + RPP*u
     if constexpr (TO_COLUMNS) {
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 if constexpr (N == 128) {   // gr < E: the XOR stays inside the low 4 bits
-                    float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ gr);
+                    float2 *b = rowb + RPP * u * N + ((jl * P + p) ^ gr);
 #pragma unroll
                     for (int k2 = 0; k2 < NT; ++k2) b[E * k2] = v[u][p * NT + k2];
                 } else {                    // E == 8: bit 3 of gr flips bit 0 of k2
                     const int hb = gr >> 3;
-                    float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ (gr & 7));
+                    float2 *b = rowb + RPP * u * N + ((jl * P + p) ^ (gr & 7));
 #pragma unroll
                     for (int k2 = 0; k2 < NT; ++k2) b[E * (k2 ^ hb)] = v[u][p * NT + k2];
                 }
@@ -245,25 +249,25 @@ __device__ __forceinline__ void transpose(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int q = 0; q < E; ++q) v[u][q] = colb[NT * q * N + 64 * u];
+            for (int q = 0; q < E; ++q) v[u][q] = colb[NT * q * N + RPP * u];
         __syncthreads();
     } else {
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int q = 0; q < E; ++q) colb[NT * q * N + 64 * u] = v[u][q];
+            for (int q = 0; q < E; ++q) colb[NT * q * N + RPP * u] = v[u][q];
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 if constexpr (N == 128) {
-                    const float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ gr);
+                    const float2 *b = rowb + RPP * u * N + ((jl * P + p) ^ gr);
 #pragma unroll
                     for (int k2 = 0; k2 < NT; ++k2) v[u][p * NT + k2] = b[E * k2];
                 } else {
                     const int hb = gr >> 3;
-                    const float2 *b = rowb + 64 * u * N + ((jl * P + p) ^ (gr & 7));
+                    const float2 *b = rowb + RPP * u * N + ((jl * P + p) ^ (gr & 7));
 #pragma unroll
                     for (int k2 = 0; k2 < NT; ++k2) v[u][p * NT + k2] = b[E * (k2 ^ hb)];
                 }
@@ -305,10 +309,10 @@ struct Idx {
     using C = FFTCfg<N>;
     static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
     // R layout
-    static __device__ __forceinline__ int row(int u) { return (threadIdx.x >> 3) + 64 * u; }
+    static __device__ __forceinline__ int row(int u) { return (threadIdx.x >> 3) + RPP * u; }
     static __device__ __forceinline__ int col(int q) { return (threadIdx.x & 7) + NT * q; }
     // K layout
-    static __device__ __forceinline__ int kx(int u) { return (threadIdx.x >> 3) + 64 * u; }
+    static __device__ __forceinline__ int kx(int u) { return (threadIdx.x >> 3) + RPP * u; }
     static __device__ __forceinline__ int ky(int e) {
         return ((threadIdx.x & 7) * P + e / NT) + E * (e % NT);
     }
@@ -322,7 +326,7 @@ __device__ __forceinline__ void flat_to_rc(int f, int &r, int &c) {
     using C = FFTCfg<N>;
     const int t = f % FFT_THREADS, s = f / FFT_THREADS;   // s = u*E + q
     const int u = s / C::E, q = s % C::E;
-    r = (t >> 3) + 64 * u;
+    r = (t >> 3) + RPP * u;
     c = (t & 7) + C::NT * q;
 }
 // ... and to (ky, kx) in K layout
@@ -331,7 +335,7 @@ __device__ __forceinline__ void flat_to_k(int f, int &ky, int &kx) {
     using C = FFTCfg<N>;
     const int t = f % FFT_THREADS, s = f / FFT_THREADS;
     const int u = s / C::E, e = s % C::E;
-    kx = (t >> 3) + 64 * u;
+    kx = (t >> 3) + RPP * u;
     ky = ((t & 7) * C::P + e / C::NT) + C::E * (e % C::NT);
 }
 

@@ -195,6 +195,8 @@ class ConventionalEngine:
     def check(self, i: int, it_pos: bool = True, it_err: bool = True) -> t.Optional[float]:
         state, eng = self.state, self.eng
         bad_group, n_out, err = int(self.status_host[0]), int(self.status_host[1]), float(self.status_host[2])
+        if bad_group >= _lib.PHB_STATUS_INTERNAL:
+            raise RuntimeError(f"internal error: fused kernel aborted in group {bad_group - _lib.PHB_STATUS_INTERNAL}")
         if bad_group >= 0:
             raise ValueError(f"NaN or inf encountered in object or probe, group {bad_group}")
         if it_pos and n_out > 0:

@@ -100,6 +100,8 @@ GROUP_CONFIGS = [
     ('lsqml', dict(seed=25, N=128, M=2, S=2), dict(update_probe=False)),
     ('epie', dict(seed=26, N=64, M=2, S=3), {}),
     ('epie', dict(seed=27, N=128, M=1, S=2), {}),
+    ('lsqml', dict(seed=28, N=64, M=2, S=8, scan_shape=(3, 3)), {}),
+    ('epie', dict(seed=29, N=64, M=1, S=6, scan_shape=(3, 3)), {}),
 ]
 
 
