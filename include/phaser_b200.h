@@ -30,6 +30,7 @@ extern "C" {
 #define PHB_ERR_CUDA           3   /* a CUDA launch or runtime call failed */
 #define PHB_ERR_NONFINITE      4   /* NaN/inf found in the object or probe */
 #define PHB_ERR_OUTSIDE        5   /* probe positions completely outside the object */
+#define PHB_ERR_SCRATCH_LIMIT  6   /* problem too large for phb_solver_group_static's fixed scratch */
 
 const char *phb_status_string(int status);
 int phb_version(void);
@@ -202,6 +203,28 @@ int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, flo
  * place (LSQ-ML, ePIE) or accumulates gradients (GRAD). */
 int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
                      void *stream);
+
+/* Allocation-free form of phb_solver_group.  It has no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory at the point where they run a
+ * reconstruction step: e.g. a plugin inside an acquisition or instrument-control
+ * process whose device memory is budgeted and owned by the host application, or
+ * code running under an allocator that forbids foreign allocations.  Such callers
+ * pass the same inputs and outputs as to phb_solver_group; `e->workspace` and
+ * `e->workspace_bytes` are ignored.  The scratch is a fixed 64 MiB array that is
+ * part of this library (every GPU that loads the library holds it until the
+ * process exits); a problem whose phb_engine_workspace_bytes(N, M, S, B, H, W)
+ * exceeds 64 MiB is rejected with PHB_ERR_SCRATCH_LIMIT.
+ *
+ * Each call rebuilds its tables from the inputs and clears every accumulator,
+ * so calls are independent; no cudaMalloc, cudaFree or allocating library
+ * routine is called.  All calls share the one array: calls whose work overlaps
+ * on the GPU (other streams, other threads) race and corrupt each other -- order
+ * them on one stream.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call waits once for its stream (propagator check). */
+int phb_solver_group_static(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
+                            void *stream);
 
 /* Per-iteration position update (phaser/engines/conventional/run.py:95-110 with
  * phaser/engines/common/position_correction.py): subtract mean, momentum or

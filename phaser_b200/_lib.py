@@ -18,6 +18,7 @@ PHB_ERR_UNSUPPORTED = 2
 PHB_ERR_CUDA = 3
 PHB_ERR_NONFINITE = 4
 PHB_ERR_OUTSIDE = 5
+PHB_ERR_SCRATCH_LIMIT = 6
 
 PHB_SOLVER_LSQML = 0
 PHB_SOLVER_EPIE = 1
@@ -95,6 +96,8 @@ _SIGNATURES = {
                                    c_void_p, c_void_p, c_void_p]),
     'phb_solver_group': (c_i32, [ctypes.POINTER(PhbEngine), ctypes.POINTER(PhbStep), c_void_p, c_i32,
                                  c_void_p]),
+    'phb_solver_group_static': (c_i32, [ctypes.POINTER(PhbEngine), ctypes.POINTER(PhbStep), c_void_p, c_i32,
+                                        c_void_p]),
     'phb_simulate_group': (c_i32, [ctypes.POINTER(PhbEngine), c_void_p, c_i32, c_void_p, c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),

@@ -1517,3 +1517,46 @@ int phb_check_finite_c64(const void *arr, int64_t n, int32_t *status, int32_t co
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free variant
+// phb_solver_group_static: the same mini-batch step as phb_solver_group, but its
+// scratch (wavefield stack, accumulators, tables) lives in a fixed device array that
+// is part of this library, so the call needs no workspace and allocates nothing.
+namespace phb {
+
+constexpr size_t kStaticScratchBytes = (size_t)64 << 20;   // 64 MiB, held by every GPU that loads the library
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+constexpr int kMaxDevices = 64;
+static void *g_static_scratch_ptr[kMaxDevices] = {nullptr};   // device address of the array, per device
+
+}  // namespace phb
+
+extern "C" int phb_solver_group_static(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
+                                       void *stream) {
+    using namespace phb;
+    if (!e || !st || !group || B < 1) return PHB_ERR_INVALID_ARG;
+    int dev = 0;
+    int rc = record_cuda(cudaGetDevice(&dev));
+    if (rc) return rc;
+    if (dev < 0 || dev >= kMaxDevices) return PHB_ERR_UNSUPPORTED;
+    if (!g_static_scratch_ptr[dev]) {
+        // one-time set-up on this device (the array's host-side name is not a device address)
+        void *p = nullptr;
+        rc = record_cuda(cudaGetSymbolAddress(&p, g_static_scratch));
+        if (rc) return rc;
+        g_static_scratch_ptr[dev] = p;
+    }
+    phb_engine ws = *e;
+    ws.B_max = B;
+    ws.workspace = g_static_scratch_ptr[dev];
+    ws.workspace_bytes = kStaticScratchBytes;
+    if (ws.N <= 0 || ws.M <= 0 || ws.S <= 0 || ws.H <= 0 || ws.W <= 0) return PHB_ERR_INVALID_ARG;
+    if (carve(nullptr, ws.N, ws.M, ws.S, B, ws.H, ws.W).bytes > kStaticScratchBytes) return PHB_ERR_SCRATCH_LIMIT;
+    if ((rc = validate(&ws))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    // the array keeps the previous call's contents: engine_init clears every accumulator and
+    // rebuilds the tables (propagator factors, mask, probe spectrum) from this call's inputs
+    rc = ws.N == 128 ? engine_init<128>(&ws, s) : engine_init<64>(&ws, s);
+    if (rc) return rc;
+    return phb_solver_group(&ws, st, group, B, stream);
+}

@@ -35,6 +35,7 @@ const char *phb_status_string(int status) {
         case PHB_ERR_CUDA: return "CUDA error";
         case PHB_ERR_NONFINITE: return "NaN or inf encountered";
         case PHB_ERR_OUTSIDE: return "probe positions completely outside object";
+        case PHB_ERR_SCRATCH_LIMIT: return "problem too large for the 64 MiB static scratch of phb_solver_group_static";
         default: return "unknown status";
     }
 }
