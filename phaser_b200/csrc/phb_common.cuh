@@ -117,6 +117,12 @@ __device__ __forceinline__ void warp_atomic_sum(double *dst, double v) {
     if ((threadIdx.x & 31) == 0) atomicAdd(dst, v);
 }
 
+// Bulk prefetch of a contiguous, 16-byte aligned global range into L2 (sm_90+);
+// `bytes` a multiple of 16.  Issued by one thread; it does not block.
+__device__ __forceinline__ void prefetch_l2(const void *ptr, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
+}
+
 // Vector fp32 atomics (sm_90+): one red per complex value.
 __device__ __forceinline__ void atomic_add_c(float2 *addr, float2 v) {
     atomicAdd(addr, v);

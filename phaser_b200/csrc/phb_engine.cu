@@ -367,6 +367,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     for (int q = 0; q < E; ++q)
                         if (cv.ok(u, q)) atomicAdd(dst + cv.off(u, q), cabs2(v[u][q]));
             }
+            PHB_T_MARK(11);
             const bool last = s == S - 1;
             if constexpr (mode == MODE_PRE_LSQML || mode == MODE_PRE_EPIE) {
                 if (last) {   // rescale: sum(I_exp*mask) / sum|psi_last|^2 (Parseval), before transmission
@@ -528,34 +529,48 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 // LSQ-ML: dO = chi conj(psi), dP = chi conj(O) (solvers.py:242-271); gradient: same adjoint.
                 // Each mode scatters its own dO (the sum over modes is linear).
                 float t4[4] = {0.f, 0.f, 0.f, 0.f};   // per-thread partials, reduced in float64
-                float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
+                float2 *__restrict__ dst = a.acc_obj + (size_t)s * a.H * a.W;
+                // chunks of 8 elements: issue all object / wavefield loads of a chunk before
+                // its atomics, so they are in flight together
+                constexpr int CH = 8;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int q = 0; q < E; ++q) {
-                        const int f = I::flat(u, q);
-                        const float2 c = v[u][q];
-                        const float2 o = cv.at(Os, u, q);
-                        const float c2 = cabs2(c);
-                        if (upd_obj) {
-                            const float2 p = ps[f];
-                            if (cv.ok(u, q)) atomic_add_c(dst + cv.off(u, q), cmulc(c, p));
-                            if (lsqml) {
-                                const float p2 = cabs2(p);
-                                t4[0] += c2 * p2;
-                                t4[1] += (c2 * p2) * p2;
-                            }
+                    for (int q0 = 0; q0 < E; q0 += CH) {
+                        float2 oo[CH], pp[CH];
+#pragma unroll
+                        for (int j = 0; j < CH; ++j) {
+                            oo[j] = cv.at(Os, u, q0 + j);
+                            pp[j] = upd_obj ? ps[I::flat(u, q0 + j)] : make_float2(0.f, 0.f);
                         }
-                        if (s == 0) {
-                            if (lsqml && upd_probe) {
-                                const float o2 = cabs2(o);
-                                t4[2] += c2 * o2;
-                                t4[3] += (c2 * o2) * o2;
+#pragma unroll
+                        for (int j = 0; j < CH; ++j) {
+                            const int q = q0 + j;
+                            const int f = I::flat(u, q);
+                            const float2 c = v[u][q];
+                            const float2 o = oo[j];
+                            const float c2 = cabs2(c);
+                            if (upd_obj) {
+                                const float2 p = pp[j];
+                                if (cv.ok(u, q)) atomic_add_c(dst + cv.off(u, q), cmulc(c, p));
+                                if (lsqml) {
+                                    const float p2 = cabs2(p);
+                                    t4[0] += c2 * p2;
+                                    t4[1] += (c2 * p2) * p2;
+                                }
                             }
-                            if (upd_pos) ps[f] = c;   // exit-wave update of slice 0 for the position step
+                            if (s == 0) {
+                                if (lsqml && upd_probe) {
+                                    const float o2 = cabs2(o);
+                                    t4[2] += c2 * o2;
+                                    t4[3] += (c2 * o2) * o2;
+                                }
+                                if (upd_pos) ps[f] = c;   // exit-wave update of slice 0 for the position step
+                            }
+                            v[u][q] = cmulc(c, o);
                         }
-                        v[u][q] = cmulc(c, o);
                     }
+                PHB_T_MARK(9);
                 if (lsqml) {
                     if (upd_obj) {
                         warp_atomic_sum(sums + a.o_numO + (int64_t)b * S + s, (double)t4[0]);
@@ -566,6 +581,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         warp_atomic_sum(sums + a.o_denP, (double)t4[3]);
                     }
                 }
+                PHB_T_MARK(10);
             } else {
                 // ePIE: dP = conj(O) chi / max|O|^2; O += beta/S sum_m conj(psi) chi / max sum_m |psi|^2
                 // (solvers.py:459-486)
@@ -620,6 +636,9 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     }
             }
             if (s > 0) {
+                // the adjoint of slice s-1 reads its stored incident wave after the next
+                // transform pair: start moving it from HBM into L2 now
+                if (upd_obj && tid == 0) prefetch_l2(psi_b + (size_t)(s - 1) * NN, NN * sizeof(float2));
                 load_prop(s - 1);
                 fwd = true;
                 phase = PH_BPROP;
@@ -671,11 +690,19 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 #pragma unroll
             for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const float2 c = ps0[I::flat(u, q)];
-                    const float2 pr = cmul(v[u][q], cv.at(a.object, u, q));
-                    t2[0] += c.x * pr.x + c.y * pr.y;
-                    t2[1] += cabs2(pr);
+                for (int q0 = 0; q0 < E; q0 += 8) {
+                    float2 oo[8], cc[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        oo[j] = cv.at(a.object, u, q0 + j);
+                        cc[j] = ps0[I::flat(u, q0 + j)];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float2 pr = cmul(v[u][q0 + j], oo[j]);
+                        t2[0] += cc[j].x * pr.x + cc[j].y * pr.y;
+                        t2[1] += cabs2(pr);
+                    }
                 }
             warp_atomic_sum(sums + a.o_pnum + 2 * b + dir, (double)t2[0]);
             warp_atomic_sum(sums + a.o_pden + 2 * b + dir, (double)t2[1]);
