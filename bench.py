@@ -68,7 +68,7 @@ def ncu_traffic_per_launch():
     try:
         for line in open(path):
             if line.strip().startswith('traffic_bytes_per_full_launch:'):
-                return float(line.split(':', 1)[1].split()[0])
+                return float(line.split(':', 1)[1].split()[0]) / 1e9   # GB per launch
     except OSError:
         pass
     return None
@@ -331,7 +331,7 @@ def run_b200(args, world, rank, local):
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     traffic = ncu_traffic_per_launch()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "k_group<128> (fused LSQ-ML mini-batch)",
+            "traffic": traffic if (args.scan == 64 and args.batch == 256) else None, "traffic_unit": "GB per launch (ncu)", "kernel": "k_group<128> (fused LSQ-ML mini-batch)",
             "launch_ms": avg_ms, "launches_timed": len(fused), "bytes_per_launch": bytes_launch,
             "peak_source": f"{peak_kind} hbm_gbs", "share_of_step": sum(fused) / t_ms if t_ms else None}
 
