@@ -167,6 +167,8 @@ typedef struct phb_step {
                                     instead of patterns[group[b]] (host-streamed data) */
     void *event_begin;    /* optional cudaEvent_t recorded just before / after the fused kernel */
     void *event_end;
+    float grad_pos_scale; /* gradient solver: grad_pos = grad_pos_scale * dL/d(y, x) (0 means 1) */
+    double *group_loss;   /* gradient solver: optional device double, += the group's summed loss */
 } phb_step;
 
 /* Bytes of workspace the engine needs for groups of up to B_max positions. */
@@ -225,6 +227,41 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
  * capture.  Every call waits once for its stream (propagator check). */
 int phb_solver_group_static(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
                             void *stream);
+
+/* ------------------------------------------------------ gradient-engine updates
+ * optax semantics of phaser/engines/gradient/solvers.py:88-138 on device arrays:
+ * d = grad_scale * grad; SGD (optax.trace momentum / Nesterov, then lr), Adam
+ * (optax.scale_by_adam, |d|^2 second moment for complex d, then lr) or Polyak
+ * (scale_by_learning_rate(scaling) then scale_by_polyak(max_lr, f_min, eps), with
+ * *polyak_sq_norm = sum |scaling d|^2 over all of the solver's parameters); the
+ * update is added to `param`, or written to `update_out` when that is non-NULL. */
+#define PHB_OPTIM_SGD    0
+#define PHB_OPTIM_ADAM   1
+#define PHB_OPTIM_POLYAK 2
+
+typedef struct phb_optim {
+    int32_t kind, nesterov;
+    float *param;             /* n elements (complex pairs when complex_elems) */
+    const float *grad;        /* same layout as param */
+    float *state1;            /* SGD trace / Adam first moment, same layout; NULL if unused */
+    float *state2;            /* Adam second moment: n reals */
+    float *update_out;        /* optional: write the update instead of adding it */
+    int64_t n;
+    int32_t complex_elems;
+    float grad_scale, lr, momentum, b1, b2, eps, eps_root;
+    int64_t count;            /* Adam: step count including this update (>= 1) */
+    const double *polyak_sq_norm;
+    float polyak_scaling, polyak_max_lr, polyak_f_min, polyak_eps, loss;
+} phb_optim;
+
+int phb_optimizer_update(const phb_optim *o, void *stream);
+
+/* *out += sum over x[0:n] of (scale * x)^2 (float64 accumulation). */
+int phb_sq_norm_f32(const float *x, int64_t n, float scale, double *out, void *stream);
+
+/* param (n x 2) += update - mean(update): position updates keep the scan centred
+ * (phaser/engines/gradient/run.py:115-118). */
+int phb_add_centred(float *param, const float *update, int64_t n, void *stream);
 
 /* Per-iteration position update (phaser/engines/conventional/run.py:95-110 with
  * phaser/engines/common/position_correction.py): subtract mean, momentum or

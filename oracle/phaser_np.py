@@ -669,3 +669,46 @@ def run_conventional(run: ConventionalRun, *, probe, obj, scan, patterns, mask,
         if iteration_callback is not None:
             iteration_callback(it, probe, obj, flat_scan.reshape(scan.shape), err)
     return probe, obj, flat_scan.reshape(scan.shape), numpy.array(errors_out)
+
+
+def noise_dloss_dI(noise: NoiseModel, intensity, patterns, mask):
+    """dL/dI of NoiseModel.loss (noise_models.py:29-45 amplitude/anscombe, 86-102 Poisson)."""
+    pat = numpy.maximum(patterns, 0.0)
+    if noise.kind == 'poisson':
+        return mask * (1.0 - pat / (intensity + noise.eps))
+    var = 1. + noise.gaussian_variance
+    sI = numpy.sqrt(intensity + noise.offset)
+    return -2. * mask * (numpy.sqrt(pat + noise.offset) - sI - noise.eps) / (var * sI)
+
+
+def grad_model_grads(geom, probe, obj, group_scan, patterns, mask, props, tilts, noise: NoiseModel):
+    """Loss and gradients of the gradient-engine model (the adjoint of
+    phaser/engines/gradient/run.py:357-405 that jax.value_and_grad evaluates).
+
+    Complex gradients are returned as g = dL/dRe + i dL/dIm; phaser's update
+    direction -conj(jax_grad) (run.py:325) equals -g.  Position gradients are
+    dL/d(y, x) through the sub-pixel shift filter (the integer cutout start has no
+    gradient).  Returns (loss, g_object (S,H,W), g_probe (M,N,N), g_pos (B,2))."""
+    S = obj.shape[0]
+    shape = probe.shape[-2:]
+    psi0, cuts, starts, filt = cutout_group(geom, probe, obj, group_scan)
+    props_t = tilt_propagators(geom.ky, geom.kx, geom.thicknesses, props, tilts)
+    psi = _forward(psi0, cuts, props_t)
+    wave = fft2c(psi[-1] * cuts[:, -1, None])
+    intensity = numpy.sum(abs2(wave), axis=1)
+    loss = noise.loss(intensity, patterns, mask)
+    g_wave = 2. * noise_dloss_dI(noise, intensity, patterns, mask)[:, None] * wave
+    g = ifft2c(g_wave)
+    g_obj = numpy.zeros_like(obj)
+    for s in range(S - 1, -1, -1):
+        add_cutouts(g_obj[s], starts, numpy.sum(g * numpy.conj(psi[s]), axis=1))
+        g = g * numpy.conj(cuts[:, s, None])
+        if s > 0:
+            g = ifft2c(fft2c(g) * numpy.conj(props_t[s - 1])[:, None])
+    g_probe = ifft2c(numpy.sum(fft2c(g) * numpy.conj(filt), axis=0))
+    pf = fft2c(probe)[None] * filt
+    g_pos = []
+    for k in (geom.ky, geom.kx):
+        d = ifft2c(pf * -2.j * numpy.pi * k)
+        g_pos.append(numpy.sum(numpy.real(numpy.conj(g) * d), axis=(1, -1, -2)))
+    return loss, g_obj, g_probe, numpy.stack(g_pos, axis=-1)

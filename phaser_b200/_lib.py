@@ -66,6 +66,25 @@ class PhbStep(ctypes.Structure):
         ('grad_object', c_void_p), ('grad_probe', c_void_p), ('grad_pos', c_void_p),
         ('status', c_void_p), ('group_index', c_i32),
         ('group_patterns', c_void_p), ('event_begin', c_void_p), ('event_end', c_void_p),
+        ('grad_pos_scale', c_f32), ('group_loss', c_void_p),
+    ]
+
+
+PHB_OPTIM_SGD = 0
+PHB_OPTIM_ADAM = 1
+PHB_OPTIM_POLYAK = 2
+
+
+class PhbOptim(ctypes.Structure):
+    """Mirror of `phb_optim` (include/phaser_b200.h)."""
+    _fields_ = [
+        ('kind', c_i32), ('nesterov', c_i32),
+        ('param', c_void_p), ('grad', c_void_p), ('state1', c_void_p), ('state2', c_void_p),
+        ('update_out', c_void_p), ('n', c_i64), ('complex_elems', c_i32),
+        ('grad_scale', c_f32), ('lr', c_f32), ('momentum', c_f32), ('b1', c_f32), ('b2', c_f32),
+        ('eps', c_f32), ('eps_root', c_f32), ('count', c_i64), ('polyak_sq_norm', c_void_p),
+        ('polyak_scaling', c_f32), ('polyak_max_lr', c_f32), ('polyak_f_min', c_f32), ('polyak_eps', c_f32),
+        ('loss', c_f32),
     ]
 
 
@@ -99,6 +118,9 @@ _SIGNATURES = {
     'phb_solver_group_static': (c_i32, [ctypes.POINTER(PhbEngine), ctypes.POINTER(PhbStep), c_void_p, c_i32,
                                         c_void_p]),
     'phb_simulate_group': (c_i32, [ctypes.POINTER(PhbEngine), c_void_p, c_i32, c_void_p, c_void_p]),
+    'phb_optimizer_update': (c_i32, [ctypes.POINTER(PhbOptim), c_void_p]),
+    'phb_sq_norm_f32': (c_i32, [c_void_p, c_i64, c_f32, c_void_p, c_void_p]),
+    'phb_add_centred': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),

@@ -741,6 +741,8 @@ struct FinArgs {
     const int64_t *group;
     double *sums, *coef;
     float *pos_update, *grad_pos, *loss;
+    float grad_pos_scale;
+    double *group_loss;
 };
 
 __global__ void k_finalize(const FinArgs f) {
@@ -790,13 +792,20 @@ __global__ void k_finalize(const FinArgs f) {
         }
     }
     if (f.mode == MODE_GRAD) {
+        const double gs = f.grad_pos_scale != 0.f ? (double)f.grad_pos_scale : 1.0;
+        double lsum = 0.0;
         for (int b = tid; b < f.B; b += blockDim.x) {
             const int64_t p = f.group[b];
             if (pos && f.grad_pos) {
-                f.grad_pos[2 * p] = (float)sums[SI.pnum + 2 * b];
-                f.grad_pos[2 * p + 1] = (float)sums[SI.pnum + 2 * b + 1];
+                f.grad_pos[2 * p] = (float)(gs * sums[SI.pnum + 2 * b]);
+                f.grad_pos[2 * p + 1] = (float)(gs * sums[SI.pnum + 2 * b + 1]);
             }
             if (f.loss) f.loss[p] = (float)sums[SI.loss + b];
+            lsum += sums[SI.loss + b];
+        }
+        if (f.group_loss) {
+            for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+            if ((tid & 31) == 0) atomicAdd(f.group_loss, lsum);
         }
     }
     __syncthreads();
@@ -1379,6 +1388,8 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     f.pos_update = sp->pos_update;
     f.grad_pos = sp->grad_pos;
     f.loss = sp->loss;
+    f.grad_pos_scale = sp->grad_pos_scale;
+    f.group_loss = sp->group_loss;
     k_finalize<<<1, 256, 0, st>>>(f);
     if ((rc = check_launch())) return rc;
 
