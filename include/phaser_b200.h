@@ -232,9 +232,11 @@ int phb_solver_group_static(const phb_engine *e, const phb_step *st, const int64
  * optax semantics of phaser/engines/gradient/solvers.py:88-138 on device arrays:
  * d = grad_scale * grad; SGD (optax.trace momentum / Nesterov, then lr), Adam
  * (optax.scale_by_adam, |d|^2 second moment for complex d, then lr) or Polyak
- * (scale_by_learning_rate(scaling) then scale_by_polyak(max_lr, f_min, eps), with
- * *polyak_sq_norm = sum |scaling d|^2 over all of the solver's parameters); the
- * update is added to `param`, or written to `update_out` when that is non-NULL. */
+ * (scale_by_learning_rate(scaling) then scale_by_polyak(max_lr, f_min, eps): the
+ * stochastic Polyak step min((loss - f_min) / (q + eps), max_lr), or 0 when
+ * q + eps <= 2^-52, with q = *polyak_sq_norm = sum |scaling d|^2 over all of the
+ * solver's parameters and loss = *polyak_loss, both device float64); the update
+ * is added to `param`, or written to `update_out` when that is non-NULL. */
 #define PHB_OPTIM_SGD    0
 #define PHB_OPTIM_ADAM   1
 #define PHB_OPTIM_POLYAK 2
@@ -251,7 +253,10 @@ typedef struct phb_optim {
     float grad_scale, lr, momentum, b1, b2, eps, eps_root;
     int64_t count;            /* Adam: step count including this update (>= 1) */
     const double *polyak_sq_norm;
-    float polyak_scaling, polyak_max_lr, polyak_f_min, polyak_eps, loss;
+    const double *polyak_loss;
+    float polyak_scaling, polyak_max_lr, polyak_f_min, polyak_eps;
+    int32_t *status;          /* optional: set to status_code (if still -1) when an updated */
+    int32_t status_code;      /* parameter value is NaN or inf (run.py:281 check_finite) */
 } phb_optim;
 
 int phb_optimizer_update(const phb_optim *o, void *stream);

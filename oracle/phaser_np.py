@@ -712,3 +712,164 @@ def grad_model_grads(geom, probe, obj, group_scan, patterns, mask, props, tilts,
         d = ifft2c(pf * -2.j * numpy.pi * k)
         g_pos.append(numpy.sum(numpy.real(numpy.conj(g) * d), axis=(1, -1, -2)))
     return loss, g_obj, g_probe, numpy.stack(g_pos, axis=-1)
+
+
+# ---------------------------------------------------------------- gradient engine (a14)
+
+class OptaxNP:
+    """The optax chains of phaser/engines/gradient/solvers.py:88-138 restated in
+    numpy (optax is a third-party dependency of the reference; its published
+    update rules are restated here):
+
+    - 'sgd'        optax.trace(momentum, nesterov) then scale_by_learning_rate(lr,
+                   flip_sign=False); without momentum only the learning rate;
+    - 'adam'       optax.scale_by_adam(b1, b2, eps, eps_root, nesterov) (Kingma & Ba
+                   2015, with optax's Nesterov variant), second moment |d|^2;
+    - 'polyak_sgd' scale_by_learning_rate(scaling) then scale_by_polyak(max_lr,
+                   f_min, eps): the stochastic Polyak step (Loizou et al. 2021)
+                   min((loss - f_min) / (sum |u|^2 + eps), max_lr), 0 for a zero
+                   gradient.
+
+    `update(d, loss)` takes the descent directions d (a dict of arrays) and returns
+    the dict of updates the reference adds to its parameters (run.py:107-124)."""
+
+    def __init__(self, kind: str, props: t.Mapping[str, t.Any], params: t.Mapping[str, numpy.ndarray]):
+        self.kind = kind
+        self.p = dict(props)
+        self.count = 0
+        self.s1 = {k: numpy.zeros_like(v) for (k, v) in params.items()}
+        self.s2 = {k: numpy.zeros(v.shape, real_dtype(v.dtype)) for (k, v) in params.items()}
+
+    def update(self, d: t.Mapping[str, numpy.ndarray], loss: float) -> t.Dict[str, numpy.ndarray]:
+        p = self.p
+        out = {}
+        if self.kind == 'sgd':
+            lr, mom = p['learning_rate'], p.get('momentum')
+            for k, g in d.items():
+                if mom is None:
+                    out[k] = lr * g
+                    continue
+                self.s1[k] = g + mom * self.s1[k]
+                u = g + mom * self.s1[k] if p.get('nesterov', True) else self.s1[k]
+                out[k] = lr * u
+        elif self.kind == 'adam':
+            b1, b2 = p.get('b1', 0.9), p.get('b2', 0.999)
+            eps, eps_root = p.get('eps', 1e-8), p.get('eps_root', 0.0)
+            self.count += 1
+            c = self.count
+            for k, g in d.items():
+                self.s1[k] = b1 * self.s1[k] + (1. - b1) * g
+                self.s2[k] = b2 * self.s2[k] + (1. - b2) * abs2(g)
+                if p.get('nesterov', False):
+                    mh = b1 * self.s1[k] / (1. - b1 ** (c + 1)) + (1. - b1) * g / (1. - b1 ** c)
+                else:
+                    mh = self.s1[k] / (1. - b1 ** c)
+                nh = self.s2[k] / (1. - b2 ** c)
+                out[k] = p['learning_rate'] * mh / (numpy.sqrt(nh + eps_root) + eps)
+        elif self.kind == 'polyak_sgd':
+            u = {k: p.get('scaling', 1.0) * g for (k, g) in d.items()}
+            q = sum(float(numpy.sum(abs2(v), dtype=numpy.float64)) for v in u.values()) + p.get('eps', 0.0)
+            step = 0.0 if q <= 2. ** -52 else min((float(loss) - p['f_min']) / q, p['max_learning_rate'])
+            out = {k: (step * v).astype(v.dtype) for (k, v) in u.items()}
+        else:
+            raise ValueError(f"unknown gradient solver '{self.kind}'")
+        return {k: v.astype(d[k].dtype) for (k, v) in out.items()}
+
+
+@dataclasses.dataclass
+class GradientRun:
+    """Inputs and knobs of one gradient-engine run (GradientEnginePlan,
+    phaser/plan.py:135-141): `solvers` maps a tuple of variables to
+    (kind, props) as in the plan's `solvers` dict."""
+    solvers: t.Dict[t.Tuple[str, ...], t.Tuple[str, t.Dict[str, t.Any]]]
+    niter: int = 2
+    grouping: int = 64
+    seed: t.Any = 'seed'
+    noise: NoiseModel = dataclasses.field(default_factory=NoiseModel)
+    update_object: bool = True
+    update_probe: bool = True
+    update_positions: bool = False
+    bwlim_frac: t.Optional[float] = 2. / 3.
+
+
+_PER_ITER = ('positions', 'tilt')
+
+
+def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sampling, corner,
+                 obj_sampling, thicknesses, wavelength, tilt=None):
+    """Rescale + `niter` iterations of the gradient engine with sparse groupings
+    (phaser/engines/gradient/run.py:156-349): per group the model's gradients,
+    the descent directions -g / B (probe) and -g / (B sum|P|^2) (others), the
+    per-group solvers applied at once; positions updated once per iteration
+    from the gathered group directions, minus their mean.  Returns
+    (probe, object, scan, mean loss per iteration)."""
+    probe = probe.copy()
+    obj = obj.copy()
+    rdt = real_dtype(probe.dtype)
+    N = probe.shape[-1]
+    ky, kx = recip_grid(probe.shape[-2:], probe_sampling, dtype=rdt)
+    geom = Geometry(numpy.asarray(corner, numpy.float64), numpy.asarray(obj_sampling, numpy.float64),
+                    ky, kx, numpy.asarray(thicknesses))
+    props = make_propagators(ky, kx, probe_sampling, wavelength, thicknesses, run.bwlim_frac)
+    scan_shape = scan.shape[:-1]
+    flat_scan = scan.reshape(-1, 2).copy()
+    flat_pat = patterns.reshape(-1, N, N)
+    flat_tilt = None if tilt is None else tilt.reshape(-1, 2)
+
+    def flat(g):
+        return numpy.ravel_multi_index(tuple(g), scan_shape)
+
+    factors = []
+    for g in sparse_groupings(scan_shape, run.grouping, run.seed, 0):
+        idx = flat(g)
+        tl = None if flat_tilt is None else flat_tilt[idx]
+        factors.append(grad_dry_run(geom, probe, obj, flat_scan[idx], flat_pat[idx], props, tl))
+    probe = probe * numpy.sqrt(numpy.mean(numpy.concatenate(factors)))
+    probe_int = numpy.sum(abs2(probe))
+
+    params = {'object': obj, 'probe': probe, 'positions': flat_scan}
+    group_solvers, iter_solvers = [], []
+    for (vs, (kind, sp)) in run.solvers.items():
+        sol = (frozenset(vs), OptaxNP(kind, sp, {v: params[v] for v in vs}))
+        (iter_solvers if set(vs) <= set(_PER_ITER) else group_solvers).append(sol)
+    enabled = {'object': run.update_object, 'probe': run.update_probe, 'positions': run.update_positions}
+    iter_vars = {v for sol in group_solvers + iter_solvers for v in sol[0] if enabled.get(v, False)}
+
+    losses_out = []
+    for it in range(1, run.niter + 1):
+        iter_d = {'positions': numpy.zeros_like(flat_scan)} if 'positions' in iter_vars else {}
+        losses = []
+        for gi, g in enumerate(sparse_groupings(scan_shape, run.grouping, run.seed, it)):
+            idx = flat(g)
+            B = len(idx)
+            tl = None if flat_tilt is None else flat_tilt[idx]
+            L, g_obj, g_probe, g_pos = grad_model_grads(geom, probe, obj, flat_scan[idx], flat_pat[idx], mask,
+                                                        props, tl, run.noise)
+            d = {'object': -g_obj / (probe_int * B), 'probe': -g_probe / B,
+                 'positions': -g_pos / (probe_int * B)}
+            d = {k: v.astype(params[k].dtype) for (k, v) in d.items() if k in iter_vars}
+            if 'positions' in d:
+                iter_d['positions'][idx] = d['positions']
+            for (vs, sol) in group_solvers:
+                dd = {k: v for (k, v) in d.items() if k in vs}
+                if not dd:
+                    continue
+                upd = sol.update(dd, L)
+                if 'probe' in upd:
+                    probe = probe + upd['probe']
+                if 'object' in upd:
+                    obj = obj + upd['object']
+            if not (numpy.all(numpy.isfinite(obj)) and numpy.all(numpy.isfinite(probe))):
+                raise ValueError(f"NaN or inf encountered in object or probe, group {gi}")
+            losses.append(L)
+        loss = float(numpy.mean(losses))
+        for (vs, sol) in iter_solvers:
+            dd = {k: v for (k, v) in iter_d.items() if k in vs}
+            if not dd:
+                continue
+            upd = sol.update(dd, loss)
+            if 'positions' in upd:
+                u = upd['positions']
+                flat_scan = flat_scan + (u - numpy.mean(u, axis=0))
+        losses_out.append(loss)
+    return probe, obj, flat_scan.reshape(scan.shape), numpy.array(losses_out)

@@ -82,9 +82,9 @@ class PhbOptim(ctypes.Structure):
         ('param', c_void_p), ('grad', c_void_p), ('state1', c_void_p), ('state2', c_void_p),
         ('update_out', c_void_p), ('n', c_i64), ('complex_elems', c_i32),
         ('grad_scale', c_f32), ('lr', c_f32), ('momentum', c_f32), ('b1', c_f32), ('b2', c_f32),
-        ('eps', c_f32), ('eps_root', c_f32), ('count', c_i64), ('polyak_sq_norm', c_void_p),
+        ('eps', c_f32), ('eps_root', c_f32), ('count', c_i64), ('polyak_sq_norm', c_void_p), ('polyak_loss', c_void_p),
         ('polyak_scaling', c_f32), ('polyak_max_lr', c_f32), ('polyak_f_min', c_f32), ('polyak_eps', c_f32),
-        ('loss', c_f32),
+        ('status', c_void_p), ('status_code', c_i32),
     ]
 
 

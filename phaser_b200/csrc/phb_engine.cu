@@ -1506,6 +1506,10 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
     if (st->solver != PHB_SOLVER_GRAD && e->noise == PHB_NOISE_POISSON) return PHB_ERR_UNSUPPORTED;
     if (st->solver == PHB_SOLVER_GRAD && (st->flags & PHB_FLAG_UPDATE_OBJECT) && !st->grad_object)
         return PHB_ERR_INVALID_ARG;
+    if (st->solver == PHB_SOLVER_GRAD && (st->flags & PHB_FLAG_UPDATE_PROBE) && !st->grad_probe)
+        return PHB_ERR_INVALID_ARG;
+    if (st->solver == PHB_SOLVER_GRAD && (st->flags & PHB_FLAG_UPDATE_POSITION) && !st->grad_pos)
+        return PHB_ERR_INVALID_ARG;
     if ((st->flags & PHB_FLAG_UPDATE_POSITION) && st->solver != PHB_SOLVER_GRAD && !st->pos_update)
         return PHB_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;

@@ -31,10 +31,12 @@ __global__ void k_optim(const phb_optim o) {
     const double bc1n = 1.0 - pow((double)o.b1, (double)(o.count + 1));
     float polyak_step = 0.f;
     if (o.kind == PHB_OPTIM_POLYAK) {
-        const double sq = *o.polyak_sq_norm;
-        polyak_step = (float)fmin(((double)o.loss - (double)o.polyak_f_min) / (sq + (double)o.polyak_eps),
-                                  (double)o.polyak_max_lr);
+        // stochastic Polyak step size (Loizou et al., AISTATS 2021), capped at max_lr
+        const double q = *o.polyak_sq_norm + (double)o.polyak_eps;
+        polyak_step = q <= 0x1p-52 ? 0.f
+                                   : (float)fmin((*o.polyak_loss - (double)o.polyak_f_min) / q, (double)o.polyak_max_lr);
     }
+    bool bad = false;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < o.n; i += (int64_t)gridDim.x * blockDim.x) {
         float2 d = CPLX ? reinterpret_cast<const float2 *>(o.grad)[i] : make_float2(o.grad[i], 0.f);
         d = cscale(d, o.grad_scale);
@@ -73,11 +75,16 @@ __global__ void k_optim(const phb_optim o) {
             else o.update_out[i] = out.x;
         } else if (CPLX) {
             float2 *p = reinterpret_cast<float2 *>(o.param) + i;
-            *p = cadd(*p, out);
+            const float2 v = cadd(*p, out);
+            *p = v;
+            bad |= !finite2(v);
         } else {
-            o.param[i] += out.x;
+            const float v = o.param[i] + out.x;
+            o.param[i] = v;
+            bad |= !isfinite(v);
         }
     }
+    if (bad && o.status) atomicCAS(o.status, -1, o.status_code);
 }
 
 // param (n, 2) += upd - mean(upd) (run.py:115-118: position updates keep the scan centred)
@@ -141,7 +148,7 @@ int phb_optimizer_update(const phb_optim *o, void *stream) {
     if (o->kind < PHB_OPTIM_SGD || o->kind > PHB_OPTIM_POLYAK) return PHB_ERR_INVALID_ARG;
     if (o->kind == PHB_OPTIM_SGD && o->momentum != 0.f && !o->state1) return PHB_ERR_INVALID_ARG;
     if (o->kind == PHB_OPTIM_ADAM && (!o->state1 || !o->state2 || o->count < 1)) return PHB_ERR_INVALID_ARG;
-    if (o->kind == PHB_OPTIM_POLYAK && !o->polyak_sq_norm) return PHB_ERR_INVALID_ARG;
+    if (o->kind == PHB_OPTIM_POLYAK && (!o->polyak_sq_norm || !o->polyak_loss)) return PHB_ERR_INVALID_ARG;
     if (o->n == 0) return PHB_OK;
     if (o->complex_elems) k_optim<true><<<optim_grid(o->n), 256, 0, (cudaStream_t)stream>>>(*o);
     else k_optim<false><<<optim_grid(o->n), 256, 0, (cudaStream_t)stream>>>(*o);

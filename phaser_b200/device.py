@@ -178,7 +178,8 @@ class DeviceEngine:
              illum_reg_object=1e-2, illum_reg_probe=1e-2, gamma=1e-4, group_index: int = 0,
              grad_object: t.Optional[torch.Tensor] = None, grad_probe: t.Optional[torch.Tensor] = None,
              grad_pos: t.Optional[torch.Tensor] = None, loss: t.Optional[torch.Tensor] = None,
-             group_patterns: t.Optional[torch.Tensor] = None, events: t.Optional[t.Tuple[int, int]] = None) -> None:
+             group_patterns: t.Optional[torch.Tensor] = None, events: t.Optional[t.Tuple[int, int]] = None,
+             grad_pos_scale: float = 1.0, group_loss: t.Optional[torch.Tensor] = None) -> None:
         st = _lib.PhbStep()
         st.solver, st.flags = SOLVERS[solver], int(flags)
         st.beta_object, st.beta_probe = float(beta_object), float(beta_probe)
@@ -189,6 +190,7 @@ class DeviceEngine:
         st.grad_object, st.grad_probe, st.grad_pos = _ptr(grad_object), _ptr(grad_probe), _ptr(grad_pos)
         st.status, st.group_index = self.status.data_ptr(), int(group_index)
         st.group_patterns = _ptr(group_patterns)
+        st.grad_pos_scale, st.group_loss = float(grad_pos_scale), _ptr(group_loss)
         if events is not None:
             st.event_begin, st.event_end = events
         _lib.call('phb_solver_group', self._eref, ctypes.byref(st), group.data_ptr(), int(B), _stream())

@@ -1,0 +1,346 @@
+"""Gradient engine on the B200 kernels.
+
+Drop-in for `phaser.engines.gradient.run:run_engine`
+(phaser/engines/gradient/run.py:156-349).  The reference differentiates its
+forward model with jax; here the fused kernel evaluates the loss and its
+hand-written adjoint in one launch per mini-batch (phb_solver_group with
+PHB_SOLVER_GRAD), and the optax solvers of phaser/engines/gradient/solvers.py
+run as device kernels (phb_optimizer_update).  Structure per iteration, as in
+the reference:
+
+  per group   loss + gradients -> descent directions -g / B (probe) and
+              -g / (B sum|P|^2) (object, positions) -> every per-group solver
+              (object / probe) updates its variables -> group constraints
+  per iter    mean loss; per-iteration solvers (positions) from the gathered
+              group directions, update minus its mean; iteration constraints;
+              positions checked against the object.
+
+Cost regularisers are not implemented yet (NotImplementedError), nor tilt
+updates.
+"""
+from __future__ import annotations
+
+import ctypes
+import logging
+import typing as t
+
+import numpy
+import torch
+
+from .. import plan as P
+from .. import _lib
+from ..constraints import build_constraints
+from ..device import DeviceEngine
+from ..groups import GroupManager
+from .conventional import _call, _noise, _object_sampling
+
+logger = logging.getLogger(__name__)
+
+_PER_ITER_VARS = frozenset({'positions', 'tilt'})
+_KINDS = {'sgd': _lib.PHB_OPTIM_SGD, 'adam': _lib.PHB_OPTIM_ADAM, 'polyak_sgd': _lib.PHB_OPTIM_POLYAK}
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _floats(x: torch.Tensor) -> torch.Tensor:
+    return torch.view_as_real(x) if x.is_complex() else x
+
+
+class DeviceSolver:
+    """One gradient solver (phaser/engines/gradient/solvers.py:48-138) with its
+    optax state on the device.  `params` maps each variable to the device tensor
+    it updates in place (positions: the update is written to a scratch tensor and
+    added minus its mean, run.py:115-118)."""
+
+    def __init__(self, kind: str, props: t.Any, params: t.Mapping[str, torch.Tensor]):
+        self.kind, self.props = kind, props
+        self.params = frozenset(params)
+        self.count = 0
+        self.hyper: t.Dict[str, float] = {}
+        if kind == 'sgd':
+            self._sched = {'learning_rate': P.get(props, 'learning_rate')}
+            if P.get(props, 'momentum', None) is not None:
+                self._sched['momentum'] = P.get(props, 'momentum')
+        elif kind == 'adam':
+            self._sched = {'learning_rate': P.get(props, 'learning_rate')}
+        else:
+            self._sched = {'max_learning_rate': P.get(props, 'max_learning_rate'),
+                           'scaling': P.get(props, 'scaling', 1.0)}
+        self._sched = {k: P.process_schedule(v) for (k, v) in self._sched.items()}
+        self.state1 = {k: torch.zeros_like(v) for (k, v) in params.items()
+                       if kind == 'adam' or (kind == 'sgd' and 'momentum' in self._sched)}
+        self.state2 = {k: torch.zeros(v.shape, dtype=torch.float32, device=v.device) for (k, v) in params.items()
+                       if kind == 'adam'}
+        dev = next(iter(params.values())).device
+        self.sq_norm = torch.zeros((1,), dtype=torch.float64, device=dev)
+
+    @classmethod
+    def name(cls) -> str:
+        return 'gradient'
+
+    def update_for_iter(self, fargs) -> None:
+        """Hyper-parameter schedules are evaluated once per iteration (solvers.py:75-80)."""
+        self.hyper = {k: f(fargs) for (k, f) in self._sched.items()}
+
+    def update(self, params: t.Mapping[str, torch.Tensor], grads: t.Mapping[str, t.Tuple[torch.Tensor, float]],
+               loss: torch.Tensor, *, update_out: t.Optional[t.Mapping[str, torch.Tensor]] = None,
+               status: t.Optional[torch.Tensor] = None, status_code: int = 0) -> None:
+        """Apply one optax update: grads[k] = (g, scale) with direction d = scale * g.
+        `loss` is a device float64 scalar (the Polyak step reads it on the device)."""
+        p = self.props
+        self.count += 1
+        if self.kind == 'polyak_sgd':
+            self.sq_norm.zero_()
+            for k, (g, scale) in grads.items():
+                gf = _floats(g)
+                _lib.call('phb_sq_norm_f32', gf.data_ptr(), gf.numel(), float(scale * self.hyper['scaling']),
+                          self.sq_norm.data_ptr(), _stream())
+        for k, (g, scale) in grads.items():
+            o = _lib.PhbOptim()
+            o.kind = _KINDS[self.kind]
+            o.nesterov = int(bool(P.get(p, 'nesterov', self.kind == 'sgd')))
+            prm = params[k]
+            out = None if update_out is None else update_out.get(k)
+            o.param = 0 if out is not None else prm.data_ptr()
+            o.update_out = 0 if out is None else out.data_ptr()
+            o.grad = g.data_ptr()
+            o.complex_elems = int(prm.is_complex())
+            o.n = prm.numel()
+            o.grad_scale = float(scale)
+            if k in self.state1:
+                o.state1 = self.state1[k].data_ptr()
+            if k in self.state2:
+                o.state2 = self.state2[k].data_ptr()
+            o.lr = float(self.hyper.get('learning_rate', 0.0))
+            o.momentum = float(self.hyper.get('momentum', 0.0))
+            o.b1, o.b2 = float(P.get(p, 'b1', 0.9)), float(P.get(p, 'b2', 0.999))
+            o.eps, o.eps_root = float(P.get(p, 'eps', 1e-8)), float(P.get(p, 'eps_root', 0.0))
+            o.count = self.count
+            if self.kind == 'polyak_sgd':
+                o.polyak_sq_norm, o.polyak_loss = self.sq_norm.data_ptr(), loss.data_ptr()
+                o.polyak_scaling = float(self.hyper['scaling'])
+                o.polyak_max_lr = float(self.hyper['max_learning_rate'])
+                o.polyak_f_min = float(P.get(p, 'f_min'))
+                o.polyak_eps = float(P.get(p, 'eps', 0.0))
+            if status is not None and out is None:
+                o.status, o.status_code = status.data_ptr(), int(status_code)
+            _lib.call('phb_optimizer_update', ctypes.byref(o), _stream())
+
+
+def process_solvers(props) -> t.Tuple[t.FrozenSet[str], t.List[t.Tuple[t.FrozenSet[str], str, t.Any]],
+                                      t.List[t.Tuple[t.FrozenSet[str], str, t.Any]]]:
+    """Split the plan's solvers into per-group and per-iteration solvers, with the
+    reference's errors for duplicates and mixed sets (run.py:29-65)."""
+    seen, duplicate = set(), set()
+    group, per_iter = [], []
+    solvers = P.get(props, 'solvers', {}) or {}
+    for key, hook in dict(solvers).items():
+        vs = P.recons_vars(key)
+        if not vs:
+            continue
+        duplicate |= vs & seen
+        seen |= vs
+        kind, sp = P.gradient_solver(hook)
+        if vs <= _PER_ITER_VARS:
+            per_iter.append((vs, kind, sp))
+            continue
+        if vs & _PER_ITER_VARS:
+            raise ValueError(f"The same solver can't handle both per-iteration "
+                             f"({', '.join(map(repr, sorted(vs & _PER_ITER_VARS)))}) and per-group "
+                             f"({', '.join(map(repr, sorted(vs - _PER_ITER_VARS)))}) variables")
+        group.append((vs, kind, sp))
+    if duplicate:
+        raise ValueError(f"Duplicate solvers for variable(s) {', '.join(map(repr, sorted(duplicate)))}.")
+    return frozenset(seen), group, per_iter
+
+
+class GradientEngine:
+    """One gradient-engine run on the device: construction uploads the state,
+    `presolve()` rescales the probe, `iteration(i)` runs one iteration and
+    `finish()` writes the result back into the host state."""
+
+    def __init__(self, args: t.Mapping[str, t.Any], props: t.Any, *,
+                 patterns_on_device: t.Optional[torch.Tensor] = None):
+        state = args['state']
+        data = args['data']
+        self.state = state
+        self.observer = args.get('observer', None)
+        dtype = numpy.dtype(args.get('dtype', numpy.float32))
+        if dtype != numpy.float32:
+            raise NotImplementedError("the B200 backend computes in float32/complex64 (plan dtype 'float32')")
+        if P.get(props, 'regularizers', None):
+            raise NotImplementedError("cost regularizers are not implemented by the B200 backend")
+        self.noise = _noise(props)
+        self.all_vars, group_specs, iter_specs = process_solvers(props)
+        self.niter = int(P.get(props, 'niter', 10))
+        grouping = int(P.get(props, 'grouping', None) or 64)
+        self.compact = bool(P.get(props, 'compact', False))
+        self.flags = {
+            'probe': P.process_flag(P.get(props, 'update_probe', True)),
+            'object': P.process_flag(P.get(props, 'update_object', True)),
+            'positions': P.process_flag(P.get(props, 'update_positions', False)),
+            'tilt': P.process_flag(P.get(props, 'update_tilt', False)),
+        }
+        self.shuffle_groups = P.process_flag(P.get(props, 'shuffle_groups', None) or not self.compact)
+
+        probe0 = numpy.asarray(state.probe.data)
+        obj0 = numpy.asarray(state.object.data)
+        self.scan0 = numpy.asarray(state.scan)
+        if probe0.dtype != numpy.complex64 or obj0.dtype != numpy.complex64:
+            raise TypeError("object and probe must be complex64")
+        self.eng = eng = DeviceEngine(
+            probe=probe0, obj=obj0, scan=self.scan0,
+            patterns=None if patterns_on_device is not None else numpy.asarray(data.patterns),
+            mask=numpy.asarray(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
+            obj_sampling=_object_sampling(state.object.sampling), thicknesses=numpy.asarray(state.object.thicknesses),
+            wavelength=float(state.wavelength), tilt=None if state.tilt is None else numpy.asarray(state.tilt),
+            noise=self.noise, bwlim_frac=P.get(props, 'bwlim_frac', 2 / 3), group_max=grouping,
+            patterns_on_device=patterns_on_device)
+        self.params = {'object': eng.object, 'probe': eng.probe, 'positions': eng.scan}
+        if 'tilt' in self.all_vars:
+            self.params['tilt'] = eng.tilt
+        self.group_solvers = [DeviceSolver(k, sp, {v: self.params[v] for v in vs}) for (vs, k, sp) in group_specs]
+        self.iter_solvers = [DeviceSolver(k, sp, {v: self.params[v] for v in vs}) for (vs, k, sp) in iter_specs]
+        self.group_cons = build_constraints(P.get(props, 'group_constraints', []) or [], eng, state, per_group=True)
+        self.iter_cons = build_constraints(P.get(props, 'iter_constraints', []) or [], eng, state, per_group=False)
+        self.groups = GroupManager(self.scan0.shape[:-1], grouping, self.compact, seed=args.get('seed', None))
+
+        dev = eng.device
+        self.grad_object = torch.zeros_like(eng.object) if 'object' in self.all_vars else None
+        self.grad_probe = torch.zeros_like(eng.probe) if 'probe' in self.all_vars else None
+        self.grad_pos = torch.zeros_like(eng.scan) if 'positions' in self.all_vars else None
+        self.pos_step = torch.zeros_like(eng.scan)
+        self.losses = torch.zeros((len(self.groups),), dtype=torch.float64, device=dev)
+        self.loss_mean = torch.zeros((1,), dtype=torch.float64, device=dev)
+        self.loss_host = torch.zeros((2,), dtype=torch.float64).pin_memory()
+        self.status_host = torch.zeros((1,), dtype=torch.int32).pin_memory()
+        self.probe_int = 0.0
+        self.start_i = int(state.iter.total_iter)
+        self.fused_events: t.Optional[t.List[t.Tuple[int, int]]] = None
+        _call(self.observer, 'init_engine', state, recons_name=args.get('recons_name', ''), plan=props,
+              noise_model=self.noise.kind)
+
+    def presolve(self) -> float:
+        """Probe intensity rescale over the first groups (run.py:199-212, 413-438)."""
+        first = self.groups.iter(self.scan0 if self.compact else None, 0)
+        gt, sizes = self.eng.group_tensor([self.groups.flat(g) for g in first])
+        rescale = self.eng.presolve(gt, sizes, 'lsqml', gradient_form=True)
+        logger.info(f"Rescaling initial probe intensity by {rescale:.2e}")
+        self.eng.probe.mul_(float(numpy.sqrt(rescale)))
+        self.eng.probe_changed()
+        self.probe_int = float(torch.sum(torch.view_as_real(self.eng.probe).double() ** 2))
+        _call(self.observer, 'start_engine', self.state)
+        return rescale
+
+    def iteration(self, i: int, *, sync: bool = True) -> t.Optional[float]:
+        """Run iteration i (1-based).  With sync=True, wait for the device, raise on
+        NaN / positions outside the object and return the mean loss."""
+        eng, state = self.eng, self.state
+        state.iter.engine_iter = i
+        state.iter.total_iter = self.start_i + i
+        fargs = {'state': state, 'niter': self.niter}
+        iter_vars = self.all_vars & {k for (k, f) in self.flags.items() if f(fargs)}
+        if 'tilt' in iter_vars:
+            raise NotImplementedError("tilt updates are not implemented by the B200 backend")
+        for sol in self.group_solvers + self.iter_solvers:
+            sol.update_for_iter(fargs)
+        flags = ((_lib.PHB_FLAG_UPDATE_OBJECT if 'object' in iter_vars else 0)
+                 | (_lib.PHB_FLAG_UPDATE_PROBE if 'probe' in iter_vars else 0)
+                 | (_lib.PHB_FLAG_UPDATE_POSITION if 'positions' in iter_vars else 0))
+        scan_host = eng.scan.cpu().numpy().reshape(self.scan0.shape) if self.compact else None
+        glist = self.groups.iter(scan_host, i, self.shuffle_groups(fargs))
+        gt, sizes = eng.group_tensor([self.groups.flat(g) for g in glist])
+        if self.losses.numel() < len(sizes):
+            self.losses = torch.zeros((len(sizes),), dtype=torch.float64, device=eng.device)
+        losses = self.losses[:len(sizes)]
+        losses.zero_()
+        eng.status.fill_(-1)
+        probe_int = self.probe_int
+        for gi, B in enumerate(sizes):
+            if 'object' in iter_vars:
+                self.grad_object.zero_()
+            if 'probe' in iter_vars:
+                self.grad_probe.zero_()
+            ev = None
+            if self.fused_events is not None:
+                ev = _new_event_pair()
+                self.fused_events.append(ev)
+            eng.step('grad', gt[gi], B, flags=flags, group_index=gi, events=ev,
+                     grad_object=self.grad_object if 'object' in iter_vars else None,
+                     grad_probe=self.grad_probe if 'probe' in iter_vars else None,
+                     grad_pos=self.grad_pos if 'positions' in iter_vars else None,
+                     grad_pos_scale=-1.0 / (probe_int * B), group_loss=losses[gi:gi + 1])
+            dirs = {}
+            if 'object' in iter_vars:
+                dirs['object'] = (self.grad_object, -1.0 / (probe_int * B))
+            if 'probe' in iter_vars:
+                dirs['probe'] = (self.grad_probe, -1.0 / B)
+            for sol in self.group_solvers:
+                d = {k: v for (k, v) in dirs.items() if k in sol.params}
+                if d:
+                    sol.update(self.params, d, losses[gi:gi + 1], status=eng.status, status_code=gi)
+            if 'probe' in iter_vars and any('probe' in s.params for s in self.group_solvers):
+                eng.probe_changed()
+            for con in self.group_cons:
+                con.apply_group()
+        torch.mean(losses, dim=0, keepdim=True, out=self.loss_mean)
+        for sol in self.iter_solvers:
+            d = {k: (self.grad_pos, 1.0) for k in sol.params if k == 'positions' and 'positions' in iter_vars}
+            if not d:
+                continue
+            sol.update(self.params, d, self.loss_mean, update_out={'positions': self.pos_step})
+            _lib.call('phb_add_centred', eng.scan.data_ptr(), self.pos_step.data_ptr(), eng.n_pos, _stream())
+        for con in self.iter_cons:
+            con.apply_iter()
+        self.loss_host[:1].copy_(self.loss_mean, non_blocking=True)
+        self.status_host.copy_(eng.status, non_blocking=True)
+        if not sync:
+            return None
+        torch.cuda.current_stream().synchronize()
+        return self.check(i, 'positions' in iter_vars)
+
+    def check(self, i: int, it_pos: bool = True) -> float:
+        state, eng = self.state, self.eng
+        bad_group = int(self.status_host[0])
+        if bad_group >= _lib.PHB_STATUS_INTERNAL:
+            raise RuntimeError(f"internal error: fused kernel aborted in group {bad_group - _lib.PHB_STATUS_INTERNAL}")
+        if bad_group >= 0:
+            raise ValueError(f"NaN or inf encountered in object or probe, group {bad_group}")
+        if it_pos:
+            scan = eng.scan.cpu().numpy()
+            lo, hi = eng.obj_sampling.check_bounds(numpy.asarray(eng.probe_extent()) / 2.)
+            outside = numpy.any((scan < lo) | (scan > hi), axis=-1)
+            if numpy.any(outside):
+                raise ValueError(f"{int(numpy.sum(outside))}/{eng.n_pos} probe positions completely outside object")
+        loss = float(self.loss_host[0])
+        state.progress.iters = numpy.concatenate([state.progress.iters, [i + self.start_i]])
+        state.progress.detector_errors = numpy.concatenate([state.progress.detector_errors, [loss]])
+        _call(self.observer, 'update_iteration', state, i, self.niter, loss)
+        return loss
+
+    def finish(self):
+        probe, obj, scan = self.eng.host_state()
+        self.state.probe.data = probe
+        self.state.object.data = obj
+        self.state.scan = scan.astype(self.scan0.dtype)
+        _call(self.observer, 'finish_engine', self.state)
+        return self.state
+
+
+def _new_event_pair() -> t.Tuple[int, int]:
+    a, b = ctypes.c_void_p(), ctypes.c_void_p()
+    _lib.call('phb_event_create', ctypes.byref(a))
+    _lib.call('phb_event_create', ctypes.byref(b))
+    return a.value, b.value
+
+
+def run_engine(args: t.Mapping[str, t.Any], props: t.Any) -> t.Any:
+    """Run a gradient engine; returns the (updated) ReconsState.
+    Signature of phaser.engines.gradient.run:run_engine (run.py:156)."""
+    eng = GradientEngine(args, props)
+    eng.presolve()
+    for i in range(1, eng.niter + 1):
+        eng.iteration(i)
+    return eng.finish()

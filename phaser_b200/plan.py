@@ -71,6 +71,34 @@ class MomentumPositionSolverProps:
 
 
 @dataclasses.dataclass(eq=False)
+class SGDSolverPlan:
+    """phaser/plan.py:144-147."""
+    learning_rate: t.Any
+    momentum: t.Any = None
+    nesterov: bool = True
+
+
+@dataclasses.dataclass(eq=False)
+class AdamSolverPlan:
+    """phaser/plan.py:150-158."""
+    learning_rate: t.Any
+    b1: float = 0.9
+    b2: float = 0.999
+    eps: float = 1.0e-8
+    eps_root: float = 0.0
+    nesterov: bool = False
+
+
+@dataclasses.dataclass(eq=False)
+class PolyakSGDSolverPlan:
+    """phaser/plan.py:161-165."""
+    max_learning_rate: t.Any
+    f_min: float
+    scaling: t.Any = 1.0
+    eps: float = 0.0
+
+
+@dataclasses.dataclass(eq=False)
 class HookSpec:
     """A resolved hook: `type` is the registry name ('lsqml', 'amplitude', ...)."""
     type: str
@@ -100,15 +128,39 @@ class ConventionalEnginePlan:
     send_every_group: bool = False
 
 
+@dataclasses.dataclass(eq=False)
+class GradientEnginePlan:
+    """Fields of phaser's GradientEnginePlan (phaser/plan.py:43-73, 135-141) that the engine reads."""
+    solvers: t.Dict[t.Any, t.Any] = dataclasses.field(default_factory=dict)
+    noise_model: t.Any = dataclasses.field(default_factory=lambda: HookSpec('amplitude', AmplitudeNoisePlan()))
+    regularizers: t.List[t.Any] = dataclasses.field(default_factory=list)
+    group_constraints: t.List[t.Any] = dataclasses.field(default_factory=list)
+    iter_constraints: t.List[t.Any] = dataclasses.field(default_factory=list)
+    niter: int = 10
+    grouping: t.Optional[int] = None
+    compact: bool = False
+    shuffle_groups: t.Any = None
+    buffer_n_groups: int = 2
+    update_probe: t.Any = True
+    update_object: t.Any = True
+    update_positions: t.Any = False
+    update_tilt: t.Any = False
+    bwlim_frac: t.Optional[float] = 2 / 3
+    send_every_group: bool = False
+
+
 _NOISE_DEFAULTS = {'amplitude': AmplitudeNoisePlan, 'anscombe': AnscombeNoisePlan, 'poisson': PoissonNoisePlan}
 _SOLVER_DEFAULTS = {'lsqml': LSQMLSolverPlan, 'epie': EPIESolverPlan}
 _POS_DEFAULTS = {'momentum': MomentumPositionSolverProps, 'steepest_descent': SteepestDescentPositionSolverProps}
+_GRAD_SOLVER_DEFAULTS = {'sgd': SGDSolverPlan, 'adam': AdamSolverPlan, 'polyak_sgd': PolyakSGDSolverPlan}
 _REF_CLASS_NAMES = {
     'AmplitudeNoiseModel': 'amplitude', 'AnscombeNoiseModel': 'anscombe', 'PoissonNoiseModel': 'poisson',
     'LSQMLSolver': 'lsqml', 'EPIESolver': 'epie',
     'MomentumPositionSolver': 'momentum', 'SteepestDescentPositionSolver': 'steepest_descent',
     'ClampObjectAmplitude': 'clamp_object_amplitude', 'LimitProbeSupport': 'limit_probe_support',
+    'SGDSolver': 'sgd', 'AdamSolver': 'adam', 'PolyakSGDSolver': 'polyak_sgd',
 }
+RECONS_VARS = ('object', 'probe', 'positions', 'tilt')
 
 
 def resolve_hook(hook: t.Any, defaults: t.Mapping[str, type]) -> t.Tuple[str, t.Any]:
@@ -150,6 +202,22 @@ def solver(hook) -> t.Tuple[str, t.Any]:
 
 def position_solver(hook) -> t.Optional[t.Tuple[str, t.Any]]:
     return None if hook is None else resolve_hook(hook, _POS_DEFAULTS)
+
+
+def gradient_solver(hook) -> t.Tuple[str, t.Any]:
+    return resolve_hook(hook, _GRAD_SOLVER_DEFAULTS)
+
+
+def recons_vars(key: t.Any) -> t.FrozenSet[str]:
+    """A `solvers` key: a comma-separated string or an iterable of variable
+    names (phaser/types.py:280-302)."""
+    if isinstance(key, str):
+        key = tuple(v.strip() for v in key.split(','))
+    out = frozenset(str(v) for v in key)
+    bad = out - set(RECONS_VARS)
+    if bad:
+        raise ValueError(f"unknown reconstruction variable(s) {sorted(bad)}; expected {RECONS_VARS}")
+    return out
 
 
 def process_flag(flag: t.Any) -> t.Callable[[t.Mapping[str, t.Any]], bool]:
