@@ -268,6 +268,43 @@ int phb_sq_norm_f32(const float *x, int64_t n, float scale, double *out, void *s
  * (phaser/engines/gradient/run.py:115-118). */
 int phb_add_centred(float *param, const float *update, int64_t n, void *stream);
 
+/* ------------------------------------------------------------- constraints
+ * RegularizeLayers (phaser/engines/common/regularizers.py:86-132): for every object
+ * pixel, O <- weight * exp(convolve1d(log O, taps, axis=0, mode='nearest'))
+ * + (1 - weight) * O over the S slices; `taps` (n_taps odd, device float32) are the
+ * normalised Gaussian the reference builds.  S <= 96. */
+int phb_regularize_layers_c64(void *obj, int64_t S, int64_t H, int64_t W, const float *taps, int32_t n_taps,
+                              float weight, void *stream);
+
+/* ObjLowPass / ObjGaussian (regularizers.py:135-192): per slice
+ * O <- ifft2(filter * fft2(O)) with phaser's centred transforms (the centring
+ * shifts cancel), `filter` (H, W) float32 in numpy.fft.fftfreq order on the
+ * device, any H and W.  `scratch`: phb_object_filter_scratch_bytes(S, H, W). */
+size_t phb_object_filter_scratch_bytes(int64_t S, int64_t H, int64_t W);
+int phb_object_filter_c64(void *obj, int64_t S, int64_t H, int64_t W, const float *filter, void *scratch,
+                          void *stream);
+
+/* RemovePhaseRamp (regularizers.py:67-83, phaser/utils/image.py:30-55): per slice,
+ * the least-squares plane p0 + p1 x + p2 y of angle(O) over the region rows
+ * [y0, y1) and columns [x0, x1) is removed from the phase; |O| is kept.
+ * `sums`: device float64 scratch of 3 S values. */
+int phb_remove_phase_ramp_c64(void *obj, int64_t S, int64_t H, int64_t W, int64_t y0, int64_t y1, int64_t x0,
+                              int64_t x1, double *sums, void *stream);
+
+/* Cost regularisers of the gradient engine on the object (regularizers.py:195-351):
+ * obj_l1 sum|O-1|, obj_l2 sum|O-1|^2, obj_phase_l1 sum|angle O|, obj_tikh
+ * sum|diff_x O|^2 + |diff_y O|^2, obj_tv sum sqrt(|g_y|^2 + |g_x|^2 + tv_eps)
+ * (forward differences, zero at the far edge), layers_tikh sum|diff_z O|^2,
+ * layers_tv sum|diff_z O|; each weighted by its cost, all by `scale` (the
+ * group's share B / n_pos).  Adds the total to *loss (device float64) and, if
+ * `grad` (S, H, W complex64) is non-NULL, dL/dRe + i dL/dIm to it. */
+typedef struct phb_obj_reg {
+    float l1, l2, phase_l1, tikh, tv, tv_eps, layers_tikh, layers_tv, scale;
+} phb_obj_reg;
+
+int phb_object_regularizers(const void *obj, int64_t S, int64_t H, int64_t W, const phb_obj_reg *reg, void *grad,
+                            double *loss, void *stream);
+
 /* Per-iteration position update (phaser/engines/conventional/run.py:95-110 with
  * phaser/engines/common/position_correction.py): subtract mean, momentum or
  * steepest-descent step with norm clipping, subtract mean, scan += update, and

@@ -790,6 +790,8 @@ class GradientRun:
     update_probe: bool = True
     update_positions: bool = False
     bwlim_frac: t.Optional[float] = 2. / 3.
+    regularizers: t.Dict[str, float] = dataclasses.field(default_factory=dict)   # name -> cost
+    tv_eps: float = 1e-8
 
 
 _PER_ITER = ('positions', 'tilt')
@@ -845,6 +847,11 @@ def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sa
             tl = None if flat_tilt is None else flat_tilt[idx]
             L, g_obj, g_probe, g_pos = grad_model_grads(geom, probe, obj, flat_scan[idx], flat_pat[idx], mask,
                                                         props, tl, run.noise)
+            if run.regularizers:
+                # cost regularisers join the loss and the object gradient (gradient/run.py:398-403)
+                r_cost, r_grad = obj_regularizer_costs(obj, run.regularizers, B / flat_scan.shape[0], run.tv_eps)
+                L = L + r_cost
+                g_obj = g_obj + r_grad
             d = {'object': -g_obj / (probe_int * B), 'probe': -g_probe / B,
                  'positions': -g_pos / (probe_int * B)}
             d = {k: v.astype(params[k].dtype) for (k, v) in d.items() if k in iter_vars}
@@ -873,3 +880,143 @@ def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sa
                 flat_scan = flat_scan + (u - numpy.mean(u, axis=0))
         losses_out.append(loss)
     return probe, obj, flat_scan.reshape(scan.shape), numpy.array(losses_out)
+
+
+# ---------------------------------------------------------------- constraints (a17)
+
+def layers_taps(thicknesses, sigma: float, dtype=numpy.float32) -> numpy.ndarray:
+    """Normalised Gaussian taps along z over +-2 sigma, layers taken as equally
+    spaced at the mean thickness (regularizers.py:99-108)."""
+    spacing = numpy.mean(thicknesses)
+    r = int(numpy.ceil(2. * sigma / spacing))
+    n = 2 * r + 1
+    zs = ((numpy.arange(n) - (n - 1) // 2) * spacing).astype(dtype)
+    taps = numpy.exp(-(zs / sigma) ** 2 / 2.)
+    return (taps / numpy.sum(taps)).astype(dtype)
+
+
+def regularize_layers(obj, thicknesses, sigma: float, weight: float):
+    """RegularizeLayers (regularizers.py:86-132): smooth log(O) along z with the
+    Gaussian taps, edges clamped (scipy 'nearest'), blend with weight."""
+    if len(thicknesses) < 2:
+        return obj
+    taps = layers_taps(thicknesses, sigma, real_dtype(obj.dtype))
+    r = (len(taps) - 1) // 2
+    lg = numpy.log(obj)
+    S = obj.shape[0]
+    conv = numpy.zeros_like(lg)
+    for s in range(S):
+        for j, w in enumerate(taps):
+            conv[s] += w * lg[min(max(s + r - j, 0), S - 1)]
+    return (weight * numpy.exp(conv) + (1 - weight) * obj).astype(obj.dtype)
+
+
+def low_pass_filter(shape, max_freq: float) -> numpy.ndarray:
+    """ObjLowPass mask (regularizers.py:140-149): |k|^2 <= max_freq^2, k in 1/px."""
+    ky, kx = numpy.meshgrid(numpy.fft.fftfreq(shape[0], 1.0), numpy.fft.fftfreq(shape[1], 1.0), indexing='ij')
+    return (ky ** 2 + kx ** 2 <= max_freq ** 2)
+
+
+def gaussian_filter(shape, sampling, sigma: float, weight: float, dtype=numpy.float32) -> numpy.ndarray:
+    """ObjGaussian filter (regularizers.py:169-180): 1 - weight (1 - exp(-2 pi^2 sigma^2 k^2))."""
+    ky = numpy.fft.fftfreq(shape[0], sampling[0]).astype(dtype)
+    kx = numpy.fft.fftfreq(shape[1], sampling[1]).astype(dtype)
+    ky, kx = numpy.meshgrid(ky, kx, indexing='ij')
+    filt = numpy.exp(-(2 * numpy.pi ** 2 * sigma ** 2) * (ky ** 2 + kx ** 2)).astype(dtype)
+    return (1. - weight * (1. - filt)).astype(dtype)
+
+
+def fourier_filter(obj, filt):
+    """O <- ifft2(filt * fft2(O)) per slice (regularizers.py:157-161, 188-192)."""
+    return ifft2c(filt * fft2c(obj)).astype(obj.dtype)
+
+
+def region_crop(shape, corner, sampling, region_min, region_max):
+    """Rows / columns of ObjectSampling.get_region_crop (object.py:367-378) with pad 0."""
+    if region_min is None:
+        lo = (0, 0)
+    else:
+        lo = numpy.ceil((numpy.asarray(region_min) - corner) / sampling).astype(int)
+    if region_max is None:
+        hi = shape
+    else:
+        hi = numpy.floor((numpy.asarray(region_max) - corner) / sampling).astype(int) + 1
+    return (max(int(lo[0]), 0), min(int(hi[0]), shape[0])), (max(int(lo[1]), 0), min(int(hi[1]), shape[1]))
+
+
+def remove_phase_ramp(obj, rows, cols):
+    """RemovePhaseRamp (regularizers.py:67-83, utils/image.py:30-55): per slice,
+    least-squares plane a + b x + c y of the phase over the region, subtracted."""
+    ph = numpy.angle(obj)
+    yy, xx = numpy.indices(obj.shape[-2:], dtype=float)
+    sel = numpy.zeros(obj.shape[-2:], bool)
+    sel[rows[0]:rows[1], cols[0]:cols[1]] = True
+    A = numpy.stack([numpy.ones(int(sel.sum())), xx[sel], yy[sel]], axis=-1)
+    out = numpy.empty_like(ph)
+    for s in range(obj.shape[0]):
+        p = numpy.linalg.lstsq(A, ph[s][sel].astype(numpy.float64), rcond=None)[0]
+        out[s] = (ph[s] - (p[0] + p[1] * xx + p[2] * yy)).astype(ph.dtype)
+    return (numpy.abs(obj) * numpy.exp(1j * out)).astype(obj.dtype)
+
+
+# ------------------------------------------------------- cost regularisers (f1)
+
+def obj_regularizer_costs(obj, costs: t.Mapping[str, float], scale: float, tv_eps: float = 1e-8):
+    """Object cost regularisers of the gradient engine (regularizers.py:195-351)
+    and their gradients (dL/dRe + i dL/dIm), each term weighted by its cost and
+    all by `scale` = B / n_pos.  Returns (cost, grad)."""
+    o = obj
+    grad = numpy.zeros_like(o)
+    total = 0.0
+    c = costs.get
+    if c('obj_l1'):
+        d = o - 1.0
+        m = numpy.abs(d)
+        total += c('obj_l1') * numpy.sum(m)
+        grad += c('obj_l1') * numpy.where(m > 0, d / numpy.where(m > 0, m, 1), 0)
+    if c('obj_l2'):
+        d = o - 1.0
+        total += c('obj_l2') * numpy.sum(abs2(d))
+        grad += 2 * c('obj_l2') * d
+    if c('obj_phase_l1'):
+        ph = numpy.angle(o)
+        total += c('obj_phase_l1') * numpy.sum(numpy.abs(ph))
+        grad += c('obj_phase_l1') * numpy.sign(ph) * 1j * o / numpy.maximum(abs2(o), 1e-30)
+    if c('obj_tikh'):
+        for ax in (-1, -2):
+            d = numpy.diff(o, axis=ax)
+            total += c('obj_tikh') * numpy.sum(abs2(d))
+            g = numpy.zeros_like(o)
+            sl_lo = [slice(None)] * o.ndim
+            sl_hi = [slice(None)] * o.ndim
+            sl_lo[ax], sl_hi[ax] = slice(None, -1), slice(1, None)
+            g[tuple(sl_lo)] -= 2 * d
+            g[tuple(sl_hi)] += 2 * d
+            grad += c('obj_tikh') * g
+    if c('obj_tv'):
+        gy = numpy.diff(o, axis=-2, append=o[..., -1:, :])
+        gx = numpy.diff(o, axis=-1, append=o[..., :, -1:])
+        tv = numpy.sqrt(abs2(gy) + abs2(gx) + tv_eps)
+        total += c('obj_tv') * numpy.sum(tv)
+        uy, ux = gy / tv, gx / tv
+        g = -(uy + ux)
+        g[..., 1:, :] += uy[..., :-1, :]
+        g[..., :, 1:] += ux[..., :, :-1]
+        grad += c('obj_tv') * g
+    if o.shape[0] > 1 and (c('layers_tikh') or c('layers_tv')):
+        d = numpy.diff(o, axis=0)
+        if c('layers_tikh'):
+            total += c('layers_tikh') * numpy.sum(abs2(d))
+            g = numpy.zeros_like(o)
+            g[:-1] -= 2 * d
+            g[1:] += 2 * d
+            grad += c('layers_tikh') * g
+        if c('layers_tv'):
+            m = numpy.abs(d)
+            total += c('layers_tv') * numpy.sum(m)
+            u = numpy.where(m > 0, d / numpy.where(m > 0, m, 1), 0)
+            g = numpy.zeros_like(o)
+            g[:-1] -= u
+            g[1:] += u
+            grad += c('layers_tv') * g
+    return float(total) * scale, (grad * scale).astype(obj.dtype)

@@ -75,6 +75,12 @@ PHB_OPTIM_ADAM = 1
 PHB_OPTIM_POLYAK = 2
 
 
+class PhbObjReg(ctypes.Structure):
+    """Mirror of `phb_obj_reg` (include/phaser_b200.h)."""
+    _fields_ = [(n, c_f32) for n in ('l1', 'l2', 'phase_l1', 'tikh', 'tv', 'tv_eps', 'layers_tikh', 'layers_tv',
+                                      'scale')]
+
+
 class PhbOptim(ctypes.Structure):
     """Mirror of `phb_optim` (include/phaser_b200.h)."""
     _fields_ = [
@@ -121,6 +127,13 @@ _SIGNATURES = {
     'phb_optimizer_update': (c_i32, [ctypes.POINTER(PhbOptim), c_void_p]),
     'phb_sq_norm_f32': (c_i32, [c_void_p, c_i64, c_f32, c_void_p, c_void_p]),
     'phb_add_centred': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
+    'phb_regularize_layers_c64': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_i32, c_f32, c_void_p]),
+    'phb_object_filter_scratch_bytes': (ctypes.c_size_t, [c_i64, c_i64, c_i64]),
+    'phb_object_filter_c64': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_void_p, c_void_p, c_void_p]),
+    'phb_remove_phase_ramp_c64': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64, c_i64, c_void_p,
+                                          c_void_p]),
+    'phb_object_regularizers': (c_i32, [c_void_p, c_i64, c_i64, c_i64, ctypes.POINTER(PhbObjReg), c_void_p,
+                                        c_void_p, c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),

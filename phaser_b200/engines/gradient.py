@@ -15,8 +15,10 @@ the reference:
               group directions, update minus its mean; iteration constraints;
               positions checked against the object.
 
-Cost regularisers are not implemented yet (NotImplementedError), nor tilt
-updates.
+Cost regularisers on the object (obj_l1, obj_l2, obj_phase_l1, obj_tv,
+obj_tikh, layers_tv, layers_tikh) add their value to each group's loss and
+their gradient to the object gradient (phb_object_regularizers); the
+Fourier-space and probe regularisers and tilt updates raise NotImplementedError.
 """
 from __future__ import annotations
 
@@ -129,6 +131,47 @@ class DeviceSolver:
             _lib.call('phb_optimizer_update', ctypes.byref(o), _stream())
 
 
+_REG_ALIASES = {'obj_tikhonov': 'obj_tikh', 'layers_tikhonov': 'layers_tikh'}
+_REG_FIELDS = {'obj_l1': 'l1', 'obj_l2': 'l2', 'obj_phase_l1': 'phase_l1', 'obj_tv': 'tv', 'obj_tikh': 'tikh',
+               'layers_tv': 'layers_tv', 'layers_tikh': 'layers_tikh'}
+
+
+class CostRegularizers:
+    """The plan's cost regularisers (phaser/engines/common/regularizers.py:195-351),
+    evaluated once per group on the device: value into the group loss, gradient
+    into the object gradient, all scaled by B / n_pos."""
+
+    def __init__(self, hooks: t.Sequence[t.Any]):
+        self.reg = _lib.PhbObjReg()
+        self.reg.tv_eps = 1e-8
+        self.active = False
+        for h in hooks or []:
+            if isinstance(h, str):
+                name, props = h, {}
+            elif isinstance(h, dict):
+                h = dict(h)
+                name, props = str(h.pop('type')), h
+            else:
+                name = getattr(h, 'type', None) or getattr(h, 'ref', '')
+                props = getattr(h, 'props', None) or {}
+                name = P._REF_CLASS_NAMES.get(str(name).rsplit(':', 1)[-1], name)
+            name = _REG_ALIASES.get(str(name), str(name))
+            field = _REG_FIELDS.get(name)
+            if field is None:
+                raise NotImplementedError(f"cost regularizer '{name}' is not implemented by the B200 backend")
+            setattr(self.reg, field, getattr(self.reg, field) + float(P.get(props, 'cost')))
+            if name == 'obj_tv':
+                self.reg.tv_eps = float(P.get(props, 'eps', 1e-8))
+            self.active = True
+
+    def apply(self, eng, B: int, grad: t.Optional[torch.Tensor], loss: torch.Tensor) -> None:
+        if not self.active:
+            return
+        self.reg.scale = float(B) / float(eng.n_pos)
+        _lib.call('phb_object_regularizers', eng.object.data_ptr(), eng.S, eng.H, eng.W, ctypes.byref(self.reg),
+                  0 if grad is None else grad.data_ptr(), loss.data_ptr(), _stream())
+
+
 def process_solvers(props) -> t.Tuple[t.FrozenSet[str], t.List[t.Tuple[t.FrozenSet[str], str, t.Any]],
                                       t.List[t.Tuple[t.FrozenSet[str], str, t.Any]]]:
     """Split the plan's solvers into per-group and per-iteration solvers, with the
@@ -170,8 +213,7 @@ class GradientEngine:
         dtype = numpy.dtype(args.get('dtype', numpy.float32))
         if dtype != numpy.float32:
             raise NotImplementedError("the B200 backend computes in float32/complex64 (plan dtype 'float32')")
-        if P.get(props, 'regularizers', None):
-            raise NotImplementedError("cost regularizers are not implemented by the B200 backend")
+        self.regularizers = CostRegularizers(P.get(props, 'regularizers', None) or [])
         self.noise = _noise(props)
         self.all_vars, group_specs, iter_specs = process_solvers(props)
         self.niter = int(P.get(props, 'niter', 10))
@@ -272,6 +314,7 @@ class GradientEngine:
                      grad_probe=self.grad_probe if 'probe' in iter_vars else None,
                      grad_pos=self.grad_pos if 'positions' in iter_vars else None,
                      grad_pos_scale=-1.0 / (probe_int * B), group_loss=losses[gi:gi + 1])
+            self.regularizers.apply(eng, B, self.grad_object if 'object' in iter_vars else None, losses[gi:gi + 1])
             dirs = {}
             if 'object' in iter_vars:
                 dirs['object'] = (self.grad_object, -1.0 / (probe_int * B))

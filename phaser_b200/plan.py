@@ -159,6 +159,12 @@ _REF_CLASS_NAMES = {
     'MomentumPositionSolver': 'momentum', 'SteepestDescentPositionSolver': 'steepest_descent',
     'ClampObjectAmplitude': 'clamp_object_amplitude', 'LimitProbeSupport': 'limit_probe_support',
     'SGDSolver': 'sgd', 'AdamSolver': 'adam', 'PolyakSGDSolver': 'polyak_sgd',
+    'RegularizeLayers': 'layers', 'ObjLowPass': 'obj_low_pass', 'ObjGaussian': 'obj_gaussian',
+    'RemovePhaseRamp': 'remove_phase_ramp',
+    'ObjL1': 'obj_l1', 'ObjL2': 'obj_l2', 'ObjPhaseL1': 'obj_phase_l1', 'ObjRecipL1': 'obj_recip_l1',
+    'ObjTotalVariation': 'obj_tv', 'ObjTikhonov': 'obj_tikh', 'LayersTotalVariation': 'layers_tv',
+    'LayersTikhonov': 'layers_tikh', 'ProbePhaseTikhonov': 'probe_phase_tikh',
+    'ProbeRecipTikhonov': 'probe_recip_tikh', 'ProbeRecipTotalVariation': 'probe_recip_tv',
 }
 RECONS_VARS = ('object', 'probe', 'positions', 'tilt')
 

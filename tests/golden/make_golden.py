@@ -263,9 +263,72 @@ def grouping_case():
     print(f"wrote {path.name}")
 
 
+def constraints_case():
+    """Iteration constraints and gradient-engine cost regularisers of
+    phaser/engines/common/regularizers.py on one small multislice state with
+    odd object sides (arbitrary-size DFT filters)."""
+    from phaser.engines.common import regularizers as R
+    from phaser.hooks.regularization import (RegularizeLayersProps, ObjLowPassProps, GaussianProps,
+                                             ClampObjectAmplitudeProps, LimitProbeSupportProps,
+                                             CostRegularizerProps, TVRegularizerProps)
+    # RegularizeLayers passes the object ARRAY to to_real_dtype
+    # (regularizers.py:97), which numpy 2 rejects; cupy and jax arrays go through
+    # numpy.dtype's `.dtype` attribute path.  Emulate that path here.
+    orig = R.to_real_dtype
+    R.to_real_dtype = lambda v: orig(v.dtype if isinstance(v, numpy.ndarray) else v)
+    c = make_case(seed=41, N=32, M=2, S=3, scan_shape=(3, 4), step=3.0, samp=0.5)
+    rng = numpy.random.default_rng(42)
+    S, H, W = c['est_obj'].shape
+    obj = (numpy.exp(1j * rng.normal(0, 0.6, (S, H, W))) * rng.uniform(0.7, 1.3, (S, H, W))).astype(C64)
+    thick = numpy.array([18., 18., 18.], F32)
+
+    def st():
+        s_ = c['state'](obj, c['probe'])
+        s_.object.thicknesses = thick.copy()
+        return s_
+
+    out = dict(obj=obj, probe=c['probe'], thick=thick, obj_sampling=numpy.asarray(c['osamp'].sampling),
+               corner=numpy.asarray(c['osamp'].corner), region_min=numpy.asarray(c['osamp'].region_min),
+               region_max=numpy.asarray(c['osamp'].region_max), probe_sampling=numpy.asarray(c['psamp'].sampling),
+               wavelength=numpy.float64(c['wavelength']), scan=c['scan'])
+
+    def apply(hook, name, what='object'):
+        s_ = st()
+        state = hook.init_state(s_)
+        s_, _ = hook.apply_iter(s_, state)
+        out[name] = numpy.asarray(getattr(s_, what).data)
+
+    apply(R.RegularizeLayers(None, RegularizeLayersProps(sigma=30.0, weight=0.6)), 'layers')
+    apply(R.ObjLowPass(None, ObjLowPassProps(max_freq=0.3)), 'low_pass')
+    apply(R.ObjGaussian(None, GaussianProps(sigma=0.7, weight=0.8)), 'gaussian')
+    apply(R.RemovePhaseRamp(None, {}), 'phase_ramp')
+    apply(R.ClampObjectAmplitude(None, ClampObjectAmplitudeProps(amplitude=1.1)), 'clamp')
+    apply(R.LimitProbeSupport(None, LimitProbeSupportProps(max_angle=20.0)), 'probe_support', 'probe')
+
+    group = numpy.indices((3, 4)).reshape(2, -1)[:, :7]
+    costs = {}
+    for name, hook in [('obj_l1', R.ObjL1(None, CostRegularizerProps(cost=0.3))),
+                       ('obj_l2', R.ObjL2(None, CostRegularizerProps(cost=0.4))),
+                       ('obj_phase_l1', R.ObjPhaseL1(None, CostRegularizerProps(cost=0.5))),
+                       ('obj_recip_l1', R.ObjRecipL1(None, CostRegularizerProps(cost=0.01))),
+                       ('obj_tv', R.ObjTotalVariation(None, TVRegularizerProps(cost=0.6, eps=1e-6))),
+                       ('obj_tikh', R.ObjTikhonov(None, CostRegularizerProps(cost=0.7))),
+                       ('layers_tv', R.LayersTotalVariation(None, CostRegularizerProps(cost=0.8))),
+                       ('layers_tikh', R.LayersTikhonov(None, CostRegularizerProps(cost=0.9))),
+                       ('probe_phase_tikh', R.ProbePhaseTikhonov(None, CostRegularizerProps(cost=0.02))),
+                       ('probe_recip_tikh', R.ProbeRecipTikhonov(None, CostRegularizerProps(cost=0.03))),
+                       ('probe_recip_tv', R.ProbeRecipTotalVariation(None, TVRegularizerProps(cost=0.04)))]:
+        s_ = st()
+        costs[name] = float(hook.calc_loss_group(group, s_, hook.init_state(s_))[0])
+    out['cost_names'] = numpy.array(list(costs))
+    out['cost_values'] = numpy.array(list(costs.values()))
+    out['cost_group_size'] = numpy.int64(group.shape[-1])
+    save('constraints.npz', **out)
+
+
+CASES = {'numerics': numerics_case, 'cutouts': cutout_case, 'groupings': grouping_case,
+         'groups': group_cases, 'engines': engine_cases, 'constraints': constraints_case}
+
 if __name__ == '__main__':
-    numerics_case()
-    cutout_case()
-    grouping_case()
-    group_cases()
-    engine_cases()
+    for name in (sys.argv[1:] or list(CASES)):
+        CASES[name]()
