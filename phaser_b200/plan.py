@@ -237,10 +237,36 @@ def process_flag(flag: t.Any) -> t.Callable[[t.Mapping[str, t.Any]], bool]:
 
 
 def process_schedule(sched: t.Any) -> t.Callable[[t.Mapping[str, t.Any]], float]:
-    """float or callable schedule -> value for this iteration (phaser/hooks/schedule.py)."""
+    """float, callable, or the plan form of a schedule hook -> value for this
+    iteration (phaser/types.py:163-167, phaser/hooks/schedule.py:33-75):
+    {'type': 'constant', 'value': v}, {'type': 'piecewise', 'init': s, 'steps':
+    {i: s}} (the value of the largest step i <= engine_iter, else init), and
+    {'type': 'expr', 'expr': '...'} evaluated with i, iter, state, niter, np."""
     if isinstance(sched, (int, float)):
         val = float(sched)
         return lambda args: val
+    if isinstance(sched, dict):
+        kind = str(sched.get('type', '')).lower()
+        if kind == 'constant':
+            return process_schedule(float(sched['value']))
+        if kind == 'piecewise':
+            init = process_schedule(sched['init'])
+            steps = sorted(((int(k), process_schedule(v)) for (k, v) in dict(sched['steps']).items()),
+                           key=lambda kv: kv[0], reverse=True)
+
+            def piecewise(args):
+                i = args['state'].iter.engine_iter
+                for thresh, f in steps:
+                    if i >= thresh:
+                        return f(args)
+                return init(args)
+            return piecewise
+        if kind == 'expr':
+            import numpy
+            expr = str(sched['expr'])
+            return lambda args: float(eval(expr, {'i': args['state'].iter.engine_iter, 'iter': args['state'].iter,
+                                                   'state': args['state'], 'niter': args['niter'], 'np': numpy}))
+        raise NotImplementedError(f"schedule type '{kind}' is not implemented by the B200 backend")
     if callable(sched):
         return lambda args: float(sched(args))
     raise TypeError(f"unsupported schedule {sched!r}")

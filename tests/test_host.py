@@ -91,3 +91,21 @@ def test_flags_and_schedules():
     assert not P.process_flag(P.Flag(after=5, every=2))(args)
     assert not P.process_flag(P.Flag(before=6))(args)
     assert P.process_schedule(0.25)(args) == 0.25
+
+
+def test_schedule_hooks_in_plan_form():
+    """phaser/hooks/schedule.py:33-75: constant, piecewise (largest step <= i), expr."""
+    class S:
+        class iter:
+            engine_iter = 6
+    args = {'state': S, 'niter': 10}
+    assert P.process_schedule({'type': 'constant', 'value': 3})(args) == 3.0
+    pw = {'type': 'piecewise', 'init': 1.0, 'steps': {5: 0.5, 8: {'type': 'constant', 'value': 0.1}}}
+    assert P.process_schedule(pw)(args) == 0.5
+    S.iter.engine_iter = 9
+    assert P.process_schedule(pw)(args) == pytest.approx(0.1)
+    S.iter.engine_iter = 2
+    assert P.process_schedule(pw)(args) == 1.0
+    assert P.process_schedule({'type': 'expr', 'expr': '0.5 ** i / niter'})(args) == pytest.approx(0.025)
+    with pytest.raises(NotImplementedError):
+        P.process_schedule({'type': 'cosine'})
