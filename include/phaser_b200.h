@@ -133,7 +133,8 @@ typedef struct phb_engine {
     float *scan;          /* (n_pos, 2) float32 (y, x) */
     const float *tilt;    /* (n_pos, 2) float32 mrad, or NULL */
     /* data */
-    const float *patterns;    /* (n_pos, N, N) float32, zero frequency in the corner */
+    const void  *patterns;    /* (n_pos, N, N) float32, or uint16 counts when pattern_u16 != 0;
+                                 zero frequency in the corner */
     const float *pattern_mask;/* (N, N) float32 */
     const void  *propagators; /* (S-1, N, N) complex64 (band-limited, untilted) or NULL when S == 1 */
     const float *thicknesses; /* (S) slice thicknesses, used for tilt ramps; NULL if no tilt */
@@ -147,6 +148,10 @@ typedef struct phb_engine {
     /* solver bookkeeping outputs (accumulated over the iteration) */
     float *new_obj_mag;   /* (N, N) float32 or NULL */
     float *new_probe_mag; /* (S, H, W) float32 or NULL */
+    /* resident pattern format: 0 = float32, 1 = uint16 detector counts (half the HBM
+       footprint and read traffic; the kernels convert each count to float32 exactly,
+       as the reference's cast to float32 does, phaser/execute.py:176-177) */
+    int32_t pattern_u16;
 } phb_engine;
 
 typedef struct phb_step {

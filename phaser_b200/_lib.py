@@ -53,6 +53,7 @@ class PhbEngine(ctypes.Structure):
         ('noise', c_i32), ('noise_eps', c_f32), ('noise_offset', c_f32), ('noise_var', c_f32),
         ('workspace', c_void_p), ('workspace_bytes', c_size),
         ('new_obj_mag', c_void_p), ('new_probe_mag', c_void_p),
+        ('pattern_u16', c_i32),
     ]
 
 

@@ -142,6 +142,27 @@ struct GroupArgs {
     double *pre_num, *pre_den;
     float *sim_out;
     const float *group_patterns;
+    const uint16_t *patterns16;   // resident uint16 counts (patterns == nullptr then)
+};
+
+// One position's measured pattern: host-streamed float32 rows (group_patterns),
+// resident float32, or resident uint16 counts converted exactly to float32.
+struct PatRow {
+    const float *f;
+    const uint16_t *h;
+    __device__ __forceinline__ PatRow(const GroupArgs &a, int64_t pos, int b, int64_t NN) {
+        if (a.group_patterns) {
+            f = a.group_patterns + (size_t)b * NN;
+            h = nullptr;
+        } else if (a.patterns16) {
+            f = nullptr;
+            h = a.patterns16 + pos * NN;
+        } else {
+            f = a.patterns + pos * NN;
+            h = nullptr;
+        }
+    }
+    __device__ __forceinline__ float at(int64_t i) const { return h ? (float)__ldg(h + i) : __ldg(f + i); }
 };
 
 template <int N>
@@ -377,11 +398,11 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 #pragma unroll
                         for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
                     if (m == 0) {
-                        const float *pat = a.patterns + pos * NN;
+                        const PatRow pat(a, pos, b, NN);
                         for (int f = tid; f < NN; f += FFT_THREADS) {
                             int ky, kx;
                             flat_to_k<N>(f, ky, kx);
-                            t[1] += (double)(__ldg(pat + ky * N + kx) * __ldg(a.mask_k + f));
+                            t[1] += (double)(pat.at(ky * N + kx) * __ldg(a.mask_k + f));
                         }
                     }
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
@@ -404,8 +425,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 #pragma unroll
                         for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
                     if (m == 0) {
-                        const float *pat = a.patterns + pos * NN;
-                        for (int f = tid; f < NN; f += FFT_THREADS) t[1] += (double)__ldg(pat + f);
+                        const PatRow pat(a, pos, b, NN);
+                        for (int f = tid; f < NN; f += FFT_THREADS) t[1] += (double)pat.at(f);
                     }
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
                     if (tid == 0) {
@@ -463,7 +484,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 cl.sync();
                 return;
             } else {
-                const float *pat = a.group_patterns ? a.group_patterns + (size_t)b * NN : a.patterns + pos * NN;
+                const PatRow pat(a, pos, b, NN);
                 double e2 = 0.0, loss = 0.0;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
@@ -473,7 +494,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         float inten = 0.f;
                         for (int r = 0; r < MR; ++r)
                                 if (r < M) inten += rxf[r][f];
-                        const float pv = __ldg(pat + I::ky(e) * N + I::kx(u));
+                        const float pv = pat.at(I::ky(e) * N + I::kx(u));
                         const float mk = mask_ones ? 1.0f : __ldg(a.mask_k + f);
                         if (calc_err && m == 0) {
                             const float d = inten - pv;
@@ -1166,6 +1187,7 @@ static int validate(const phb_engine *e) {
         return PHB_ERR_INVALID_ARG;
     if (e->S > 1 && !e->propagators) return PHB_ERR_INVALID_ARG;
     if (e->tilt && !e->thicknesses) return PHB_ERR_INVALID_ARG;
+    if (e->pattern_u16 != 0 && e->pattern_u16 != 1) return PHB_ERR_INVALID_ARG;
     if (!(e->samp_y > 0) || !(e->samp_x > 0)) return PHB_ERR_INVALID_ARG;
     if (!e->workspace || ((uintptr_t)e->workspace & 255)) return PHB_ERR_INVALID_ARG;
     const size_t need = carve(nullptr, e->N, e->M, e->S, e->B_max, e->H, e->W).bytes;
@@ -1198,7 +1220,8 @@ static GroupArgs make_args(const phb_engine *e, const Workspace &w, int mode, in
     a.tilt = e->tilt;
     a.thick = e->thicknesses;
     a.group = group;
-    a.patterns = e->patterns;
+    if (e->pattern_u16) a.patterns16 = (const uint16_t *)e->patterns;
+    else a.patterns = (const float *)e->patterns;
     a.mask_k = w.mask_k;
     a.prop1d = w.prop1d;
     a.band = w.band;

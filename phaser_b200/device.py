@@ -39,7 +39,8 @@ class DeviceEngine:
     """Device-resident state + workspace of one reconstruction.
 
     probe (M, N, N) complex64, object (S, H, W) complex64, scan (P, 2) float32,
-    patterns (P, N, N) float32, mask (N, N).  `probe_sampling` is the (dy, dx)
+    patterns (P, N, N) float32 or uint16 counts (kept resident in that format),
+    mask (N, N).  `probe_sampling` is the (dy, dx)
     pixel size of the probe grid; `obj_sampling` the object's ObjectSampling.
     """
 
@@ -93,7 +94,10 @@ class DeviceEngine:
         if patterns_on_device is not None:
             self.patterns = patterns_on_device.reshape(-1, N, N)
         else:
-            self.patterns = up(numpy.asarray(patterns).reshape(-1, N, N), numpy.float32)
+            pat = numpy.asarray(patterns).reshape(-1, N, N)
+            self.patterns = up(pat, numpy.uint16 if pat.dtype == numpy.uint16 else numpy.float32)
+        if self.patterns.dtype not in (torch.float32, torch.uint16) or not self.patterns.is_contiguous():
+            raise TypeError("patterns must be contiguous float32 or uint16")
         if self.patterns.shape[0] != self.n_pos:
             raise ValueError(f"{self.n_pos} scan positions but {self.patterns.shape[0]} patterns")
         self.mask = up(mask, numpy.float32)
@@ -120,6 +124,7 @@ class DeviceEngine:
         e.object, e.probe, e.scan = self.object.data_ptr(), self.probe.data_ptr(), self.scan.data_ptr()
         e.tilt = _ptr(self.tilt)
         e.patterns, e.pattern_mask = self.patterns.data_ptr(), self.mask.data_ptr()
+        e.pattern_u16 = int(self.patterns.dtype == torch.uint16)
         e.propagators = _ptr(self.props)
         e.thicknesses = self.thick.data_ptr() if self.tilt is not None else 0
         e.ky, e.kx = self.fy.data_ptr(), self.fx.data_ptr()

@@ -189,3 +189,42 @@ def test_unsupported_shapes_fail_loudly():
     eng = engine_for(c, 2)
     with pytest.raises(ValueError):
         eng.group_tensor([numpy.arange(4)])
+
+
+@pytest.mark.parametrize('solver', ['lsqml', 'epie', 'grad'])
+def test_uint16_resident_patterns_match_float32(solver):
+    """Patterns held as uint16 counts give the float32 results (the kernels convert
+    each count exactly): presolve rescale, one group step, errors / loss."""
+    c = make_case(seed=55, N=64, M=2, S=3)
+    n = c.scan.shape[0] * c.scan.shape[1]
+    counts = numpy.round(c.patterns * (4000.0 / c.patterns.max())).astype(numpy.uint16)
+    idx = numpy.random.default_rng(3).permutation(n)[:10].astype(numpy.int64)
+    spec = NoiseSpec('poisson', 1e-3, 0.0, 0.1) if solver == 'grad' else NoiseSpec()
+    out = []
+    for pats in (counts, counts.astype(numpy.float32)):
+        eng = DeviceEngine(probe=c.probe, obj=c.obj, scan=c.scan, patterns=pats, mask=c.mask,
+                           probe_sampling=c.probe_sampling, obj_sampling=c.osamp, thicknesses=c.thick,
+                           wavelength=c.wavelength, noise=spec, group_max=len(idx))
+        assert eng.patterns.dtype == (torch.uint16 if pats.dtype == numpy.uint16 else torch.float32)
+        gt, sizes = eng.group_tensor([idx])
+        rescale = eng.presolve(gt, sizes, 'epie' if solver == 'epie' else 'lsqml', gradient_form=solver == 'grad')
+        flags = (_lib.PHB_FLAG_UPDATE_OBJECT | _lib.PHB_FLAG_UPDATE_PROBE | _lib.PHB_FLAG_UPDATE_POSITION
+                 | _lib.PHB_FLAG_CALC_ERROR)
+        eng.status.fill_(-1)
+        if solver == 'grad':
+            g_obj, loss = torch.zeros_like(eng.object), torch.zeros((1,), dtype=torch.float64, device='cuda')
+            eng.step('grad', gt[0], sizes[0], flags=_lib.PHB_FLAG_UPDATE_OBJECT, grad_object=g_obj, group_loss=loss)
+            res = (rescale, g_obj.cpu().numpy(), float(loss.cpu()[0]))
+        else:
+            eng.step(solver, gt[0], sizes[0], flags=flags, beta_object=0.9, beta_probe=0.8)
+            p, o, _ = eng.host_state()
+            res = (rescale, o, p, eng.errors.cpu().numpy()[idx])
+        assert int(eng.status.cpu()[0]) == -1
+        out.append(res)
+    (a, b) = out
+    assert a[0] == pytest.approx(b[0], rel=1e-6)
+    for x, y in zip(a[1:], b[1:]):
+        if isinstance(x, float):
+            assert x == pytest.approx(y, rel=1e-6)
+        else:
+            assert rel_l2(x, y) < 1e-6

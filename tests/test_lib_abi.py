@@ -3,6 +3,7 @@
 import ctypes
 import os
 import re
+import subprocess
 
 from phaser_b200 import _lib
 
@@ -37,11 +38,32 @@ def test_host_only_entry_points():
     assert lib.phb_engine_workspace_bytes(0, 4, 8, 256, 517, 517) == 0
 
 
-def test_struct_layouts_match_header():
-    # phb_engine: 4 int32, 3 int64, 4 double, 10 pointers, int32 + 3 float, pointer, size_t, 2 pointers
-    p = ctypes.sizeof(ctypes.c_void_p)
-    assert ctypes.sizeof(_lib.PhbEngine) == 16 + 24 + 32 + 10 * p + 16 + p + 8 + 2 * p
-    assert _lib.PhbStep.pos_update.offset == 32
+STRUCTS = {'phb_engine': _lib.PhbEngine, 'phb_step': _lib.PhbStep, 'phb_optim': _lib.PhbOptim,
+           'phb_obj_reg': _lib.PhbObjReg}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every field offset and struct size of the ctypes mirrors against the C
+    compiler's view of include/phaser_b200.h (gcc on a generated probe)."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "phaser_b200.h"', 'int main(void) {']
+    for cname, py in STRUCTS.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['return 0;', '}']
+    src = tmp_path / 'probe.c'
+    src.write_text('\n'.join(lines))
+    exe = tmp_path / 'probe'
+    subprocess.run(['gcc', '-std=c11', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split('\n')
+    seen = 0
+    for line in filter(None, out):
+        cname, field, val = line.split()
+        py = STRUCTS[cname]
+        want = ctypes.sizeof(py) if field == 'size' else getattr(py, field).offset
+        assert int(val) == want, (cname, field)
+        seen += 1
+    assert seen == sum(len(py._fields_) + 1 for py in STRUCTS.values())
 
 
 def test_invalid_arguments_are_rejected_without_a_gpu():
