@@ -176,7 +176,7 @@ __device__ __forceinline__ float2 obj_px(const float2 *Os, const CutoutIndex &ci
 // validity bit per register slot (identical for every slice).
 template <int N>
 struct CutView {
-    int32_t base[FFTCfg<N>::U];   // (y0 + row(u)) * W + x0 + jl, inside one slice (H*W < 2^31)
+    int32_t base[FFTCfg<N>::U];   // (y0 + row(u)) * W + x0 + col(0), inside one slice (H*W < 2^31)
     uint64_t valid;               // bit u*E + q: pixel (row(u), col(q)) inside the object
     static_assert(FFTCfg<N>::U * FFTCfg<N>::E <= 64, "per-thread slot bits must fit 64 bits");
     __device__ __forceinline__ void init(const CutoutIndex &ci, int64_t H, int64_t W) {
@@ -185,7 +185,7 @@ struct CutView {
 #pragma unroll
         for (int u = 0; u < I::U; ++u) {
             const int64_t y = ci.y0 + I::row(u);
-            base[u] = (int32_t)(y * W + ci.x0 + (threadIdx.x & 7));
+            base[u] = (int32_t)(y * W + ci.x0 + I::col(0));
             const bool rowok = y >= 0 && y < H;
 #pragma unroll
             for (int q = 0; q < I::E; ++q) {
@@ -196,9 +196,9 @@ struct CutView {
     }
     __device__ __forceinline__ bool ok(int u, int q) const { return (valid >> (u * FFTCfg<N>::E + q)) & 1ull; }
     // offset of pixel (row(u), col(q)) inside one object slice (valid only if ok(u, q))
-    __device__ __forceinline__ int32_t off(int u, int q) const { return base[u] + FFTCfg<N>::NT * q; }
+    __device__ __forceinline__ int32_t off(int u, int q) const { return base[u] + Idx<N>::CS * q; }
     __device__ __forceinline__ float2 at(const float2 *Os, int u, int q) const {
-        return (valid >> (u * FFTCfg<N>::E + q)) & 1ull ? __ldg(Os + base[u] + FFTCfg<N>::NT * q)
+        return (valid >> (u * FFTCfg<N>::E + q)) & 1ull ? __ldg(Os + base[u] + Idx<N>::CS * q)
                                                       : make_float2(1.f, 0.f);
     }
 };
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                const int f = I::ky(e) * N + I::kx(u);
+                const int f = I::ky(u, e) * N + I::kx(u, e);
                 if ((band[f >> 5] >> (f & 31)) & 1u) kb |= 1ull << (u * E + e);
             }
         s_bits[FFT_THREADS + tid] = kb;
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                const int ky = I::ky(e), kx = I::kx(u);
+                const int ky = I::ky(u, e), kx = I::kx(u, e);
                 float2 g = cmul(__ldg(pk + I::flat(u, e)), cmul(hy[ky], hx[kx]));
                 if (dir >= 0) {
                     const float w = twopi * (dir == 0 ? a.fy[ky] : a.fx[kx]);
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const int ky = I::ky(e), kx = I::kx(u);
+                    const int ky = I::ky(u, e), kx = I::kx(u, e);
                     const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
                     v[u][e] = cscale(cmul(v[u][e], p), inv_nn);
                 }
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                             float inten = 0.f;
                             for (int r = 0; r < MR; ++r)
                                 if (r < M) inten += rxf[r][f];
-                            a.sim_out[(size_t)b * NN + I::ky(e) * N + I::kx(u)] = inten;
+                            a.sim_out[(size_t)b * NN + I::ky(u, e) * N + I::kx(u, e)] = inten;
                         }
                 }
                 cl.sync();
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         float inten = 0.f;
                         for (int r = 0; r < MR; ++r)
                                 if (r < M) inten += rxf[r][f];
-                        const float pv = pat.at(I::ky(e) * N + I::kx(u));
+                        const float pv = pat.at(I::ky(u, e) * N + I::kx(u, e));
                         const float mk = mask_ones ? 1.0f : __ldg(a.mask_k + f);
                         if (calc_err && m == 0) {
                             const float d = inten - pv;
@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const int ky = I::ky(e), kx = I::kx(u);
+                    const int ky = I::ky(u, e), kx = I::kx(u, e);
                     const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
                     v[u][e] = cscale(cmulc(v[u][e], p), inv_nn);
                 }
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             for (int u = 0; u < U; ++u)
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const float2 h = cmul(hy[I::ky(e)], hx[I::kx(u)]);
+                    const float2 h = cmul(hy[I::ky(u, e)], hx[I::kx(u, e)]);
                     atomic_add_c(ap + I::flat(u, e), cscale(cmulc(v[u][e], h), inv_n));
                 }
             if (!upd_pos) return;
@@ -1020,7 +1020,7 @@ __global__ void k_pack_c64(const float2 *src, float2 *dst) {
 #pragma unroll
     for (int u = 0; u < I::U; ++u)
 #pragma unroll
-        for (int e = 0; e < I::E; ++e) dst[base + I::flat(u, e)] = src[base + I::ky(e) * N + I::kx(u)];
+        for (int e = 0; e < I::E; ++e) dst[base + I::flat(u, e)] = src[base + I::ky(u, e) * N + I::kx(u, e)];
 }
 template <int N>
 __global__ void k_pack_f32(const float *src, float *dst) {
@@ -1028,7 +1028,7 @@ __global__ void k_pack_f32(const float *src, float *dst) {
 #pragma unroll
     for (int u = 0; u < I::U; ++u)
 #pragma unroll
-        for (int e = 0; e < I::E; ++e) dst[I::flat(u, e)] = src[I::ky(e) * N + I::kx(u)];
+        for (int e = 0; e < I::E; ++e) dst[I::flat(u, e)] = src[I::ky(u, e) * N + I::kx(u, e)];
 }
 
 // ---------------------------------------------------------------- per-iteration helpers

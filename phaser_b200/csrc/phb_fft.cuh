@@ -1,26 +1,32 @@
 // Register-resident 2D FFT of one N x N complex64 tile per CTA (N = 64, 128).
 //
-// A CTA of 256 threads holds the whole tile in registers (64 or 16 complex
-// values per thread) and exchanges through ONE N*N complex shared-memory
-// buffer.  A 1D line FFT of length N = E * NT runs as
-//     radix-E DFT in registers (elements strided by NT)
-//     -> twiddle W_N^{jj*k1} -> shared-memory exchange among the NT threads
-//        of the line -> E/NT radix-NT DFTs in registers,
-// so a 2D transform is 3 exchanges (line, transpose, line).  The forward
-// transform leaves the spectrum in a fixed permuted register order
-// ("K layout"); the inverse consumes that order and returns natural order
-// ("R layout").  Pointwise work between the two (propagators, the detector
-// constraint, shift filters) is done in K layout with explicit (ky, kx)
-// indices, so no reorder pass is ever needed.
+// A CTA of 512 threads holds the whole tile in registers and exchanges through
+// one shared-memory buffer (Lay<N>::BUF complex values).  Forward transforms
+// leave the spectrum in a fixed permuted register order ("K layout"), inverse
+// transforms consume that order and return natural order ("R layout").
+// Pointwise work between the two (propagators, the detector constraint, shift
+// filters) is done in K layout with explicit (ky, kx) indices from Idx<N>, so
+// no reorder pass is ever needed.  Transforms are unnormalised DFTs with
+// exp(-2 pi i nk/N) forward.
 //
-// Layouts (tid = threadIdx.x, rsel = tid / 8, jl = tid % 8, unit u, RPP = threads / 8):
-//   R layout: v[u][q]          = x[row = rsel + RPP*u][col = jl + 8q]
-//   K layout: v[u][p*NT + k2]  = X[ky = (jl*P + p) + E*k2][kx = rsel + RPP*u]
-// The transforms are unnormalised DFTs with exp(-2 pi i nk/N) forward.
+// N = 128 (32 values per thread, TWO exchanges per 2D transform):
+//   x = n1 + 4 n2, kx = k2 + 32 k1;  y = y1 + 16 m2, ky = ky2 + 8 ky1
+//   pass A  thread (y = t/4, n1 = t%4):   DFT-32 over n2            -> k2
+//   pass B  thread (k2 = t%32, y1 = t/32): twiddle W128^{n1 k2}, DFT-4 over n1 -> k1,
+//                                          DFT-8 over m2 -> ky2, twiddle W128^{y1 ky2}
+//   pass C  thread (ky2 = t/64, kx = t%64 + 64c, c = 0, 1): DFT-16 over y1 -> ky1
+//   R layout: v[0][q]        = x[y = t/4][x = t%4 + 4q]
+//   K layout: v[0][16c + j]  = X[ky = t/64 + 8j][kx = t%64 + 64c]
+//   Exchange 1 stores row (4y + n1) with stride 33, exchange 2 row (128 ky2 + kx)
+//   with stride 17: both sides of both exchanges are conflict-free (two
+//   wavefronts per warp-wide 8-byte access) and every address is a per-thread
+//   base plus a compile-time offset.
 //
-// Shared-memory addresses are padded / XOR-swizzled so that every 8-byte
-// access of a half-warp (two lines x 8 threads) hits 16 distinct 8-byte bank
-// pairs.  The exchange buffer holds Lay<N>::BUF complex values.
+// N = 64 (8 values per thread, three exchanges): a line FFT of length
+// N = E * NT runs as a radix-E DFT in registers (elements strided by NT) ->
+// twiddle -> exchange among the NT threads of the line -> radix-NT DFTs:
+//   R layout: v[u][q]        = x[row = t/8 + RPP u][col = t%8 + 8q]
+//   K layout: v[u][p NT + k2] = X[ky = (t%8) P + p + E k2][kx = t/8 + RPP u]
 #pragma once
 
 #include "phb_common.cuh"
@@ -34,7 +40,7 @@ constexpr int FFT_THREADS = PHB_FFT_THREADS;  // threads per tile (256: 4 lines 
 constexpr int RPP = FFT_THREADS / 8;          // rows (lines) handled per pass: 8 threads per line
 
 template <int N> struct FFTCfg;
-template <> struct FFTCfg<128> { static constexpr int E = 16, NT = 8, P = 2, U = 128 / RPP; };
+template <> struct FFTCfg<128> { static constexpr int E = 32, U = 1; };
 template <> struct FFTCfg<64>  { static constexpr int E = 8,  NT = 8, P = 1, U = 64 / RPP; };
 
 // ----------------------------------------------------------------- small DFTs
@@ -116,6 +122,51 @@ __device__ __forceinline__ void dftL(float2 *x) {
     else static_assert(L < 0, "unsupported radix");
 }
 
+// cos(2 pi j / 32) and multiplication by W32^j (forward sign; INV conjugates).
+// Called with j a compile-time constant after unrolling, so it folds to
+// constants, and the trivial angles cost no multiplication.
+__device__ __forceinline__ constexpr float cos32(int j) {
+    j &= 31;
+    const int a = j <= 8 ? j : j <= 16 ? 16 - j : j <= 24 ? j - 16 : 32 - j;
+    const float c = a == 0 ? 1.0f : a == 1 ? 0.98078528040323043f : a == 2 ? 0.92387953251128674f
+                  : a == 3 ? 0.83146961230254524f : a == 4 ? 0.70710678118654752f : a == 5 ? 0.55557023301960218f
+                  : a == 6 ? 0.38268343236508977f : a == 7 ? 0.19509032201612825f : 0.0f;
+    return (j <= 8 || j >= 24) ? c : -c;
+}
+
+template <bool INV>
+__device__ __forceinline__ float2 tw32(float2 a, int j) {
+    j &= 31;
+    if (j == 0) return a;
+    if (j == 16) return make_float2(-a.x, -a.y);
+    if (j == 8) return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);     // * -i (fwd)
+    if (j == 24) return INV ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+    const float c = cos32(j), s = cos32(j - 8);   // sin(2 pi j / 32)
+    return cmul(a, make_float2(c, INV ? s : -s));
+}
+
+// 32-point DFT in place, natural order: n = n2 + 8 n1, k = k1 + 4 k2
+// (DFT-4 over n1, twiddle W32^{n2 k1}, DFT-8 over n2).
+template <bool INV>
+__device__ __forceinline__ void dft32(float2 *x) {
+#pragma unroll
+    for (int n2 = 0; n2 < 8; ++n2) dft4<INV>(x[n2], x[n2 + 8], x[n2 + 16], x[n2 + 24]);
+#pragma unroll
+    for (int k1 = 1; k1 < 4; ++k1)
+#pragma unroll
+        for (int n2 = 1; n2 < 8; ++n2) x[n2 + 8 * k1] = tw32<INV>(x[n2 + 8 * k1], n2 * k1);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft8<INV>(&x[8 * k1]);
+    // slot 8 k1 + k2 holds X[k1 + 4 k2]
+    float2 t[32];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) t[k1 + 4 * k2] = x[8 * k1 + k2];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) x[i] = t[i];
+}
+
 // --------------------------------------------------------------- addressing
 // Every shared-memory access below is (per-thread base) + (compile-time
 // offset), so the compiler keeps a handful of base registers instead of one
@@ -129,6 +180,15 @@ __device__ __forceinline__ void dftL(float2 *x) {
 // Transpose tile: (r, c) at r*N + (c ^ g(r)); for every access pattern used
 // here g(r) depends only on per-thread bits, so the XOR folds into the base.
 template <int N>
+struct Lay;
+
+template <>
+struct Lay<128> {
+    static constexpr int S1 = 33, S2 = 17;   // row strides of exchanges 1 and 2
+    static constexpr int BUF = 1024 * S2;    // complex elements of the exchange buffer (>= 512 * S1)
+};
+
+template <int N>
 struct Lay {
     using C = FFTCfg<N>;
     static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
@@ -140,16 +200,134 @@ struct Lay {
     }
 };
 
-// twiddle table: twid[k1 * NT + jj] = exp(-2 pi i jj k1 / N), N entries
+// twiddle table, N entries: N = 128: twid[j] = exp(-2 pi i j / 128);
+// N = 64: twid[k1 * NT + jj] = exp(-2 pi i jj k1 / 64)
 template <int N>
 __device__ __forceinline__ void fft_init_twiddles(float2 *twid) {
-    using C = FFTCfg<N>;
-    for (int i = threadIdx.x; i < C::E * C::NT; i += blockDim.x) {
-        int k1 = i / C::NT, jj = i % C::NT;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        int e;
+        if constexpr (N == 128) e = i;
+        else e = (i % FFTCfg<N>::NT) * (i / FFTCfg<N>::NT);
         float s, c;
-        sincospif(-2.0f * (float)(jj * k1) / (float)N, &s, &c);
+        sincospif(-2.0f * (float)e / (float)N, &s, &c);
         twid[i] = make_float2(c, s);
     }
+}
+
+// ------------------------------------------------- N = 128: two-exchange form
+// Forward: R layout in, K layout out.
+__device__ __forceinline__ void fft128_r2k(float2 (&v)[1][32], float2 *xb, const float2 *twid) {
+    static_assert(FFT_THREADS == 512, "the 128-point transform is laid out for 512 threads");
+    constexpr int S1 = Lay<128>::S1, S2 = Lay<128>::S2;
+    const int t = threadIdx.x;
+    float2 *x = v[0];
+    dft32<false>(x);                                        // pass A: over n2 -> k2
+    {
+        float2 *wb = xb + t * S1;                           // row 4y + n1 == t
+#pragma unroll
+        for (int k2 = 0; k2 < 32; ++k2) wb[k2] = x[k2];
+    }
+    __syncthreads();
+    const int k2 = t & 31, y1 = t >> 5;
+    {
+        const float2 *rb = xb + 4 * y1 * S1 + k2;          // row 4 (y1 + 16 m2) + n1
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1)
+#pragma unroll
+            for (int m2 = 0; m2 < 8; ++m2) x[8 * n1 + m2] = rb[(64 * m2 + n1) * S1];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int n1 = 1; n1 < 4; ++n1) {                        // twiddle W128^{n1 k2}
+        const float2 w = twid[n1 * k2];
+#pragma unroll
+        for (int m2 = 0; m2 < 8; ++m2) x[8 * n1 + m2] = cmul(x[8 * n1 + m2], w);
+    }
+#pragma unroll
+    for (int m2 = 0; m2 < 8; ++m2) dft4<false>(x[m2], x[8 + m2], x[16 + m2], x[24 + m2]);   // n1 -> k1
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft8<false>(&x[8 * k1]);                                 // m2 -> ky2
+#pragma unroll
+    for (int ky2 = 1; ky2 < 8; ++ky2) {                     // twiddle W128^{y1 ky2}
+        const float2 w = twid[y1 * ky2];
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
+    }
+    {
+        float2 *wb = xb + k2 * S2 + y1;                     // row 128 ky2 + k2 + 32 k1
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+            for (int ky2 = 0; ky2 < 8; ++ky2) wb[(128 * ky2 + 32 * k1) * S2] = x[8 * k1 + ky2];
+    }
+    __syncthreads();
+    {
+        const float2 *rb = xb + ((t >> 6) * 128 + (t & 63)) * S2;   // row 128 ky2 + kx
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int y = 0; y < 16; ++y) x[16 * c + y] = rb[64 * c * S2 + y];
+    }
+    __syncthreads();
+    dft16<false>(&x[0]);                                    // pass C: over y1 -> ky1
+    dft16<false>(&x[16]);
+}
+
+// Inverse (unnormalised): K layout in, R layout out.
+__device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const float2 *twid) {
+    constexpr int S1 = Lay<128>::S1, S2 = Lay<128>::S2;
+    const int t = threadIdx.x;
+    float2 *x = v[0];
+    dft16<true>(&x[0]);                                     // pass C: ky1 -> y1
+    dft16<true>(&x[16]);
+    {
+        float2 *wb = xb + ((t >> 6) * 128 + (t & 63)) * S2;
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int y = 0; y < 16; ++y) wb[64 * c * S2 + y] = x[16 * c + y];
+    }
+    __syncthreads();
+    const int k2 = t & 31, y1 = t >> 5;
+    {
+        const float2 *rb = xb + k2 * S2 + y1;
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = rb[(128 * ky2 + 32 * k1) * S2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ky2 = 1; ky2 < 8; ++ky2) {                     // conj twiddle W128^{y1 ky2}
+        const float2 w = twid[y1 * ky2];
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft8<true>(&x[8 * k1]);                                  // ky2 -> m2
+#pragma unroll
+    for (int m2 = 0; m2 < 8; ++m2) dft4<true>(x[m2], x[8 + m2], x[16 + m2], x[24 + m2]);    // k1 -> n1
+#pragma unroll
+    for (int n1 = 1; n1 < 4; ++n1) {                        // conj twiddle W128^{n1 k2}
+        const float2 w = twid[n1 * k2];
+#pragma unroll
+        for (int m2 = 0; m2 < 8; ++m2) x[8 * n1 + m2] = cmulc(x[8 * n1 + m2], w);
+    }
+    {
+        float2 *wb = xb + 4 * y1 * S1 + k2;
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1)
+#pragma unroll
+            for (int m2 = 0; m2 < 8; ++m2) wb[(64 * m2 + n1) * S1] = x[8 * n1 + m2];
+    }
+    __syncthreads();
+    {
+        const float2 *rb = xb + t * S1;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) x[k] = rb[k];
+    }
+    __syncthreads();
+    dft32<true>(x);                                         // pass A: k2 -> n2
 }
 
 // ----------------------------------------------------------------- line passes
@@ -289,54 +467,85 @@ __device__ __forceinline__ void transpose_kr(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>
 template <int N>
 __device__ __forceinline__ void fft2_r2k(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
                                          const float2 *twid) {
-    line_pass_fwd<N>(v, xb, twid);
-    transpose_rk<N>(v, xb);
-    line_pass_fwd<N>(v, xb, twid);
+    if constexpr (N == 128) {
+        fft128_r2k(v, xb, twid);
+    } else {
+        line_pass_fwd<N>(v, xb, twid);
+        transpose_rk<N>(v, xb);
+        line_pass_fwd<N>(v, xb, twid);
+    }
 }
 
 // Inverse 2D DFT (unnormalised): K layout in, R layout out.
 template <int N>
 __device__ __forceinline__ void ifft2_k2r(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
                                           const float2 *twid) {
-    line_pass_inv<N>(v, xb, twid);
-    transpose_kr<N>(v, xb);
-    line_pass_inv<N>(v, xb, twid);
+    if constexpr (N == 128) {
+        fft128_k2r(v, xb, twid);
+    } else {
+        line_pass_inv<N>(v, xb, twid);
+        transpose_kr<N>(v, xb);
+        line_pass_inv<N>(v, xb, twid);
+    }
 }
 
 // ------------------------------------------------------------- index helpers
+// R layout: element (u, q) of a thread is pixel (row(u), col(q)); col(q) - col(0) = CS * q.
+// K layout: element (u, e) is frequency (ky(u, e), kx(u, e)).
+// flat(u, e): register-order index (coalesced per warp), used for scratch and packed tables.
 template <int N>
-struct Idx {
-    using C = FFTCfg<N>;
-    static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
-    // R layout
+struct Idx;
+
+template <>
+struct Idx<128> {
+    static constexpr int U = 1, E = 32, CS = 4;
+    static __device__ __forceinline__ int row(int) { return threadIdx.x >> 2; }
+    static __device__ __forceinline__ int col(int q) { return (threadIdx.x & 3) + 4 * q; }
+    static __device__ __forceinline__ int kx(int, int e) { return (threadIdx.x & 63) + 64 * (e >> 4); }
+    static __device__ __forceinline__ int ky(int, int e) { return (threadIdx.x >> 6) + 8 * (e & 15); }
+    static __device__ __forceinline__ int flat(int u, int e) { return (u * E + e) * FFT_THREADS + threadIdx.x; }
+    static __host__ __device__ __forceinline__ void rc_of(int t, int u, int q, int &r, int &c) {
+        (void)u;
+        r = t >> 2;
+        c = (t & 3) + 4 * q;
+    }
+    static __host__ __device__ __forceinline__ void k_of(int t, int u, int e, int &ky_, int &kx_) {
+        (void)u;
+        kx_ = (t & 63) + 64 * (e >> 4);
+        ky_ = (t >> 6) + 8 * (e & 15);
+    }
+};
+
+template <>
+struct Idx<64> {
+    using C = FFTCfg<64>;
+    static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U, CS = C::NT;
     static __device__ __forceinline__ int row(int u) { return (threadIdx.x >> 3) + RPP * u; }
     static __device__ __forceinline__ int col(int q) { return (threadIdx.x & 7) + NT * q; }
-    // K layout
-    static __device__ __forceinline__ int kx(int u) { return (threadIdx.x >> 3) + RPP * u; }
-    static __device__ __forceinline__ int ky(int e) {
-        return ((threadIdx.x & 7) * P + e / NT) + E * (e % NT);
-    }
-    // register-order flat index (coalesced per warp), used for scratch and packed tables
+    static __device__ __forceinline__ int kx(int u, int) { return (threadIdx.x >> 3) + RPP * u; }
+    static __device__ __forceinline__ int ky(int, int e) { return ((threadIdx.x & 7) * P + e / NT) + E * (e % NT); }
     static __device__ __forceinline__ int flat(int u, int e) { return (u * E + e) * FFT_THREADS + threadIdx.x; }
+    static __host__ __device__ __forceinline__ void rc_of(int t, int u, int q, int &r, int &c) {
+        r = (t >> 3) + RPP * u;
+        c = (t & 7) + NT * q;
+    }
+    static __host__ __device__ __forceinline__ void k_of(int t, int u, int e, int &ky_, int &kx_) {
+        kx_ = (t >> 3) + RPP * u;
+        ky_ = ((t & 7) * P + e / NT) + E * (e % NT);
+    }
 };
 
 // decode a register-order flat index (from any thread) to (row, col) in R layout
 template <int N>
 __device__ __forceinline__ void flat_to_rc(int f, int &r, int &c) {
-    using C = FFTCfg<N>;
     const int t = f % FFT_THREADS, s = f / FFT_THREADS;   // s = u*E + q
-    const int u = s / C::E, q = s % C::E;
-    r = (t >> 3) + RPP * u;
-    c = (t & 7) + C::NT * q;
+    Idx<N>::rc_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, r, c);
 }
 // ... and to (ky, kx) in K layout
 template <int N>
 __device__ __forceinline__ void flat_to_k(int f, int &ky, int &kx) {
-    using C = FFTCfg<N>;
     const int t = f % FFT_THREADS, s = f / FFT_THREADS;
-    const int u = s / C::E, e = s % C::E;
-    kx = (t >> 3) + RPP * u;
-    ky = ((t & 7) * C::P + e / C::NT) + C::E * (e % C::NT);
+    Idx<N>::k_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, ky, kx);
 }
 
 }  // namespace phb

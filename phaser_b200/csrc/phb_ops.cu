@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                int ky = I::ky(e), kx = I::kx(u);
+                int ky = I::ky(u, e), kx = I::kx(u, e);
                 float s = ((ky + kx) & 1) ? -scale : scale;
                 dst[ky * N + kx] = cscale(v[u][e], s);
             }
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                int ky = I::ky(e), kx = I::kx(u);
+                int ky = I::ky(u, e), kx = I::kx(u, e);
                 float s = ((ky + kx) & 1) ? -scale : scale;
                 v[u][e] = cscale(src[ky * N + kx], s);
             }
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[u][e] = cscale(v[u][e], sc * __ldg(mask + I::ky(e) * N + I::kx(u)));
+        for (int e = 0; e < E; ++e) v[u][e] = cscale(v[u][e], sc * __ldg(mask + I::ky(u, e) * N + I::kx(u, e)));
     ifft2_k2r<N>(v, xb, twid);
 #pragma unroll
     for (int u = 0; u < U; ++u)
