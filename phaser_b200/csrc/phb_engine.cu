@@ -176,30 +176,31 @@ __device__ __forceinline__ float2 obj_px(const float2 *Os, const CutoutIndex &ci
 // validity bit per register slot (identical for every slice).
 template <int N>
 struct CutView {
-    int32_t base[FFTCfg<N>::U];   // (y0 + row(u)) * W + x0 + col(0), inside one slice (H*W < 2^31)
-    uint64_t valid;               // bit u*E + q: pixel (row(u), col(q)) inside the object
+    int32_t base[FFTCfg<N>::U];   // (y0 + row(u, 0)) * W + x0 + col(u, 0), inside one slice (H*W < 2^31)
+    int32_t w;                    // object row length W
+    uint64_t valid;               // bit u*E + q: pixel (row(u, q), col(u, q)) inside the object
     static_assert(FFTCfg<N>::U * FFTCfg<N>::E <= 64, "per-thread slot bits must fit 64 bits");
     __device__ __forceinline__ void init(const CutoutIndex &ci, int64_t H, int64_t W) {
         using I = Idx<N>;
         valid = 0ull;
+        w = (int32_t)W;
 #pragma unroll
         for (int u = 0; u < I::U; ++u) {
-            const int64_t y = ci.y0 + I::row(u);
-            base[u] = (int32_t)(y * W + ci.x0 + I::col(0));
-            const bool rowok = y >= 0 && y < H;
+            base[u] = (int32_t)((ci.y0 + I::row(u, 0)) * W + ci.x0 + I::col(u, 0));
 #pragma unroll
             for (int q = 0; q < I::E; ++q) {
-                const int64_t x = ci.x0 + I::col(q);
-                if (rowok && x >= 0 && x < W) valid |= 1ull << (u * I::E + q);
+                const int64_t y = ci.y0 + I::row(u, q), x = ci.x0 + I::col(u, q);
+                if (y >= 0 && y < H && x >= 0 && x < W) valid |= 1ull << (u * I::E + q);
             }
         }
     }
     __device__ __forceinline__ bool ok(int u, int q) const { return (valid >> (u * FFTCfg<N>::E + q)) & 1ull; }
-    // offset of pixel (row(u), col(q)) inside one object slice (valid only if ok(u, q))
-    __device__ __forceinline__ int32_t off(int u, int q) const { return base[u] + Idx<N>::CS * q; }
+    // offset of pixel (row(u, q), col(u, q)) inside one object slice (valid only if ok(u, q))
+    __device__ __forceinline__ int32_t off(int u, int q) const {
+        return base[u] + Idx<N>::drow(q) * w + Idx<N>::dcol(q);
+    }
     __device__ __forceinline__ float2 at(const float2 *Os, int u, int q) const {
-        return (valid >> (u * FFTCfg<N>::E + q)) & 1ull ? __ldg(Os + base[u] + Idx<N>::CS * q)
-                                                      : make_float2(1.f, 0.f);
+        return (valid >> (u * FFTCfg<N>::E + q)) & 1ull ? __ldg(Os + off(u, q)) : make_float2(1.f, 0.f);
     }
 };
 
@@ -272,6 +273,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
         c.valid = s_bits[tid];
 #pragma unroll
         for (int u = 0; u < U; ++u) c.base[u] = s_base[u * FFT_THREADS + tid];
+        c.w = (int32_t)a.W;
         return c;
     };
 
@@ -922,7 +924,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
         for (int u = 0; u < U; ++u)
 #pragma unroll
             for (int q = 0; q < E; ++q) {
-                const int idx = I::row(u) * N + I::col(q);
+                const int idx = I::row(u, q) * N + I::col(u, q);
                 float2 d = cscale(v[u][q], sc);
                 if (a.mode == MODE_GRAD) {
                     a.grad_probe[(size_t)m * NN + idx] = cadd(a.grad_probe[(size_t)m * NN + idx], d);
@@ -949,7 +951,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
     for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int q = 0; q < E; ++q) {
-            v[u][q] = P[I::row(u) * N + I::col(q)];
+            v[u][q] = P[I::row(u, q) * N + I::col(u, q)];
             bad |= !finite2(v[u][q]);
         }
     __syncthreads();

@@ -10,17 +10,18 @@
 // exp(-2 pi i nk/N) forward.
 //
 // N = 128 (32 values per thread, TWO exchanges per 2D transform):
-//   x = n1 + 4 n2, kx = k2 + 32 k1;  y = y1 + 16 m2, ky = ky2 + 8 ky1
-//   pass A  thread (y = t/4, n1 = t%4):   DFT-32 over n2            -> k2
-//   pass B  thread (k2 = t%32, y1 = t/32): twiddle W128^{n1 k2}, DFT-4 over n1 -> k1,
-//                                          DFT-8 over m2 -> ky2, twiddle W128^{y1 ky2}
-//   pass C  thread (ky2 = t/64, kx = t%64 + 64c, c = 0, 1): DFT-16 over y1 -> ky1
-//   R layout: v[0][q]        = x[y = t/4][x = t%4 + 4q]
-//   K layout: v[0][16c + j]  = X[ky = t/64 + 8j][kx = t%64 + 64c]
-//   Exchange 1 stores row (4y + n1) with stride 33, exchange 2 row (128 ky2 + kx)
-//   with stride 17: both sides of both exchanges are conflict-free (two
-//   wavefronts per warp-wide 8-byte access) and every address is a per-thread
-//   base plus a compile-time offset.
+//   x = xt + 32 j, kx = k1 + 4 k2;  y = yt + 16 m, ky = ky2 + 8 ky1
+//   pass A  thread (xt = t%32, yt = t/32): DFT-4 over j -> k1, DFT-8 over m -> ky2,
+//                                          twiddles W128^{xt k1} W128^{yt ky2}
+//   pass B  thread (yt = t%16, ky2 = t/16%8, k1 = t/128): DFT-32 over xt -> k2
+//   pass C  thread (ky2 = t/64, kx = t%64 + 64c, c = 0, 1): DFT-16 over yt -> ky1
+//   R layout: v[0][8j + m]   = x[y = t/32 + 16m][x = t%32 + 32j]   (a warp covers 32
+//                              consecutive pixels of one row: coalesced object access)
+//   K layout: v[0][16c + i]  = X[ky = t/64 + 8i][kx = t%64 + 64c]
+//   Exchange 1 stores row (yt + 16 (ky2 + 8 k1)) with stride 33, exchange 2 row
+//   (128 ky2 + kx) with stride 17: both sides of both exchanges are conflict-free
+//   (two wavefronts per warp-wide 8-byte access) and every address is a
+//   per-thread base plus a compile-time offset.
 //
 // N = 64 (8 values per thread, three exchanges): a line FFT of length
 // N = E * NT runs as a radix-E DFT in registers (elements strided by NT) ->
@@ -221,55 +222,54 @@ __device__ __forceinline__ void fft128_r2k(float2 (&v)[1][32], float2 *xb, const
     constexpr int S1 = Lay<128>::S1, S2 = Lay<128>::S2;
     const int t = threadIdx.x;
     float2 *x = v[0];
-    dft32<false>(x);                                        // pass A: over n2 -> k2
-    {
-        float2 *wb = xb + t * S1;                           // row 4y + n1 == t
+    {   // pass A: thread (xt, yt), slot 8 j + m
+        const int xt = t & 31, yt = t >> 5;
 #pragma unroll
-        for (int k2 = 0; k2 < 32; ++k2) wb[k2] = x[k2];
-    }
-    __syncthreads();
-    const int k2 = t & 31, y1 = t >> 5;
-    {
-        const float2 *rb = xb + 4 * y1 * S1 + k2;          // row 4 (y1 + 16 m2) + n1
+        for (int m = 0; m < 8; ++m) dft4<false>(x[m], x[8 + m], x[16 + m], x[24 + m]);   // j -> k1
 #pragma unroll
-        for (int n1 = 0; n1 < 4; ++n1)
+        for (int k1 = 0; k1 < 4; ++k1) dft8<false>(&x[8 * k1]);                         // m -> ky2
 #pragma unroll
-            for (int m2 = 0; m2 < 8; ++m2) x[8 * n1 + m2] = rb[(64 * m2 + n1) * S1];
-    }
-    __syncthreads();
+        for (int k1 = 1; k1 < 4; ++k1) {
+            const float2 w = twid[xt * k1];
 #pragma unroll
-    for (int n1 = 1; n1 < 4; ++n1) {                        // twiddle W128^{n1 k2}
-        const float2 w = twid[n1 * k2];
+            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
+        }
 #pragma unroll
-        for (int m2 = 0; m2 < 8; ++m2) x[8 * n1 + m2] = cmul(x[8 * n1 + m2], w);
-    }
+        for (int ky2 = 1; ky2 < 8; ++ky2) {
+            const float2 w = twid[yt * ky2];
 #pragma unroll
-    for (int m2 = 0; m2 < 8; ++m2) dft4<false>(x[m2], x[8 + m2], x[16 + m2], x[24 + m2]);   // n1 -> k1
-#pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1) dft8<false>(&x[8 * k1]);                                 // m2 -> ky2
-#pragma unroll
-    for (int ky2 = 1; ky2 < 8; ++ky2) {                     // twiddle W128^{y1 ky2}
-        const float2 w = twid[y1 * ky2];
-#pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
-    }
-    {
-        float2 *wb = xb + k2 * S2 + y1;                     // row 128 ky2 + k2 + 32 k1
+            for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
+        }
+        float2 *wb = xb + yt * S1 + xt;                     // row yt + 16 (ky2 + 8 k1)
 #pragma unroll
         for (int k1 = 0; k1 < 4; ++k1)
 #pragma unroll
-            for (int ky2 = 0; ky2 < 8; ++ky2) wb[(128 * ky2 + 32 * k1) * S2] = x[8 * k1 + ky2];
+            for (int ky2 = 0; ky2 < 8; ++ky2) wb[16 * (ky2 + 8 * k1) * S1] = x[8 * k1 + ky2];
     }
     __syncthreads();
+    {   // pass B: this thread's row t, DFT-32 over xt
+        const float2 *rb = xb + t * S1;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x[i] = rb[i];
+    }
+    __syncthreads();
+    dft32<false>(x);
     {
-        const float2 *rb = xb + ((t >> 6) * 128 + (t & 63)) * S2;   // row 128 ky2 + kx
+        const int yt = t & 15, ky2 = (t >> 4) & 7, k1 = t >> 7;
+        float2 *wb = xb + (ky2 * 128 + k1) * S2 + yt;       // row 128 ky2 + kx, kx = k1 + 4 k2
+#pragma unroll
+        for (int k2 = 0; k2 < 32; ++k2) wb[4 * k2 * S2] = x[k2];
+    }
+    __syncthreads();
+    {   // pass C: DFT-16 over yt for two columns
+        const float2 *rb = xb + ((t >> 6) * 128 + (t & 63)) * S2;
 #pragma unroll
         for (int c = 0; c < 2; ++c)
 #pragma unroll
             for (int y = 0; y < 16; ++y) x[16 * c + y] = rb[64 * c * S2 + y];
     }
     __syncthreads();
-    dft16<false>(&x[0]);                                    // pass C: over y1 -> ky1
+    dft16<false>(&x[0]);
     dft16<false>(&x[16]);
 }
 
@@ -278,7 +278,7 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
     constexpr int S1 = Lay<128>::S1, S2 = Lay<128>::S2;
     const int t = threadIdx.x;
     float2 *x = v[0];
-    dft16<true>(&x[0]);                                     // pass C: ky1 -> y1
+    dft16<true>(&x[0]);                                     // pass C: ky1 -> yt
     dft16<true>(&x[16]);
     {
         float2 *wb = xb + ((t >> 6) * 128 + (t & 63)) * S2;
@@ -288,46 +288,45 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
             for (int y = 0; y < 16; ++y) wb[64 * c * S2 + y] = x[16 * c + y];
     }
     __syncthreads();
-    const int k2 = t & 31, y1 = t >> 5;
+    {   // pass B: k2 -> xt
+        const int yt = t & 15, ky2 = (t >> 4) & 7, k1 = t >> 7;
+        const float2 *rb = xb + (ky2 * 128 + k1) * S2 + yt;
+#pragma unroll
+        for (int k2 = 0; k2 < 32; ++k2) x[k2] = rb[4 * k2 * S2];
+    }
+    __syncthreads();
+    dft32<true>(x);
     {
-        const float2 *rb = xb + k2 * S2 + y1;
+        float2 *wb = xb + t * S1;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) wb[i] = x[i];
+    }
+    __syncthreads();
+    {   // pass A: conj twiddles, ky2 -> m, k1 -> j
+        const int xt = t & 31, yt = t >> 5;
+        const float2 *rb = xb + yt * S1 + xt;
 #pragma unroll
         for (int k1 = 0; k1 < 4; ++k1)
 #pragma unroll
-            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = rb[(128 * ky2 + 32 * k1) * S2];
+            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = rb[16 * (ky2 + 8 * k1) * S1];
+        __syncthreads();
+#pragma unroll
+        for (int ky2 = 1; ky2 < 8; ++ky2) {
+            const float2 w = twid[yt * ky2];
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
+        }
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) {
+            const float2 w = twid[xt * k1];
+#pragma unroll
+            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) dft8<true>(&x[8 * k1]);                          // ky2 -> m
+#pragma unroll
+        for (int m = 0; m < 8; ++m) dft4<true>(x[m], x[8 + m], x[16 + m], x[24 + m]);    // k1 -> j
     }
-    __syncthreads();
-#pragma unroll
-    for (int ky2 = 1; ky2 < 8; ++ky2) {                     // conj twiddle W128^{y1 ky2}
-        const float2 w = twid[y1 * ky2];
-#pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1) dft8<true>(&x[8 * k1]);                                  // ky2 -> m2
-#pragma unroll
-    for (int m2 = 0; m2 < 8; ++m2) dft4<true>(x[m2], x[8 + m2], x[16 + m2], x[24 + m2]);    // k1 -> n1
-#pragma unroll
-    for (int n1 = 1; n1 < 4; ++n1) {                        // conj twiddle W128^{n1 k2}
-        const float2 w = twid[n1 * k2];
-#pragma unroll
-        for (int m2 = 0; m2 < 8; ++m2) x[8 * n1 + m2] = cmulc(x[8 * n1 + m2], w);
-    }
-    {
-        float2 *wb = xb + 4 * y1 * S1 + k2;
-#pragma unroll
-        for (int n1 = 0; n1 < 4; ++n1)
-#pragma unroll
-            for (int m2 = 0; m2 < 8; ++m2) wb[(64 * m2 + n1) * S1] = x[8 * n1 + m2];
-    }
-    __syncthreads();
-    {
-        const float2 *rb = xb + t * S1;
-#pragma unroll
-        for (int k = 0; k < 32; ++k) x[k] = rb[k];
-    }
-    __syncthreads();
-    dft32<true>(x);                                         // pass A: k2 -> n2
 }
 
 // ----------------------------------------------------------------- line passes
@@ -490,7 +489,8 @@ __device__ __forceinline__ void ifft2_k2r(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E
 }
 
 // ------------------------------------------------------------- index helpers
-// R layout: element (u, q) of a thread is pixel (row(u), col(q)); col(q) - col(0) = CS * q.
+// R layout: element (u, q) of a thread is pixel (row(u, q), col(u, q)), offset (drow(q), dcol(q))
+// from element (u, 0).
 // K layout: element (u, e) is frequency (ky(u, e), kx(u, e)).
 // flat(u, e): register-order index (coalesced per warp), used for scratch and packed tables.
 template <int N>
@@ -498,16 +498,19 @@ struct Idx;
 
 template <>
 struct Idx<128> {
-    static constexpr int U = 1, E = 32, CS = 4;
-    static __device__ __forceinline__ int row(int) { return threadIdx.x >> 2; }
-    static __device__ __forceinline__ int col(int q) { return (threadIdx.x & 3) + 4 * q; }
+    static constexpr int U = 1, E = 32;
+    static __device__ __forceinline__ int row(int, int q) { return (threadIdx.x >> 5) + 16 * (q & 7); }
+    static __device__ __forceinline__ int col(int, int q) { return (threadIdx.x & 31) + 32 * (q >> 3); }
+    // offsets of element q from element 0 of the same u: rows and columns (compile-time)
+    static __host__ __device__ __forceinline__ constexpr int drow(int q) { return 16 * (q & 7); }
+    static __host__ __device__ __forceinline__ constexpr int dcol(int q) { return 32 * (q >> 3); }
     static __device__ __forceinline__ int kx(int, int e) { return (threadIdx.x & 63) + 64 * (e >> 4); }
     static __device__ __forceinline__ int ky(int, int e) { return (threadIdx.x >> 6) + 8 * (e & 15); }
     static __device__ __forceinline__ int flat(int u, int e) { return (u * E + e) * FFT_THREADS + threadIdx.x; }
     static __host__ __device__ __forceinline__ void rc_of(int t, int u, int q, int &r, int &c) {
         (void)u;
-        r = t >> 2;
-        c = (t & 3) + 4 * q;
+        r = (t >> 5) + 16 * (q & 7);
+        c = (t & 31) + 32 * (q >> 3);
     }
     static __host__ __device__ __forceinline__ void k_of(int t, int u, int e, int &ky_, int &kx_) {
         (void)u;
@@ -519,9 +522,11 @@ struct Idx<128> {
 template <>
 struct Idx<64> {
     using C = FFTCfg<64>;
-    static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U, CS = C::NT;
-    static __device__ __forceinline__ int row(int u) { return (threadIdx.x >> 3) + RPP * u; }
-    static __device__ __forceinline__ int col(int q) { return (threadIdx.x & 7) + NT * q; }
+    static constexpr int E = C::E, NT = C::NT, P = C::P, U = C::U;
+    static __device__ __forceinline__ int row(int u, int) { return (threadIdx.x >> 3) + RPP * u; }
+    static __device__ __forceinline__ int col(int, int q) { return (threadIdx.x & 7) + NT * q; }
+    static __host__ __device__ __forceinline__ constexpr int drow(int) { return 0; }
+    static __host__ __device__ __forceinline__ constexpr int dcol(int q) { return NT * q; }
     static __device__ __forceinline__ int kx(int u, int) { return (threadIdx.x >> 3) + RPP * u; }
     static __device__ __forceinline__ int ky(int, int e) { return ((threadIdx.x & 7) * P + e / NT) + E * (e % NT); }
     static __device__ __forceinline__ int flat(int u, int e) { return (u * E + e) * FFT_THREADS + threadIdx.x; }

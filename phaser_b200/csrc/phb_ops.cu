@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int q = 0; q < E; ++q) v[u][q] = src[I::row(u) * N + I::col(q)];
+            for (int q = 0; q < E; ++q) v[u][q] = src[I::row(u, q) * N + I::col(u, q)];
         __syncthreads();
         fft2_r2k<N>(v, xb, twid);
 #pragma unroll
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int q = 0; q < E; ++q) dst[I::row(u) * N + I::col(q)] = v[u][q];
+            for (int q = 0; q < E; ++q) dst[I::row(u, q) * N + I::col(u, q)] = v[u][q];
     }
 }
 
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-        for (int q = 0; q < E; ++q) v[u][q] = t[I::row(u) * N + I::col(q)];
+        for (int q = 0; q < E; ++q) v[u][q] = t[I::row(u, q) * N + I::col(u, q)];
     __syncthreads();
     fft2_r2k<N>(v, xb, twid);
     const float sc = 1.0f / (float)(N * N);
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
 #pragma unroll
     for (int u = 0; u < U; ++u)
 #pragma unroll
-        for (int q = 0; q < E; ++q) t[I::row(u) * N + I::col(q)] = v[u][q];
+        for (int q = 0; q < E; ++q) t[I::row(u, q) * N + I::col(u, q)] = v[u][q];
 }
 
 template <int N>
