@@ -332,6 +332,10 @@ def run_b200(args, world, rank, local):
     if not args.no_nrmse:
         nrmse = nrmse_run(new_engine(), ds, args.nrmse_iters, stream)
 
+    extra = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        extra = extra_configs(dev, stream)
+
     # ---------------- roofline of the fused kernel
     peak, peak_kind = measured_peaks()
     B = args.batch
@@ -352,7 +356,8 @@ def run_b200(args, world, rank, local):
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pats_host.numel() * 4),
                         "d2h_bytes_per_step": 32},
-                "gpu_launches": int(launches), "clocks": clk.summary(), "nrmse": nrmse}
+                "gpu_launches": int(launches), "clocks": clk.summary(), "nrmse": nrmse,
+                "other_configs": extra}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -410,6 +415,79 @@ def nrmse_run(eng, ds, iters: int, stream):
                           "removed, global phase fitted; reference = the true (simulated) object"}
 
 
+def extra_configs(dev, stream):
+    """The other two configurations of the benchmark description, measured on the
+    same GPU (device time of whole iterations, patterns resident):
+      single-slice ePIE: 64^2 probe, 1 mode, 32x32 scan at 4 px (+-0.5 px jitter),
+        1e5 e-/pattern, grouping 64, 10 iterations from the flat start;
+      gradient engine: 16 x 2 nm slices of 774^2 (reference geometry of a 128x128 scan
+        at 5 px), probe 128^2 x 2 modes, Poisson negative log-likelihood, Adam on object
+        and probe, grouping 64, 2 timed iterations after 1 warm-up."""
+    import torch
+    from phaser_b200.synthetic import epie_single_slice_config, gradient_multislice_config, simulate_patterns
+    from phaser_b200.engines.conventional import ConventionalEngine
+    from phaser_b200.engines.gradient import GradientEngine
+    from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
+    from phaser_b200.sampling import Sampling
+    from phaser_b200 import plan as PL
+    from phaser_b200.constraints import RemovePhaseRamp
+
+    def state_of(ds):
+        N = ds.probe.shape[-1]
+        return ReconsState(iter=IterState(), wavelength=ds.wavelength,
+                           probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
+                           object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
+                           scan=ds.scan.copy())
+
+    def timed(eng, first, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(first, first + n):
+            eng.iteration(i, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+        eng.check(first + n - 1)
+        return e0.elapsed_time(e1) / 1e3
+
+    out = {}
+    ds = epie_single_slice_config(seed=1)
+    pats = simulate_patterns(ds, seed=1, device=dev, group=64)
+    props = PL.ConventionalEnginePlan(noise_model={'type': 'amplitude'}, solver={'type': 'epie'}, niter=10,
+                                      grouping=64)
+    eng = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state_of(ds), 'dtype': numpy.float32,
+                              'seed': 'bench-c1', 'recons_name': 'c1'}, props, patterns_on_device=pats)
+    eng.presolve()
+    secs = timed(eng, 1, 10)
+    n_pos = int(numpy.prod(ds.scan.shape[:-1]))
+    crop = RemovePhaseRamp(eng.eng, None, None)
+    ref = torch.from_numpy(ds.true_object).to(dev)
+    out['single_slice_epie'] = {
+        "workload": "single-slice ePIE: 64^2 probe x 1 mode, 32x32 scan @ 4 px, object "
+                    f"{ds.obj_sampling.shape[0]}x{ds.obj_sampling.shape[1]}, grouping 64, 10 iterations",
+        "value": n_pos * 1 * 10 / secs, "unit": UNIT, "seconds_10_iterations": secs,
+        "nrmse_after_10": object_nrmse(eng.eng.object, ref, crop.rows, crop.cols)}
+    del eng, pats
+    ds = gradient_multislice_config(seed=2)
+    pats = simulate_patterns(ds, seed=2, device=dev, group=256)
+    props = PL.GradientEnginePlan(
+        solvers={'object': {'type': 'adam', 'learning_rate': 1e-2}, 'probe': {'type': 'adam', 'learning_rate': 1e-3}},
+        noise_model={'type': 'poisson', 'eps': 1e-3}, niter=3, grouping=64)
+    eng = GradientEngine({'data': Patterns(None, ds.mask), 'state': state_of(ds), 'dtype': numpy.float32,
+                          'seed': 'bench-c3', 'recons_name': 'c3'}, props, patterns_on_device=pats)
+    eng.presolve()
+    timed(eng, 1, 1)
+    secs = timed(eng, 2, 2)
+    n_pos = int(numpy.prod(ds.scan.shape[:-1]))
+    S = ds.true_object.shape[0]
+    out['gradient_multislice'] = {
+        "workload": f"gradient engine: {S} x {ds.obj_sampling.shape[0]}^2 slices, 128^2 probe x 2 modes, "
+                    "128x128 scan @ 5 px, Poisson NLL, Adam, grouping 64",
+        "value": n_pos * S * 2 / secs, "unit": UNIT, "ms_per_iteration": secs / 2 * 1e3}
+    del eng, pats
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -419,6 +497,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-nrmse', action='store_true')
+    ap.add_argument('--no-extra', action='store_true', help='skip the single-slice ePIE and gradient-engine lines')
     ap.add_argument('--nrmse-iters', type=int, default=20, help='iterations of the NRMSE run (20 = the configuration)')
     ap.add_argument('--scan', type=int, default=64, help='scan side (64 = the benchmark configuration)')
     ap.add_argument('--batch', type=int, default=256, help='mini-batch size (256 = the benchmark configuration)')

@@ -112,6 +112,13 @@ def epie_single_slice_config(seed: int = 0) -> Dataset:
                         peak_rad=0.4, counts=1e5, scan_jitter_px=0.5, seed=seed)
 
 
+# the gradient-engine configuration (16 x 2 nm slices, 128^2 probe, 2 modes, 128^2 scan at 5 px)
+def gradient_multislice_config(seed: int = 0, scan: int = 128) -> Dataset:
+    return make_dataset(N=128, M=2, S=16, scan_shape=(scan, scan), step_px=5.0, sampling=0.2, kv=300e3,
+                        conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
+                        peak_rad=0.2, counts=1e6, mode_powers=(0.7, 0.3), seed=seed)
+
+
 def simulate_patterns(ds: Dataset, *, seed: int = 0, group: int = 256, device='cuda'):
     """Noisy patterns (n_pos, N, N) float32 on the device, from the B200 forward kernel."""
     import torch
