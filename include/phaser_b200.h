@@ -310,6 +310,43 @@ typedef struct phb_obj_reg {
 int phb_object_regularizers(const void *obj, int64_t S, int64_t H, int64_t W, const phb_obj_reg *reg, void *grad,
                             double *loss, void *stream);
 
+/* ---------------------------------------------------- learned warm start
+ * A small convolutional network (no counterpart in the reference) predicts the
+ * object patch under the probe from each diffraction pattern; the stitched
+ * prediction seeds the iterative solvers.  Activations NCHW float32, weights
+ * (Co, Ci, 3, 3) bfloat16, accumulation float32, padding 1, stride 1 or 2
+ * (Ho = Hi / stride).  The caller zeroes dw / db before phb_conv3x3_bwd_weight,
+ * which accumulates into them. */
+int phb_conv3x3_fwd(const float *in, const void *w_bf16, const float *bias, float *out, int32_t Nb, int32_t Ci,
+                    int32_t Hi, int32_t Wi, int32_t Co, int32_t stride, int32_t relu, void *stream);
+int phb_conv3x3_bwd_data(const float *dout, const void *w_bf16, float *din, int32_t Nb, int32_t Ci, int32_t Hi,
+                         int32_t Wi, int32_t Co, int32_t stride, void *stream);
+int phb_conv3x3_bwd_weight(const float *in, const float *dout, float *dw, float *db, int32_t Nb, int32_t Ci,
+                           int32_t Hi, int32_t Wi, int32_t Co, int32_t stride, void *stream);
+int phb_relu_bwd(float *grad, const float *y, int64_t n, void *stream);   /* grad *= (y > 0) */
+int phb_upsample2(const float *in, float *out, int64_t planes, int32_t H, int32_t W, void *stream);
+int phb_upsample2_bwd(const float *gout, float *gin, int64_t planes, int32_t H, int32_t W, void *stream);
+/* *loss += mean (pred - target)^2 (float64), grad = d/dpred (either may be NULL) */
+int phb_mse(const float *pred, const float *target, float *grad, int64_t n, double *loss, void *stream);
+int phb_to_bf16(const float *x, void *y, int64_t n, void *stream);
+/* network input: log(1 + I) of each pattern (rows `index`, or 0..B-1 when NULL), zero
+ * frequency centred, binned bin x bin, scaled to a maximum of 1: (B, N/bin, N/bin) */
+int phb_pattern_features(const float *patterns, const int64_t *index, int32_t B, int32_t N, int32_t bin, float *out,
+                         void *stream);
+/* training targets: centred P x P patch of the projected object `proj` (H, W) under each
+ * position's cutout (exact reference cutout start), as (Re - 1, Im): (B, 2, P, P) */
+int phb_patch_targets(const void *proj, int64_t H, int64_t W, const float *scan, const int64_t *index, int32_t B,
+                      double corner_y, double corner_x, double samp_y, double samp_x, int32_t N, int32_t P,
+                      float *out, void *stream);
+/* stitching: accumulate predicted (B, 2, P, P) patches into acc (H, W complex) and wgt (H, W);
+ * then obj = acc / wgt where covered, 1 elsewhere */
+int phb_stitch_patches(const float *pred, const float *scan, const int64_t *index, int32_t B, double corner_y,
+                       double corner_x, double samp_y, double samp_x, int32_t N, int32_t P, void *acc, float *wgt,
+                       int64_t H, int64_t W, void *stream);
+int phb_stitch_finish(const void *acc, const float *wgt, void *obj, int64_t n, void *stream);
+/* product over the S slices of an (S, HW) complex64 object */
+int phb_project_slices(const void *obj, int64_t S, int64_t HW, void *out, void *stream);
+
 /* Per-iteration position update (phaser/engines/conventional/run.py:95-110 with
  * phaser/engines/common/position_correction.py): subtract mean, momentum or
  * steepest-descent step with norm clipping, subtract mean, scan += update, and

@@ -135,6 +135,24 @@ _SIGNATURES = {
                                           c_void_p]),
     'phb_object_regularizers': (c_i32, [c_void_p, c_i64, c_i64, c_i64, ctypes.POINTER(PhbObjReg), c_void_p,
                                         c_void_p, c_void_p]),
+    'phb_conv3x3_fwd': (c_i32, [c_void_p, c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32,
+                                c_i32, c_void_p]),
+    'phb_conv3x3_bwd_data': (c_i32, [c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32,
+                                     c_void_p]),
+    'phb_conv3x3_bwd_weight': (c_i32, [c_void_p, c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_i32, c_i32,
+                                       c_i32, c_void_p]),
+    'phb_relu_bwd': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
+    'phb_upsample2': (c_i32, [c_void_p, c_void_p, c_i64, c_i32, c_i32, c_void_p]),
+    'phb_upsample2_bwd': (c_i32, [c_void_p, c_void_p, c_i64, c_i32, c_i32, c_void_p]),
+    'phb_mse': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p, c_void_p]),
+    'phb_to_bf16': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
+    'phb_pattern_features': (c_i32, [c_void_p, c_void_p, c_i32, c_i32, c_i32, c_void_p, c_void_p]),
+    'phb_patch_targets': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p, c_i32, c_f64, c_f64, c_f64, c_f64,
+                                  c_i32, c_i32, c_void_p, c_void_p]),
+    'phb_stitch_patches': (c_i32, [c_void_p, c_void_p, c_void_p, c_i32, c_f64, c_f64, c_f64, c_f64, c_i32, c_i32,
+                                   c_void_p, c_void_p, c_i64, c_i64, c_void_p]),
+    'phb_stitch_finish': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p]),
+    'phb_project_slices': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),

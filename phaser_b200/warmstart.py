@@ -1,0 +1,352 @@
+"""Learned warm start for the iterative solvers.
+
+A small convolutional network maps each diffraction pattern (64 x 64, log
+scale, zero frequency centred) to the 32 x 32 complex object patch under the
+centre of the probe; the patches are stitched into an initial object that
+LSQ-ML / ePIE / the gradient engine then refine.  The reference has no such
+component; the solvers stay the authority and the fallback: the warm start is
+used only when its simulated patterns fit the measurements better than the
+flat object does.
+
+Network: 3x3 convolutions with bfloat16 weights and float32 accumulation
+(libphaser_b200 phb_conv3x3_*):
+    conv 1->32 stride 2, ReLU    64^2 -> 32^2
+    conv 32->64 stride 2, ReLU   32^2 -> 16^2
+    conv 64->64, ReLU, 2x up     16^2 -> 32^2
+    conv 64->32, ReLU            32^2
+    conv 32->2                   32^2 x (Re - 1, Im)
+trained with mean squared error and Adam (phb_optimizer_update) on patterns the
+B200 forward model simulates from random Gaussian-atom lattices.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+import typing as t
+
+import numpy
+import torch
+
+from . import _lib
+
+LAYERS = ((1, 32, 2, True, False), (32, 64, 2, True, False), (64, 64, 1, True, True),
+          (64, 32, 1, True, False), (32, 2, 1, False, False))
+IN_SIDE, PATCH = 64, 32
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class WarmStartNet:
+    """The network's parameters (float32 master copies, bfloat16 working copies),
+    gradients, Adam state and activation buffers, all on one device."""
+
+    def __init__(self, seed: int = 0, device: t.Union[str, torch.device] = 'cuda'):
+        self.device = torch.device(device)
+        rng = numpy.random.default_rng(seed)
+        self.w, self.b, self.wq, self.gw, self.gb, self.m, self.v = [], [], [], [], [], [], []
+        for (ci, co, *_r) in LAYERS:
+            w = rng.normal(0.0, math.sqrt(2.0 / (ci * 9)), (co, ci, 3, 3)).astype(numpy.float32)
+            self.w.append(torch.from_numpy(w).to(self.device))
+            self.b.append(torch.zeros(co, dtype=torch.float32, device=self.device))
+            self.wq.append(torch.empty((co, ci, 3, 3), dtype=torch.bfloat16, device=self.device))
+        for p in self.w + self.b:
+            (self.gw if p.dim() == 4 else self.gb).append(torch.zeros_like(p))
+        self.params = self.w + self.b
+        self.grads = self.gw + self.gb
+        self.m = [torch.zeros_like(p) for p in self.params]
+        self.v = [torch.zeros_like(p) for p in self.params]
+        self.count = 0
+        self._acts: t.Dict[int, t.List[torch.Tensor]] = {}
+        self.quantize()
+
+    def quantize(self) -> None:
+        for w, q in zip(self.w, self.wq):
+            _lib.call('phb_to_bf16', w.data_ptr(), q.data_ptr(), w.numel(), _stream())
+
+    # activation buffers: [x, a1, a2, a3, a3 upsampled, a4, y] and matching gradients
+    def _buffers(self, B: int) -> t.List[torch.Tensor]:
+        if B not in self._acts:
+            shapes = [(1, 64), (32, 32), (64, 16), (64, 16), (64, 32), (32, 32), (2, 32)]
+            acts = [torch.empty((B, c, s, s), dtype=torch.float32, device=self.device) for (c, s) in shapes]
+            grads = [torch.empty_like(a) for a in acts]
+            self._acts = {B: acts + grads}
+        return self._acts[B]
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        """x (B, 1, 64, 64) float32 -> (B, 2, 32, 32): the patch as (Re - 1, Im)."""
+        B = x.shape[0]
+        bufs = self._buffers(B)
+        acts = bufs[:7]
+        acts[0].copy_(x.reshape(B, 1, IN_SIDE, IN_SIDE))
+        k = 0
+        st = _stream()
+        for li, (ci, co, s, relu, up) in enumerate(LAYERS):
+            src, dst = acts[k], acts[k + 1]
+            _lib.call('phb_conv3x3_fwd', src.data_ptr(), self.wq[li].data_ptr(), self.b[li].data_ptr(),
+                      dst.data_ptr(), B, ci, src.shape[2], src.shape[3], co, s, int(relu), st)
+            k += 1
+            if up:
+                _lib.call('phb_upsample2', acts[k].data_ptr(), acts[k + 1].data_ptr(), B * co, acts[k].shape[2],
+                          acts[k].shape[3], st)
+                k += 1
+        return acts[6]
+
+    def backward(self, gy: torch.Tensor) -> None:
+        """Gradients of sum(gy * forward(x)) into self.grads (zeroed here first)."""
+        B = gy.shape[0]
+        bufs = self._buffers(B)
+        acts, grads = bufs[:7], bufs[7:]
+        st = _stream()
+        for g in self.grads:
+            g.zero_()
+        grads[6].copy_(gy)
+        k = 6
+        for li in range(len(LAYERS) - 1, -1, -1):
+            ci, co, s, relu, up = LAYERS[li]
+            if up:
+                _lib.call('phb_upsample2_bwd', grads[k].data_ptr(), grads[k - 1].data_ptr(), B * co,
+                          acts[k - 1].shape[2], acts[k - 1].shape[3], st)
+                k -= 1
+            g, out, inp = grads[k], acts[k], acts[k - 1]
+            if relu:
+                _lib.call('phb_relu_bwd', g.data_ptr(), out.data_ptr(), g.numel(), st)
+            _lib.call('phb_conv3x3_bwd_weight', inp.data_ptr(), g.data_ptr(), self.gw[li].data_ptr(),
+                      self.gb[li].data_ptr(), B, ci, inp.shape[2], inp.shape[3], co, s, st)
+            if li > 0:
+                _lib.call('phb_conv3x3_bwd_data', g.data_ptr(), self.wq[li].data_ptr(), grads[k - 1].data_ptr(),
+                          B, ci, inp.shape[2], inp.shape[3], co, s, st)
+            k -= 1
+
+    def adam_step(self, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8) -> None:
+        self.count += 1
+        for p, g, m, v in zip(self.params, self.grads, self.m, self.v):
+            o = _lib.PhbOptim()
+            o.kind, o.nesterov = _lib.PHB_OPTIM_ADAM, 0
+            o.param, o.grad, o.state1, o.state2 = p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr()
+            o.n, o.complex_elems = p.numel(), 0
+            o.grad_scale, o.lr, o.b1, o.b2, o.eps, o.eps_root = -1.0, lr, b1, b2, eps, 0.0
+            o.count = self.count
+            _lib.call('phb_optimizer_update', ctypes.byref(o), _stream())
+        self.quantize()
+
+    def train(self, feats: torch.Tensor, targets: torch.Tensor, *, epochs: int = 2, batch: int = 256,
+              lr: float = 1e-3, seed: int = 0) -> t.List[float]:
+        """Mean training loss per epoch (one host synchronisation per epoch)."""
+        n = feats.shape[0]
+        gen = torch.Generator(device=feats.device)
+        gen.manual_seed(seed)
+        loss = torch.zeros((1,), dtype=torch.float64, device=self.device)
+        out = []
+        for _ in range(epochs):
+            order = torch.randperm(n, generator=gen, device=feats.device)
+            loss.zero_()
+            steps = 0
+            for i in range(0, n - batch + 1, batch):
+                idx = order[i:i + batch]
+                x, tgt = feats[idx], targets[idx]
+                y = self.forward(x)
+                gy = self._buffers(batch)[7 + 6]
+                _lib.call('phb_mse', y.data_ptr(), tgt.data_ptr(), gy.data_ptr(), y.numel(), loss.data_ptr(),
+                          _stream())
+                self.backward(gy)
+                self.adam_step(lr)
+                steps += 1
+            out.append(float(loss.cpu()[0]) / max(steps, 1))
+        return out
+
+    def predict(self, feats: torch.Tensor, batch: int = 256) -> torch.Tensor:
+        outs = []
+        for i in range(0, feats.shape[0], batch):
+            outs.append(self.forward(feats[i:i + batch]).clone())
+        return torch.cat(outs)
+
+    def numpy_params(self) -> t.List[t.Tuple[numpy.ndarray, numpy.ndarray]]:
+        return [(w.cpu().numpy(), b.cpu().numpy()) for (w, b) in zip(self.w, self.b)]
+
+
+# ------------------------------------------------------------------ data
+def lattice_phase_fast(shape: t.Tuple[int, int], spacing: float, sigma: float, peak: float,
+                       rng: numpy.random.Generator, jitter: float = 0.5) -> numpy.ndarray:
+    """Gaussian atoms (sigma px, height `peak` rad) on a jittered hexagonal lattice of
+    `spacing` px with a random offset, splatted at once (numpy.bincount)."""
+    H, W = shape
+    dy = spacing * numpy.sqrt(3) / 2
+    off = rng.uniform(0, spacing, 2)
+    rows = numpy.arange(-1, int(H / dy) + 2)
+    cols = numpy.arange(-1, int(W / spacing) + 2)
+    cy = (rows[:, None] * dy + off[0]) + numpy.zeros(len(cols))[None, :]
+    cx = cols[None, :] * spacing + off[1] + numpy.where(rows % 2 == 1, spacing / 2, 0.)[:, None]
+    cy = cy.ravel() + rng.uniform(-jitter, jitter, cy.size)
+    cx = cx.ravel() + rng.uniform(-jitter, jitter, cx.size)
+    r = int(numpy.ceil(4 * sigma))
+    oy, ox = numpy.mgrid[-r:r + 1, -r:r + 1]
+    iy, ix = numpy.round(cy).astype(int), numpy.round(cx).astype(int)
+    vals = peak * numpy.exp(-((oy.ravel()[None] - (cy - iy)[:, None]) ** 2
+                              + (ox.ravel()[None] - (cx - ix)[:, None]) ** 2) / (2 * sigma ** 2))
+    ys, xs = iy[:, None] + oy.ravel()[None], ix[:, None] + ox.ravel()[None]
+    ok = (ys >= 0) & (ys < H) & (xs >= 0) & (xs < W)
+    return numpy.bincount((ys * W + xs)[ok], weights=vals[ok], minlength=H * W).reshape(H, W)
+
+
+def random_lattice_dataset(rng: numpy.random.Generator, *, scan: int = 32, N: int = 64, counts: float = 1e5,
+                           slices: t.Tuple[int, int] = (4, 12)):
+    """One training object of the single-slice configuration's geometry (64^2 probe,
+    20 mrad, 200 kV, 100 A defocus, 0.2 A/px, scan at 4 px) with 4-12 slices of
+    random lattices (spacing 6-14 px, peak phase 0.1-0.5 rad, 2 nm slices)."""
+    from .synthetic import make_dataset
+    S = int(rng.integers(slices[0], slices[1] + 1))
+    ds = make_dataset(N=N, M=1, S=1, scan_shape=(scan, scan), step_px=4.0, sampling=0.2, kv=200e3,
+                      conv_mrad=20.0, defocus=100.0, slice_thickness=0.0, spacing_px=10.0, sigma_px=1.5,
+                      peak_rad=0.0, counts=counts, scan_jitter_px=0.5, seed=int(rng.integers(1 << 31)))
+    H, W = ds.true_object.shape[-2:]
+    spacing, peak = float(rng.uniform(6, 14)), float(rng.uniform(0.1, 0.5))
+    phase = numpy.stack([lattice_phase_fast((H, W), spacing, 1.5, peak, rng) for _ in range(S)])
+    ds.true_object = numpy.exp(1j * phase).astype(numpy.complex64)
+    ds.init_object = numpy.ones((S, H, W), numpy.complex64)
+    ds.thicknesses = numpy.full(S, 20.0, numpy.float32)
+    return ds
+
+
+def features_and_targets(ds, pats: torch.Tensor, *, with_targets: bool = True):
+    """Network inputs (n, 1, 64, 64) of the dataset's patterns and, optionally, the
+    training targets (n, 2, 32, 32) from its true object."""
+    dev = pats.device
+    n, N = pats.shape[0], pats.shape[-1]
+    st = _stream()
+    feats = torch.empty((n, 1, IN_SIDE, IN_SIDE), dtype=torch.float32, device=dev)
+    _lib.call('phb_pattern_features', pats.data_ptr(), None, n, N, N // IN_SIDE, feats.data_ptr(), st)
+    if not with_targets:
+        return feats, None
+    S, H, W = ds.true_object.shape
+    obj = torch.from_numpy(ds.true_object).to(dev)
+    proj = torch.empty((H, W), dtype=torch.complex64, device=dev)
+    _lib.call('phb_project_slices', obj.data_ptr(), S, H * W, proj.data_ptr(), st)
+    scan = torch.from_numpy(numpy.ascontiguousarray(ds.scan.reshape(-1, 2), numpy.float32)).to(dev)
+    targets = torch.empty((n, 2, PATCH, PATCH), dtype=torch.float32, device=dev)
+    os_ = ds.obj_sampling
+    _lib.call('phb_patch_targets', proj.data_ptr(), H, W, scan.data_ptr(), None, n, float(os_.corner[0]),
+              float(os_.corner[1]), float(os_.sampling[0]), float(os_.sampling[1]), N, PATCH, targets.data_ptr(), st)
+    return feats, targets
+
+
+def training_set(n_objects: int, *, seed: int = 0, scan: int = 32, slices: t.Tuple[int, int] = (4, 12),
+                 device='cuda'):
+    """(features, targets) of n_objects random-lattice objects x scan^2 positions."""
+    from .synthetic import simulate_patterns
+    rng = numpy.random.default_rng(seed)
+    fs, ts = [], []
+    for k in range(n_objects):
+        ds = random_lattice_dataset(rng, scan=scan, slices=slices)
+        pats = simulate_patterns(ds, seed=seed * 100003 + k, device=device)
+        f, tg = features_and_targets(ds, pats)
+        fs.append(f)
+        ts.append(tg)
+    return torch.cat(fs), torch.cat(ts)
+
+
+def stitch(net: WarmStartNet, feats: torch.Tensor, scan: numpy.ndarray, obj_sampling, shape, N: int) -> torch.Tensor:
+    """Predicted patches stitched into an (H, W) complex64 object (1 outside the patches)."""
+    dev = feats.device
+    H, W = shape
+    pred = net.predict(feats)
+    acc = torch.zeros((H, W), dtype=torch.complex64, device=dev)
+    wgt = torch.zeros((H, W), dtype=torch.float32, device=dev)
+    sc = torch.from_numpy(numpy.ascontiguousarray(scan.reshape(-1, 2), numpy.float32)).to(dev)
+    st = _stream()
+    _lib.call('phb_stitch_patches', pred.data_ptr(), sc.data_ptr(), None, pred.shape[0],
+              float(obj_sampling.corner[0]), float(obj_sampling.corner[1]), float(obj_sampling.sampling[0]),
+              float(obj_sampling.sampling[1]), N, PATCH, acc.data_ptr(), wgt.data_ptr(), H, W, st)
+    out = torch.empty_like(acc)
+    _lib.call('phb_stitch_finish', acc.data_ptr(), wgt.data_ptr(), out.data_ptr(), H * W, st)
+    return out
+
+
+def pattern_residual(eng, obj: torch.Tensor) -> float:
+    """sum (sqrt(I_model) - sqrt(I_measured))^2 over all positions for the object
+    `obj` (S, H, W) with the engine's current probe (the fallback criterion)."""
+    saved = eng.object.clone()
+    eng.object.copy_(obj)
+    n, G = eng.n_pos, eng.group_max
+    idx = numpy.arange(n, dtype=numpy.int64)
+    gt, sizes = eng.group_tensor([idx[i:i + G] for i in range(0, n, G)])
+    total = torch.zeros((), dtype=torch.float64, device=eng.device)
+    for g, B in enumerate(sizes):
+        sim = eng.simulate(gt[g], B)
+        meas = eng.patterns[g * G:g * G + B]
+        total += torch.sum((torch.sqrt(sim) - torch.sqrt(torch.clamp(meas, min=0))) ** 2, dtype=torch.float64)
+    eng.object.copy_(saved)
+    return float(total)
+
+
+def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.ndarray) -> t.Tuple[torch.Tensor, dict]:
+    """The stitched warm-start object for the engine's geometry (each of the S slices
+    gets the S-th root of the predicted transmission), or the engine's current
+    object when the prediction fits the patterns worse.  Returns (object, info)."""
+    S, H, W = eng.object.shape
+    feats, _ = features_and_targets(None, pats, with_targets=False)
+    proj = stitch(net, feats, scan, eng.obj_sampling, (H, W), eng.N)
+    cand = torch.exp(torch.log(proj) / S).unsqueeze(0).expand(S, H, W).contiguous()
+    r_warm = pattern_residual(eng, cand)
+    r_flat = pattern_residual(eng, eng.object)
+    use = r_warm < r_flat
+    return (cand if use else eng.object.clone()), {"residual_warm": r_warm, "residual_flat": r_flat,
+                                                   "used": bool(use)}
+
+
+def compare_with_plain(net: WarmStartNet, ds, pats: torch.Tensor, *, iters: int = 20, solver: str = 'lsqml',
+                       grouping: int = 64) -> dict:
+    """Warm start against the plain method on one dataset: NRMSE of the projected
+    object after every iteration (against ds.true_object) and the device time to
+    reach the plain run's final NRMSE.  The warm arm's time includes the network
+    inference, the stitching and the fallback test."""
+    from .constraints import RemovePhaseRamp
+    from .engines.conventional import ConventionalEngine
+    from .metrics import object_nrmse
+    from .plan import ConventionalEnginePlan
+    from .sampling import Sampling
+    from .state import IterState, ObjectState, Patterns, ProbeState, ReconsState
+    N = ds.probe.shape[-1]
+    ref = torch.from_numpy(ds.true_object).to(pats.device)
+    props = ConventionalEnginePlan(noise_model={'type': 'amplitude'}, solver={'type': solver}, niter=iters,
+                                   grouping=grouping)
+    out = {}
+    for arm in ('plain', 'warm'):
+        state = ReconsState(iter=IterState(), wavelength=ds.wavelength,
+                            probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
+                            object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
+                            scan=ds.scan.copy())
+        eng = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
+                                  'seed': 'warm-start', 'recons_name': arm}, props, patterns_on_device=pats)
+        eng.presolve()
+        crop = RemovePhaseRamp(eng.eng, None, None)
+        info = None
+        t_prep = 0.0
+        if arm == 'warm':
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            obj, info = warm_start_object(net, eng.eng, pats, ds.scan)
+            eng.eng.object.copy_(obj)
+            torch.cuda.synchronize()
+            t_prep = time.perf_counter() - t0
+        curve = [object_nrmse(eng.eng.object, ref, crop.rows, crop.cols)]
+        times = [t_prep]
+        for i in range(1, iters + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.iteration(i, sync=False)
+            e1.record()
+            e1.synchronize()
+            eng.check(i)
+            times.append(times[-1] + e0.elapsed_time(e1) / 1e3)
+            curve.append(object_nrmse(eng.eng.object, ref, crop.rows, crop.cols))
+        out[arm] = {"curve": curve, "seconds": times, "fallback_test": info}
+    target = out['plain']['curve'][-1]
+    for arm in ('plain', 'warm'):
+        hit = next((i for i, v in enumerate(out[arm]['curve']) if v <= target), None)
+        out[arm]['iterations_to_target'] = hit
+        out[arm]['seconds_to_target'] = None if hit is None else out[arm]['seconds'][hit]
+    out['target_nrmse'] = target
+    return out

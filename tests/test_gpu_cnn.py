@@ -1,0 +1,94 @@
+"""The warm-start network's CUDA kernels against the numpy oracle
+(oracle/cnn_np.py, itself checked against finite differences on the CPU).
+
+Weights are rounded to bfloat16 in both; accumulation is float32 on the GPU
+and float64 in the oracle: layer outputs and gradients within 1e-5 relative
+L2, the whole network's loss within 1e-5 and its gradients within 1e-4."""
+import numpy
+import pytest
+import torch
+
+from oracle import cnn_np as C
+from phaser_b200 import _lib
+from phaser_b200.warmstart import WarmStartNet
+
+from .test_gpu_engine import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def st():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def bf16_tensor(w):
+    q = torch.empty(w.shape, dtype=torch.bfloat16, device='cuda')
+    wt = torch.from_numpy(w.astype(numpy.float32)).cuda()
+    _lib.call('phb_to_bf16', wt.data_ptr(), q.data_ptr(), wt.numel(), st())
+    return q
+
+
+@pytest.mark.parametrize('ci,co,stride,H', [(1, 32, 2, 64), (32, 64, 2, 32), (64, 64, 1, 16), (64, 32, 1, 32),
+                                            (32, 2, 1, 32), (3, 5, 1, 20), (5, 17, 2, 18)])
+def test_conv_layer_matches_oracle(ci, co, stride, H):
+    rng = numpy.random.default_rng(ci * 100 + co)
+    B = 3
+    x = rng.normal(size=(B, ci, H, H)).astype(numpy.float32)
+    w = rng.normal(0, 0.3, (co, ci, 3, 3)).astype(numpy.float32)
+    b = rng.normal(0, 0.1, co).astype(numpy.float32)
+    dy = rng.normal(size=(B, co, H // stride, H // stride)).astype(numpy.float32)
+    wq = C.bf16(w)
+    xd, bd, dyd = (torch.from_numpy(a).cuda() for a in (x, b, dy))
+    q = bf16_tensor(w)
+    y = torch.empty((B, co, H // stride, H // stride), device='cuda')
+    _lib.call('phb_conv3x3_fwd', xd.data_ptr(), q.data_ptr(), bd.data_ptr(), y.data_ptr(), B, ci, H, H, co, stride,
+              1, st())
+    ref = C.conv3x3(x.astype(numpy.float64), wq.astype(numpy.float64), b.astype(numpy.float64), stride, relu=True)
+    assert rel_l2(y.cpu().numpy(), ref) < 1e-5
+    dx = torch.empty_like(xd)
+    dw = torch.zeros((co, ci, 3, 3), device='cuda')
+    db = torch.zeros((co,), device='cuda')
+    _lib.call('phb_conv3x3_bwd_data', dyd.data_ptr(), q.data_ptr(), dx.data_ptr(), B, ci, H, H, co, stride, st())
+    _lib.call('phb_conv3x3_bwd_weight', xd.data_ptr(), dyd.data_ptr(), dw.data_ptr(), db.data_ptr(), B, ci, H, H, co,
+              stride, st())
+    rdx, rdw, rdb = C.conv3x3_backward(x.astype(numpy.float64), wq.astype(numpy.float64), dy.astype(numpy.float64),
+                                       stride)
+    assert rel_l2(dx.cpu().numpy(), rdx) < 1e-5
+    assert rel_l2(dw.cpu().numpy(), rdw) < 1e-5
+    assert rel_l2(db.cpu().numpy(), rdb) < 1e-5
+
+
+def test_network_loss_and_gradients_match_oracle():
+    net = WarmStartNet(seed=3)
+    rng = numpy.random.default_rng(4)
+    for b in net.b:
+        b.copy_(torch.from_numpy(rng.normal(0, 0.05, b.shape[0]).astype(numpy.float32)))
+    x = rng.uniform(size=(4, 1, 64, 64)).astype(numpy.float32)
+    t = rng.normal(0, 0.1, (4, 2, 32, 32)).astype(numpy.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    y = net.forward(xd)
+    gy = torch.empty_like(y)
+    loss = torch.zeros((1,), dtype=torch.float64, device='cuda')
+    _lib.call('phb_mse', y.data_ptr(), td.data_ptr(), gy.data_ptr(), y.numel(), loss.data_ptr(), st())
+    net.backward(gy)
+    params = [(w.astype(numpy.float64), b.astype(numpy.float64)) for (w, b) in net.numpy_params()]
+    ref_loss, ref_grads = C.loss_and_grads(params, x.astype(numpy.float64), t.astype(numpy.float64))
+    assert float(loss.cpu()[0]) == pytest.approx(ref_loss, rel=1e-5)
+    for (gw, gb), (rw, rb) in zip(zip(net.gw, net.gb), ref_grads):
+        assert rel_l2(gw.cpu().numpy(), rw) < 1e-4
+        assert rel_l2(gb.cpu().numpy(), rb) < 1e-4
+
+
+def test_upsample_and_relu_kernels():
+    rng = numpy.random.default_rng(6)
+    x = torch.from_numpy(rng.normal(size=(2, 3, 5, 7)).astype(numpy.float32)).cuda()
+    up = torch.empty((2, 3, 10, 14), device='cuda')
+    _lib.call('phb_upsample2', x.data_ptr(), up.data_ptr(), 6, 5, 7, st())
+    assert torch.equal(up.cpu(), torch.from_numpy(C.upsample2(x.cpu().numpy())))
+    g = torch.from_numpy(rng.normal(size=(2, 3, 10, 14)).astype(numpy.float32)).cuda()
+    gin = torch.empty_like(x)
+    _lib.call('phb_upsample2_bwd', g.data_ptr(), gin.data_ptr(), 6, 5, 7, st())
+    assert numpy.allclose(gin.cpu().numpy(), C.upsample2_backward(g.cpu().numpy()), rtol=1e-6, atol=1e-6)
+    g2 = g.clone()
+    _lib.call('phb_relu_bwd', g2.data_ptr(), up.data_ptr(), g2.numel(), st())
+    assert torch.equal(g2.cpu(), (g * (up > 0)).cpu())
