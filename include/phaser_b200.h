@@ -310,6 +310,24 @@ typedef struct phb_obj_reg {
 int phb_object_regularizers(const void *obj, int64_t S, int64_t H, int64_t W, const phb_obj_reg *reg, void *grad,
                             double *loss, void *stream);
 
+/* Fourier-space cost regularisers of the gradient engine.
+ * Probe (regularizers.py:354-426, scale 1): with R = fft2(P) (M, N, N), N = 64 / 128:
+ * probe_phase_tikh sum |diff angle R|^2, probe_recip_tikh sum |diff fftshift R|^2,
+ * probe_recip_tv sum sqrt(|g_y|^2 + |g_x|^2 + tv_eps) of fftshift R.  Adds the value to
+ * *loss and, if `grad` is non-NULL, dL/dRe + i dL/dIm of P to it.
+ * Object (regularizers.py:233-253): obj_recip_l1 cost * sum |fft2(prod_s O_s)| (any H, W;
+ * `cost` already includes the group scale B / n_pos). */
+typedef struct phb_probe_reg {
+    float phase_tikh, recip_tikh, recip_tv, tv_eps;
+} phb_probe_reg;
+
+size_t phb_probe_regularizers_scratch_bytes(int32_t M, int32_t N);
+int phb_probe_regularizers(const void *probe, int32_t M, int32_t N, const phb_probe_reg *reg, void *grad,
+                           double *loss, void *scratch, void *stream);
+size_t phb_object_recip_l1_scratch_bytes(int64_t S, int64_t H, int64_t W);
+int phb_object_recip_l1(const void *obj, int64_t S, int64_t H, int64_t W, float cost, void *grad, double *loss,
+                        void *scratch, void *stream);
+
 /* ---------------------------------------------------- learned warm start
  * A small convolutional network (no counterpart in the reference) predicts the
  * object patch under the probe from each diffraction pattern; the stitched

@@ -848,10 +848,20 @@ def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sa
             L, g_obj, g_probe, g_pos = grad_model_grads(geom, probe, obj, flat_scan[idx], flat_pat[idx], mask,
                                                         props, tl, run.noise)
             if run.regularizers:
-                # cost regularisers join the loss and the object gradient (gradient/run.py:398-403)
-                r_cost, r_grad = obj_regularizer_costs(obj, run.regularizers, B / flat_scan.shape[0], run.tv_eps)
+                # cost regularisers join the loss and the gradients (gradient/run.py:398-403)
+                regs = run.regularizers
+                r_cost, r_grad = obj_regularizer_costs(obj, regs, B / flat_scan.shape[0], run.tv_eps)
                 L = L + r_cost
                 g_obj = g_obj + r_grad
+                if regs.get('obj_recip_l1'):
+                    r_cost, r_grad = obj_recip_l1(obj, regs['obj_recip_l1'], B / flat_scan.shape[0])
+                    L = L + r_cost
+                    g_obj = g_obj + r_grad
+                pr = {k: v for (k, v) in regs.items() if k.startswith('probe_')}
+                if pr:
+                    r_cost, r_grad = probe_regularizer_costs(probe, pr, run.tv_eps)
+                    L = L + r_cost
+                    g_probe = g_probe + r_grad
             d = {'object': -g_obj / (probe_int * B), 'probe': -g_probe / B,
                  'positions': -g_pos / (probe_int * B)}
             d = {k: v.astype(params[k].dtype) for (k, v) in d.items() if k in iter_vars}
@@ -1020,3 +1030,73 @@ def obj_regularizer_costs(obj, costs: t.Mapping[str, float], scale: float, tv_ep
             g[1:] += u
             grad += c('layers_tv') * g
     return float(total) * scale, (grad * scale).astype(obj.dtype)
+
+
+def obj_recip_l1(obj, cost: float, scale: float):
+    """ObjRecipL1 (regularizers.py:233-253): cost * scale * sum |fft2(prod_s O_s)|.
+    The centring shift of fft2 only multiplies the spectrum by a phase ramp, so the
+    magnitudes are those of the plain DFT.  Returns (value, gradient on O)."""
+    S = obj.shape[0]
+    P = numpy.prod(obj, axis=0)
+    n = P.size
+    Z = numpy.fft.fft2(P) / numpy.sqrt(n)
+    m = numpy.abs(Z)
+    gP = numpy.fft.ifft2(numpy.where(m > 0, Z / numpy.where(m > 0, m, 1), 0)) * numpy.sqrt(n)
+    grad = numpy.empty_like(obj)
+    for s in range(S):
+        others = numpy.prod(numpy.delete(obj, s, axis=0), axis=0) if S > 1 else numpy.ones_like(P)
+        grad[s] = gP * numpy.conj(others)
+    return float(numpy.sum(m)) * cost * scale, (grad * cost * scale).astype(obj.dtype)
+
+
+def _tikh(R):
+    """sum |diff_x R|^2 + |diff_y R|^2 over the last two axes and its gradient (g convention)."""
+    total = 0.0
+    g = numpy.zeros_like(R)
+    for ax in (-1, -2):
+        d = numpy.diff(R, axis=ax)
+        total += float(numpy.sum(numpy.abs(d) ** 2))
+        lo = [slice(None)] * R.ndim
+        hi = [slice(None)] * R.ndim
+        lo[ax], hi[ax] = slice(None, -1), slice(1, None)
+        g[tuple(lo)] -= 2 * d
+        g[tuple(hi)] += 2 * d
+    return total, g
+
+
+def probe_regularizer_costs(probe, costs: t.Mapping[str, float], tv_eps: float = 1e-8):
+    """Probe cost regularisers (regularizers.py:354-426), scale 1:
+    probe_phase_tikh  sum |diff angle(fft2 P)|^2 (no unwrapping),
+    probe_recip_tikh  sum |diff fftshift(fft2 P)|^2,
+    probe_recip_tv    sum sqrt(|g_y|^2 + |g_x|^2 + eps) of fftshift(fft2 P) (forward
+                      differences, zero at the far edge).
+    fft2 is unitary, so the probe gradient is ifft2 of the spectrum gradient.
+    Returns (value, gradient on P)."""
+    R = fft2c(probe)
+    total = 0.0
+    gR = numpy.zeros_like(R)
+    c = costs.get
+    if c('probe_phase_tikh'):
+        th = numpy.angle(R)
+        v, gth = _tikh(th.astype(numpy.float64))
+        total += c('probe_phase_tikh') * v
+        m2 = numpy.abs(R) ** 2
+        gR += c('probe_phase_tikh') * gth * 1j * R / numpy.where(m2 > 0, m2, 1)
+    Rs = numpy.fft.fftshift(R, axes=(-1, -2))
+    gRs = numpy.zeros_like(Rs)
+    if c('probe_recip_tikh'):
+        v, g = _tikh(Rs)
+        total += c('probe_recip_tikh') * v
+        gRs += c('probe_recip_tikh') * g
+    if c('probe_recip_tv'):
+        gy = numpy.diff(Rs, axis=-2, append=Rs[..., -1:, :])
+        gx = numpy.diff(Rs, axis=-1, append=Rs[..., :, -1:])
+        tv = numpy.sqrt(numpy.abs(gy) ** 2 + numpy.abs(gx) ** 2 + tv_eps)
+        total += c('probe_recip_tv') * float(numpy.sum(tv))
+        uy, ux = gy / tv, gx / tv
+        g = -(uy + ux)
+        g[..., 1:, :] += uy[..., :-1, :]
+        g[..., :, 1:] += ux[..., :, :-1]
+        gRs += c('probe_recip_tv') * g
+    gR += numpy.fft.ifftshift(gRs, axes=(-1, -2))
+    return total, ifft2c(gR).astype(probe.dtype)

@@ -82,6 +82,11 @@ class PhbObjReg(ctypes.Structure):
                                       'scale')]
 
 
+class PhbProbeReg(ctypes.Structure):
+    """Mirror of `phb_probe_reg` (include/phaser_b200.h)."""
+    _fields_ = [(n, c_f32) for n in ('phase_tikh', 'recip_tikh', 'recip_tv', 'tv_eps')]
+
+
 class PhbOptim(ctypes.Structure):
     """Mirror of `phb_optim` (include/phaser_b200.h)."""
     _fields_ = [
@@ -153,6 +158,11 @@ _SIGNATURES = {
                                    c_void_p, c_void_p, c_i64, c_i64, c_void_p]),
     'phb_stitch_finish': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p]),
     'phb_project_slices': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p]),
+    'phb_probe_regularizers_scratch_bytes': (ctypes.c_size_t, [c_i32, c_i32]),
+    'phb_probe_regularizers': (c_i32, [c_void_p, c_i32, c_i32, ctypes.POINTER(PhbProbeReg), c_void_p, c_void_p,
+                                       c_void_p, c_void_p]),
+    'phb_object_recip_l1_scratch_bytes': (ctypes.c_size_t, [c_i64, c_i64, c_i64]),
+    'phb_object_recip_l1': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_f32, c_void_p, c_void_p, c_void_p, c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),

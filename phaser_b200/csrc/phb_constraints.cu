@@ -262,6 +262,102 @@ __global__ void k_obj_reg(const float2 *obj, int64_t S, int64_t H, int64_t W, co
     if (loss) warp_atomic_sum(loss, acc * (double)r.scale);
 }
 
+// ------------------------------------------- Fourier-space cost regularisers
+// probe costs on R = fft2(P) (M, N, N), natural order; the recip terms act on
+// fftshift(R).  Writes dL/dR (g convention) to gR and adds the value to *loss.
+__global__ void k_probe_reg(const float2 *R, int64_t M, int N, const phb_probe_reg r, float2 *gR, double *loss) {
+    const int64_t NN = (int64_t)N * N, total = M * NN;
+    const int h = N / 2;
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = i / NN;
+        const int y = (int)(i % NN / N), x = (int)(i % N);
+        const float2 *Rm = R + m * NN;
+        float2 g = make_float2(0.f, 0.f);
+        double c = 0.0;
+        if (r.phase_tikh != 0.f) {   // sum of squared differences of angle(R), no unwrapping
+            auto th = [&](int yy, int xx) { const float2 v = Rm[yy * N + xx]; return atan2f(v.y, v.x); };
+            const float t0 = th(y, x);
+            float d = 0.f;   // dL/dtheta at (y, x)
+            if (x + 1 < N) { const float e = th(y, x + 1) - t0; c += (double)e * e; d -= 2.f * e; }
+            if (x > 0) d += 2.f * (t0 - th(y, x - 1));
+            if (y + 1 < N) { const float e = th(y + 1, x) - t0; c += (double)e * e; d -= 2.f * e; }
+            if (y > 0) d += 2.f * (t0 - th(y - 1, x));
+            c *= r.phase_tikh;
+            const float2 v = Rm[y * N + x];
+            const float m2 = cabs2(v);
+            if (m2 > 0.f) g = cadd(g, cscale(make_float2(-v.y, v.x), r.phase_tikh * d / m2));   // d * i R / |R|^2
+        }
+        if (r.recip_tikh != 0.f || r.recip_tv != 0.f) {
+            // shifted coordinates: Rs(ys, xs) = R((ys + h) % N, (xs + h) % N); this element is Rs(ys, xs)
+            const int ys = (y + h) % N, xs = (x + h) % N;
+            auto rs = [&](int yy, int xx) { return Rm[((yy + h) % N) * N + (xx + h) % N]; };
+            const float2 v = Rm[y * N + x];
+            if (r.recip_tikh != 0.f) {
+                if (xs + 1 < N) { const float2 e = csub(rs(ys, xs + 1), v); c += (double)r.recip_tikh * cabs2(e);
+                                  g = csub(g, cscale(e, 2.f * r.recip_tikh)); }
+                if (xs > 0) g = cadd(g, cscale(csub(v, rs(ys, xs - 1)), 2.f * r.recip_tikh));
+                if (ys + 1 < N) { const float2 e = csub(rs(ys + 1, xs), v); c += (double)r.recip_tikh * cabs2(e);
+                                  g = csub(g, cscale(e, 2.f * r.recip_tikh)); }
+                if (ys > 0) g = cadd(g, cscale(csub(v, rs(ys - 1, xs)), 2.f * r.recip_tikh));
+            }
+            if (r.recip_tv != 0.f) {
+                auto term = [&](int yy, int xx, float2 *gy, float2 *gx) {
+                    const float2 w = rs(yy, xx);
+                    *gy = (yy + 1 < N) ? csub(rs(yy + 1, xx), w) : make_float2(0.f, 0.f);
+                    *gx = (xx + 1 < N) ? csub(rs(yy, xx + 1), w) : make_float2(0.f, 0.f);
+                    return sqrtf(cabs2(*gy) + cabs2(*gx) + r.tv_eps);
+                };
+                float2 gy, gx;
+                const float t0 = term(ys, xs, &gy, &gx);
+                c += (double)r.recip_tv * t0;
+                g = csub(g, cscale(cadd(gy, gx), r.recip_tv / t0));
+                if (ys > 0) { const float t1 = term(ys - 1, xs, &gy, &gx); g = cadd(g, cscale(gy, r.recip_tv / t1)); }
+                if (xs > 0) { const float t2 = term(ys, xs - 1, &gy, &gx); g = cadd(g, cscale(gx, r.recip_tv / t2)); }
+            }
+        }
+        acc += c;
+        if (gR) gR[i] = g;
+    }
+    if (loss) warp_atomic_sum(loss, acc);
+}
+
+// U = Z / |Z| (0 where Z = 0); *loss += scale * sum |Z|
+__global__ void k_unit_phase(float2 *Z, int64_t n, float scale, double *loss) {
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 z = Z[i];
+        const float m = hypotf(z.x, z.y);
+        acc += m;
+        Z[i] = m > 0.f ? cscale(z, 1.f / m) : make_float2(0.f, 0.f);
+    }
+    if (loss) warp_atomic_sum(loss, acc * (double)scale);
+}
+
+// grad[s] += scale * gP * conj(prod_{t != s} O_t), prefix products kept in `pre` (S, HW)
+__global__ void k_recip_grad(const float2 *obj, int64_t S, int64_t HW, const float2 *gP, float scale, float2 *pre,
+                             float2 *grad) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < HW; i += (int64_t)gridDim.x * blockDim.x) {
+        float2 p = make_float2(1.f, 0.f);
+        for (int64_t s = 0; s < S; ++s) {
+            pre[s * HW + i] = p;
+            p = cmul(p, obj[s * HW + i]);
+        }
+        float2 suf = make_float2(1.f, 0.f);
+        const float2 g = cscale(gP[i], scale);
+        for (int64_t s = S - 1; s >= 0; --s) {
+            const float2 others = cmul(pre[s * HW + i], suf);
+            grad[s * HW + i] = cadd(grad[s * HW + i], cmulc(g, others));
+            suf = cmul(suf, obj[s * HW + i]);
+        }
+    }
+}
+
+__global__ void k_add_c(float2 *dst, const float2 *src, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = cadd(dst[i], src[i]);
+}
+
 }  // namespace phb
 
 using namespace phb;
@@ -333,6 +429,58 @@ int phb_object_regularizers(const void *obj, int64_t S, int64_t H, int64_t W, co
     if (!obj || !reg || S < 1 || H < 1 || W < 1 || (!grad && !loss)) return PHB_ERR_INVALID_ARG;
     k_obj_reg<<<flat_grid(S * H * W), 256, 0, (cudaStream_t)stream>>>((const float2 *)obj, S, H, W, *reg,
                                                                        (float2 *)grad, loss);
+    return check_launch();
+}
+
+size_t phb_probe_regularizers_scratch_bytes(int32_t M, int32_t N) {
+    return (M < 1 || N < 1) ? 0 : (size_t)2 * M * N * N * sizeof(float2);
+}
+
+int phb_probe_regularizers(const void *probe, int32_t M, int32_t N, const phb_probe_reg *reg, void *grad,
+                           double *loss, void *scratch, void *stream) {
+    if (!probe || !reg || !scratch || M < 1 || (!grad && !loss)) return PHB_ERR_INVALID_ARG;
+    if (N != 64 && N != 128) return PHB_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = (int64_t)M * N * N;
+    float2 *R = (float2 *)scratch, *gR = R + n;
+    int rc = phb_fft2_c64(probe, R, M, N, 0, stream);
+    if (rc) return rc;
+    k_probe_reg<<<flat_grid(n), 256, 0, st>>>(R, M, N, *reg, grad ? gR : nullptr, loss);
+    if ((rc = check_launch())) return rc;
+    if (!grad) return PHB_OK;
+    if ((rc = phb_fft2_c64(gR, R, M, N, 1, stream))) return rc;   // fft2 is unitary: adjoint = ifft2
+    k_add_c<<<flat_grid(n), 256, 0, st>>>((float2 *)grad, R, n);
+    return check_launch();
+}
+
+size_t phb_object_recip_l1_scratch_bytes(int64_t S, int64_t H, int64_t W) {
+    return (S < 1 || H < 1 || W < 1) ? 0 : (size_t)(2 + S) * H * W * sizeof(float2);
+}
+
+int phb_object_recip_l1(const void *obj, int64_t S, int64_t H, int64_t W, float cost, void *grad, double *loss,
+                        void *scratch, void *stream) {
+    if (!obj || !scratch || S < 1 || H < 1 || W < 1 || (!grad && !loss)) return PHB_ERR_INVALID_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t HW = H * W;
+    float2 *a = (float2 *)scratch, *b = a + HW, *pre = b + HW;
+    int rc = phb_project_slices(obj, S, HW, a, stream);
+    if (rc) return rc;
+    const float sc = (float)(1.0 / sqrt((double)HW));
+    auto grid = [&](int64_t R, int64_t C) { return dim3((unsigned)((C + DT - 1) / DT), (unsigned)((R + DT - 1) / DT), 1u); };
+    // Z = DFT2(P) / sqrt(HW) (the centring shift of fft2 changes only the phases of Z)
+    k_dft_t<<<grid(H, W), 256, 0, st>>>(a, b, H, W, -1, 1.f, nullptr);
+    if ((rc = check_launch())) return rc;
+    k_dft_t<<<grid(W, H), 256, 0, st>>>(b, a, W, H, -1, sc, nullptr);
+    if ((rc = check_launch())) return rc;
+    k_unit_phase<<<flat_grid(HW), 256, 0, st>>>(a, HW, cost, loss);
+    if ((rc = check_launch())) return rc;
+    if (!grad) return PHB_OK;
+    // gP = IDFT2(Z / |Z|) / sqrt(HW), then the product rule over slices
+    k_dft_t<<<grid(H, W), 256, 0, st>>>(a, b, H, W, +1, 1.f, nullptr);
+    if ((rc = check_launch())) return rc;
+    k_dft_t<<<grid(W, H), 256, 0, st>>>(b, a, W, H, +1, sc, nullptr);
+    if ((rc = check_launch())) return rc;
+    k_recip_grad<<<flat_grid(HW), 256, 0, st>>>((const float2 *)obj, S, HW, a, cost, pre, (float2 *)grad);
     return check_launch();
 }
 

@@ -15,10 +15,10 @@ the reference:
               group directions, update minus its mean; iteration constraints;
               positions checked against the object.
 
-Cost regularisers on the object (obj_l1, obj_l2, obj_phase_l1, obj_tv,
-obj_tikh, layers_tv, layers_tikh) add their value to each group's loss and
-their gradient to the object gradient (phb_object_regularizers); the
-Fourier-space and probe regularisers and tilt updates raise NotImplementedError.
+Every cost regulariser of the reference (object: obj_l1, obj_l2, obj_phase_l1,
+obj_recip_l1, obj_tv, obj_tikh, layers_tv, layers_tikh; probe: probe_phase_tikh,
+probe_recip_tikh, probe_recip_tv) adds its value to each group's loss and its
+gradient to the object / probe gradient; tilt updates raise NotImplementedError.
 """
 from __future__ import annotations
 
@@ -131,20 +131,27 @@ class DeviceSolver:
             _lib.call('phb_optimizer_update', ctypes.byref(o), _stream())
 
 
-_REG_ALIASES = {'obj_tikhonov': 'obj_tikh', 'layers_tikhonov': 'layers_tikh'}
+_REG_ALIASES = {'obj_tikhonov': 'obj_tikh', 'layers_tikhonov': 'layers_tikh',
+                'probe_phase_tikhonov': 'probe_phase_tikh', 'probe_recip_tikhonov': 'probe_recip_tikh'}
 _REG_FIELDS = {'obj_l1': 'l1', 'obj_l2': 'l2', 'obj_phase_l1': 'phase_l1', 'obj_tv': 'tv', 'obj_tikh': 'tikh',
                'layers_tv': 'layers_tv', 'layers_tikh': 'layers_tikh'}
+_PROBE_FIELDS = {'probe_phase_tikh': 'phase_tikh', 'probe_recip_tikh': 'recip_tikh', 'probe_recip_tv': 'recip_tv'}
 
 
 class CostRegularizers:
-    """The plan's cost regularisers (phaser/engines/common/regularizers.py:195-351),
+    """The plan's cost regularisers (phaser/engines/common/regularizers.py:195-426),
     evaluated once per group on the device: value into the group loss, gradient
-    into the object gradient, all scaled by B / n_pos."""
+    into the object / probe gradient.  Object terms are scaled by B / n_pos,
+    probe terms by 1, as in the reference."""
 
     def __init__(self, hooks: t.Sequence[t.Any]):
         self.reg = _lib.PhbObjReg()
         self.reg.tv_eps = 1e-8
-        self.active = False
+        self.preg = _lib.PhbProbeReg()
+        self.preg.tv_eps = 1e-8
+        self.recip_l1 = 0.0
+        self.active = self.probe_active = False
+        self._scratch: t.Dict[str, torch.Tensor] = {}
         for h in hooks or []:
             if isinstance(h, str):
                 name, props = h, {}
@@ -156,20 +163,49 @@ class CostRegularizers:
                 props = getattr(h, 'props', None) or {}
                 name = P._REF_CLASS_NAMES.get(str(name).rsplit(':', 1)[-1], name)
             name = _REG_ALIASES.get(str(name), str(name))
-            field = _REG_FIELDS.get(name)
-            if field is None:
+            cost = float(P.get(props, 'cost'))
+            if name in _REG_FIELDS:
+                field = _REG_FIELDS[name]
+                setattr(self.reg, field, getattr(self.reg, field) + cost)
+                if name == 'obj_tv':
+                    self.reg.tv_eps = float(P.get(props, 'eps', 1e-8))
+                self.active = True
+            elif name == 'obj_recip_l1':
+                self.recip_l1 += cost
+            elif name in _PROBE_FIELDS:
+                field = _PROBE_FIELDS[name]
+                setattr(self.preg, field, getattr(self.preg, field) + cost)
+                if name == 'probe_recip_tv':
+                    self.preg.tv_eps = float(P.get(props, 'eps', 1e-8))
+                self.probe_active = True
+            else:
                 raise NotImplementedError(f"cost regularizer '{name}' is not implemented by the B200 backend")
-            setattr(self.reg, field, getattr(self.reg, field) + float(P.get(props, 'cost')))
-            if name == 'obj_tv':
-                self.reg.tv_eps = float(P.get(props, 'eps', 1e-8))
-            self.active = True
 
-    def apply(self, eng, B: int, grad: t.Optional[torch.Tensor], loss: torch.Tensor) -> None:
-        if not self.active:
-            return
-        self.reg.scale = float(B) / float(eng.n_pos)
-        _lib.call('phb_object_regularizers', eng.object.data_ptr(), eng.S, eng.H, eng.W, ctypes.byref(self.reg),
-                  0 if grad is None else grad.data_ptr(), loss.data_ptr(), _stream())
+    def _buf(self, key: str, nbytes: int, device) -> torch.Tensor:
+        b = self._scratch.get(key)
+        if b is None or b.numel() < nbytes:
+            b = torch.empty((nbytes,), dtype=torch.uint8, device=device)
+            self._scratch[key] = b
+        return b
+
+    def apply(self, eng, B: int, grad: t.Optional[torch.Tensor], loss: torch.Tensor,
+              grad_probe: t.Optional[torch.Tensor] = None) -> None:
+        scale = float(B) / float(eng.n_pos)
+        st = _stream()
+        if self.active:
+            self.reg.scale = scale
+            _lib.call('phb_object_regularizers', eng.object.data_ptr(), eng.S, eng.H, eng.W, ctypes.byref(self.reg),
+                      0 if grad is None else grad.data_ptr(), loss.data_ptr(), st)
+        if self.recip_l1:
+            n = eng.lib.phb_object_recip_l1_scratch_bytes(eng.S, eng.H, eng.W)
+            buf = self._buf('recip', n, eng.device)
+            _lib.call('phb_object_recip_l1', eng.object.data_ptr(), eng.S, eng.H, eng.W, self.recip_l1 * scale,
+                      0 if grad is None else grad.data_ptr(), loss.data_ptr(), buf.data_ptr(), st)
+        if self.probe_active:
+            n = eng.lib.phb_probe_regularizers_scratch_bytes(eng.M, eng.N)
+            buf = self._buf('probe', n, eng.device)
+            _lib.call('phb_probe_regularizers', eng.probe.data_ptr(), eng.M, eng.N, ctypes.byref(self.preg),
+                      0 if grad_probe is None else grad_probe.data_ptr(), loss.data_ptr(), buf.data_ptr(), st)
 
 
 def process_solvers(props) -> t.Tuple[t.FrozenSet[str], t.List[t.Tuple[t.FrozenSet[str], str, t.Any]],
@@ -314,7 +350,8 @@ class GradientEngine:
                      grad_probe=self.grad_probe if 'probe' in iter_vars else None,
                      grad_pos=self.grad_pos if 'positions' in iter_vars else None,
                      grad_pos_scale=-1.0 / (probe_int * B), group_loss=losses[gi:gi + 1])
-            self.regularizers.apply(eng, B, self.grad_object if 'object' in iter_vars else None, losses[gi:gi + 1])
+            self.regularizers.apply(eng, B, self.grad_object if 'object' in iter_vars else None, losses[gi:gi + 1],
+                                    self.grad_probe if 'probe' in iter_vars else None)
             dirs = {}
             if 'object' in iter_vars:
                 dirs['object'] = (self.grad_object, -1.0 / (probe_int * B))

@@ -100,3 +100,53 @@ def test_gradient_run_with_regularizers_matches_oracle():
     assert rel_l2(state.object.data, obj) < 1e-4
     assert rel_l2(state.object.data - c.obj, obj - c.obj) < 1e-2
     assert rel_l2(state.probe.data, probe) < 1e-4
+
+
+def test_probe_and_recip_regularizers_match_oracle(g):
+    rng = numpy.random.default_rng(12)
+    probe = (rng.normal(size=(2, 64, 64)) + 1j * rng.normal(size=(2, 64, 64))).astype(numpy.complex64)
+    pd = torch.from_numpy(probe).cuda()
+    costs = {'probe_phase_tikh': 0.02, 'probe_recip_tikh': 0.03, 'probe_recip_tv': 0.04}
+    reg = _lib.PhbProbeReg(phase_tikh=0.02, recip_tikh=0.03, recip_tv=0.04, tv_eps=1e-6)
+    scratch = torch.empty((2 * 2 * 64 * 64,), dtype=torch.complex64, device='cuda')
+    grad = torch.zeros_like(pd)
+    loss = torch.zeros((1,), dtype=torch.float64, device='cuda')
+    _lib.call('phb_probe_regularizers', pd.data_ptr(), 2, 64, ctypes.byref(reg), grad.data_ptr(), loss.data_ptr(),
+              scratch.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    ref_cost, ref_grad = P.probe_regularizer_costs(probe.astype(numpy.complex128), costs, tv_eps=1e-6)
+    assert float(loss.cpu()[0]) == pytest.approx(ref_cost, rel=1e-4)
+    assert rel_l2(grad.cpu().numpy(), ref_grad) < 1e-4
+    # object: sum |fft2(prod O)| on an odd-sized grid
+    obj = torch.from_numpy(g['obj']).cuda()
+    S, H, W = obj.shape
+    scr = torch.empty(((2 + S) * H * W,), dtype=torch.complex64, device='cuda')
+    grad = torch.zeros_like(obj)
+    loss.zero_()
+    _lib.call('phb_object_recip_l1', obj.data_ptr(), S, H, W, 0.01 * 0.25, grad.data_ptr(), loss.data_ptr(),
+              scr.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    ref_cost, ref_grad = P.obj_recip_l1(g['obj'].astype(numpy.complex128), 0.01, 0.25)
+    assert float(loss.cpu()[0]) == pytest.approx(ref_cost, rel=1e-5)
+    assert rel_l2(grad.cpu().numpy(), ref_grad) < 1e-4
+
+
+def test_gradient_run_with_fourier_regularizers_matches_oracle():
+    c = make_case(seed=94, N=64, M=2, S=2, scan_shape=(5, 5))
+    regs = {'obj_recip_l1': 1e-3, 'probe_recip_tikh': 1e-4, 'probe_recip_tv': 1e-4}
+    props = PL.GradientEnginePlan(
+        solvers={'object': {'type': 'sgd', 'learning_rate': 2.0, 'momentum': 0.5},
+                 'probe': {'type': 'adam', 'learning_rate': 1e-3}},
+        regularizers=[{'type': k, 'cost': v} for (k, v) in regs.items()],
+        noise_model={'type': 'poisson', 'eps': 1e-3}, niter=3, grouping=10)
+    state = run_gradient({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                          'seed': 'reg-seed', 'recons_name': 't'}, props)
+    run = P.GradientRun(solvers={('object',): ('sgd', dict(learning_rate=2.0, momentum=0.5)),
+                                 ('probe',): ('adam', dict(learning_rate=1e-3))},
+                        niter=3, grouping=10, seed='reg-seed', noise=P.NoiseModel(kind='poisson', eps=1e-3),
+                        regularizers=regs)
+    probe, obj, scan, losses = P.run_gradient(
+        run, probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+        probe_sampling=c.probe_sampling, corner=c.osamp.corner, obj_sampling=c.osamp.sampling,
+        thicknesses=c.thick, wavelength=c.wavelength)
+    assert numpy.allclose(state.progress.detector_errors, losses, rtol=1e-4)
+    assert rel_l2(state.object.data, obj) < 1e-4
+    assert rel_l2(state.probe.data, probe) < 1e-4

@@ -195,6 +195,7 @@ def test_autograd_function_matches_oracle_adjoint():
     scan = eng.scan.clone().requires_grad_()
     loss = multislice_loss(obj, probe, scan, eng, gt[0], sizes[0])
     (2.0 * loss).backward()
+    loss = loss.detach()
     L, r_obj, r_probe, r_pos = P.grad_model_grads(
         c.geom(), c.probe, c.obj, c.scan.reshape(-1, 2)[idx], c.patterns.reshape(-1, 64, 64)[idx],
         c.mask, c.props(), None, onoise)

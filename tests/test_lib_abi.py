@@ -39,7 +39,7 @@ def test_host_only_entry_points():
 
 
 STRUCTS = {'phb_engine': _lib.PhbEngine, 'phb_step': _lib.PhbStep, 'phb_optim': _lib.PhbOptim,
-           'phb_obj_reg': _lib.PhbObjReg}
+           'phb_obj_reg': _lib.PhbObjReg, 'phb_probe_reg': _lib.PhbProbeReg}
 
 
 def test_struct_layouts_match_header(tmp_path):

@@ -79,3 +79,38 @@ def test_cost_gradients_match_finite_differences(name):
             fd = (P.obj_regularizer_costs(op, costs, 0.25, tv_eps=1e-3)[0]
                   - P.obj_regularizer_costs(om, costs, 0.25, tv_eps=1e-3)[0]) / (2 * h)
             assert fd == pytest.approx(part[s, y, x], rel=1e-4, abs=1e-6)
+
+
+def test_fourier_and_probe_costs_match_reference(g):
+    ref = dict(zip(g['cost_names'], g['cost_values']))
+    n_pos = g['scan'].shape[0] * g['scan'].shape[1]
+    scale = float(g['cost_group_size']) / n_pos
+    v, _ = P.obj_recip_l1(g['obj'].astype(numpy.complex128), 0.01, scale)
+    assert v == pytest.approx(ref['obj_recip_l1'], rel=1e-4)
+    # the phase of fft2(P) outside the probe aperture is the phase of rounding noise, so
+    # probe_phase_tikh depends on the FFT's rounding (complex64 here as in the reference):
+    # its value agrees to a few percent only
+    for name, cost, rel in (('probe_phase_tikh', 0.02, 3e-2), ('probe_recip_tikh', 0.03, 1e-4),
+                            ('probe_recip_tv', 0.04, 1e-4)):
+        v, _ = P.probe_regularizer_costs(g['probe'], {name: cost}, tv_eps=1e-8)
+        assert v == pytest.approx(ref[name], rel=rel), name
+
+
+def test_fourier_and_probe_cost_gradients_match_finite_differences():
+    rng = numpy.random.default_rng(10)
+    obj = numpy.exp(1j * rng.normal(0, 0.5, (2, 7, 9))) * rng.uniform(0.8, 1.2, (2, 7, 9))
+    probe = (rng.normal(size=(2, 8, 8)) + 1j * rng.normal(size=(2, 8, 8)))
+    h = 1e-6
+    cases = [(lambda o: P.obj_recip_l1(o, 0.3, 0.5), obj)]
+    for name in ('probe_phase_tikh', 'probe_recip_tikh', 'probe_recip_tv'):
+        cases.append((lambda p, name=name: P.probe_regularizer_costs(p, {name: 0.7}, tv_eps=1e-3), probe))
+    for f, x in cases:
+        _, grad = f(x)
+        for _ in range(10):
+            i = tuple(rng.integers(s) for s in x.shape)
+            for unit, part in ((1.0, grad.real), (1j, grad.imag)):
+                xp, xm = x.copy(), x.copy()
+                xp[i] += h * unit
+                xm[i] -= h * unit
+                fd = (f(xp)[0] - f(xm)[0]) / (2 * h)
+                assert fd == pytest.approx(part[i], rel=1e-4, abs=1e-6)
