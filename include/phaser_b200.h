@@ -174,6 +174,7 @@ typedef struct phb_step {
     void *event_end;
     float grad_pos_scale; /* gradient solver: grad_pos = grad_pos_scale * dL/d(y, x) (0 means 1) */
     double *group_loss;   /* gradient solver: optional device double, += the group's summed loss */
+    int32_t b_begin, b_end; /* with PHB_FLAG_PARTIAL: the rows [b_begin, b_end) of the group this call runs */
 } phb_step;
 
 /* Bytes of workspace the engine needs for groups of up to B_max positions. */
@@ -208,6 +209,18 @@ int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, flo
  * (solvers.py:415-504) or the gradient engine's loss and adjoint
  * (gradient/run.py:357-405 under jax.value_and_grad).  Updates object/probe in
  * place (LSQ-ML, ePIE) or accumulates gradients (GRAD). */
+/* Data-parallel split of a mini-batch over ranks (one process per GPU): with
+ * PHB_FLAG_PARTIAL in st->flags, phb_solver_group runs only rows [b_begin, b_end)
+ * of the group and leaves its share in the workspace accumulators.  The caller then
+ * sums, over all ranks, the float32 byte range [out4[0], out4[0] + out4[1]) and the
+ * float64 byte range [out4[2], out4[2] + out4[3]) of the workspace
+ * (phb_engine_reduce_layout) -- one all-reduce each -- and calls
+ * phb_solver_group_finish with the same step, which applies the updates (identical
+ * on every rank).  No counterpart in the reference (single process). */
+#define PHB_FLAG_PARTIAL 16
+int phb_engine_reduce_layout(int32_t N, int32_t M, int32_t S, int32_t B_max, int64_t H, int64_t W, int64_t *out4);
+int phb_solver_group_finish(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B, void *stream);
+
 int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
                      void *stream);
 

@@ -31,6 +31,7 @@ PHB_FLAG_UPDATE_OBJECT = 1
 PHB_FLAG_UPDATE_PROBE = 2
 PHB_FLAG_UPDATE_POSITION = 4
 PHB_FLAG_CALC_ERROR = 8
+PHB_FLAG_PARTIAL = 16
 PHB_STATUS_INTERNAL = 1 << 30
 
 c_void_p = ctypes.c_void_p
@@ -67,7 +68,7 @@ class PhbStep(ctypes.Structure):
         ('grad_object', c_void_p), ('grad_probe', c_void_p), ('grad_pos', c_void_p),
         ('status', c_void_p), ('group_index', c_i32),
         ('group_patterns', c_void_p), ('event_begin', c_void_p), ('event_end', c_void_p),
-        ('grad_pos_scale', c_f32), ('group_loss', c_void_p),
+        ('grad_pos_scale', c_f32), ('group_loss', c_void_p), ('b_begin', c_i32), ('b_end', c_i32),
     ]
 
 
@@ -163,6 +164,9 @@ _SIGNATURES = {
                                        c_void_p, c_void_p]),
     'phb_object_recip_l1_scratch_bytes': (ctypes.c_size_t, [c_i64, c_i64, c_i64]),
     'phb_object_recip_l1': (c_i32, [c_void_p, c_i64, c_i64, c_i64, c_f32, c_void_p, c_void_p, c_void_p, c_void_p]),
+    'phb_engine_reduce_layout': (c_i32, [c_i32, c_i32, c_i32, c_i32, c_i64, c_i64, ctypes.POINTER(c_i64)]),
+    'phb_solver_group_finish': (c_i32, [ctypes.POINTER(PhbEngine), ctypes.POINTER(PhbStep), c_void_p, c_i32,
+                                        c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),

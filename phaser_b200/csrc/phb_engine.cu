@@ -143,6 +143,7 @@ struct GroupArgs {
     float *sim_out;
     const float *group_patterns;
     const uint16_t *patterns16;   // resident uint16 counts (patterns == nullptr then)
+    int b_off;                    // first group row of this launch (partial launches)
 };
 
 // One position's measured pattern: host-streamed float32 rows (group_patterns),
@@ -235,6 +236,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     const int S = a.S;
     const int m = (int)cl.block_rank();
     const int b = blockIdx.x / M;
+    const int bs = b + a.b_off;   // this position's row in the group-wide sums (partial launches)
     const int tid = threadIdx.x;
 
     extern __shared__ float4 smem_raw[];
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int u = 0; u < U; ++u)
 #pragma unroll
                     for (int q = 0; q < E; ++q) n0 += cabs2(v[u][q]);
-                warp_atomic_sum(sums + a.o_pnorm + b, (double)n0);
+                warp_atomic_sum(sums + a.o_pnorm + bs, (double)n0);
             }
             if (upd_obj) {
                 float2 *dst = psi_b + (size_t)s * NN;
@@ -530,7 +532,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
                     if (tid == 0) {
                         if (calc_err) a.errors[pos] = (float)sqrt(t[0]);
-                        if (grad) sums[a.o_loss + b] = t[1];
+                        if (grad) sums[a.o_loss + bs] = t[1];
                     }
                 }
                 fwd = false;
@@ -596,11 +598,11 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 PHB_T_MARK(9);
                 if (lsqml) {
                     if (upd_obj) {
-                        warp_atomic_sum(sums + a.o_numO + (int64_t)b * S + s, (double)t4[0]);
+                        warp_atomic_sum(sums + a.o_numO + (int64_t)bs * S + s, (double)t4[0]);
                         warp_atomic_sum(sums + a.o_denO + s, (double)t4[1]);
                     }
                     if (s == 0 && upd_probe) {
-                        warp_atomic_sum(sums + a.o_numP + (int64_t)b * M + m, (double)t4[2]);
+                        warp_atomic_sum(sums + a.o_numP + (int64_t)bs * M + m, (double)t4[2]);
                         warp_atomic_sum(sums + a.o_denP, (double)t4[3]);
                     }
                 }
@@ -727,8 +729,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         t2[1] += cabs2(pr);
                     }
                 }
-            warp_atomic_sum(sums + a.o_pnum + 2 * b + dir, (double)t2[0]);
-            warp_atomic_sum(sums + a.o_pden + 2 * b + dir, (double)t2[1]);
+            warp_atomic_sum(sums + a.o_pnum + 2 * bs + dir, (double)t2[0]);
+            warp_atomic_sum(sums + a.o_pden + 2 * bs + dir, (double)t2[1]);
             if (dir == 1) return;
             dir = 1;
             load_probe_spectrum(1);
@@ -1369,6 +1371,9 @@ static int simulate(const phb_engine *e, const int64_t *group, int B, float *out
 }
 
 template <int N>
+static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t *group, int B, cudaStream_t st);
+
+template <int N>
 static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *group, int B, cudaStream_t st) {
     int rc = configure_kernels<N>();
     if (rc) return rc;
@@ -1376,7 +1381,12 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     const int mode = sp->solver == PHB_SOLVER_EPIE ? MODE_EPIE : (sp->solver == PHB_SOLVER_GRAD ? MODE_GRAD : MODE_LSQML);
     const int flags = sp->flags;
     const bool upd_obj = flags & PHB_FLAG_UPDATE_OBJECT, upd_probe = flags & PHB_FLAG_UPDATE_PROBE;
-    GroupArgs a = make_args(e, w, mode, flags, group, B);
+    // partial launch: rows [b_begin, b_end) of the group; the accumulators then hold this
+    // share only, and the caller sums them over ranks before phb_solver_group_finish
+    const bool partial = flags & PHB_FLAG_PARTIAL;
+    const int b0 = partial ? sp->b_begin : 0, b1 = partial ? sp->b_end : B;
+    GroupArgs a = make_args(e, w, mode, flags, group + b0, b1 - b0);
+    a.b_off = b0;
     a.errors = sp->errors;
     a.beta_object = sp->beta_object;
     if (mode == MODE_LSQML) {
@@ -1396,6 +1406,21 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     if (sp->event_begin && (rc = record_cuda(cudaEventRecord((cudaEvent_t)sp->event_begin, st)))) return rc;
     if ((rc = launch_group<N>(a, st))) return rc;
     if (sp->event_end && (rc = record_cuda(cudaEventRecord((cudaEvent_t)sp->event_end, st)))) return rc;
+    if (partial) return PHB_OK;
+    return solver_finish<N>(e, sp, group, B, st);
+}
+
+// Step sizes, position / probe / object updates of one mini-batch from the
+// accumulators in the workspace (all of the group's rows present).
+template <int N>
+static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t *group, int B, cudaStream_t st) {
+    int rc = configure_kernels<N>();
+    if (rc) return rc;
+    Workspace w = carve(e->workspace, N, e->M, e->S, e->B_max, e->H, e->W);
+    const int mode = sp->solver == PHB_SOLVER_EPIE ? MODE_EPIE : (sp->solver == PHB_SOLVER_GRAD ? MODE_GRAD : MODE_LSQML);
+    const int flags = sp->flags & ~PHB_FLAG_PARTIAL;
+    const bool upd_obj = flags & PHB_FLAG_UPDATE_OBJECT, upd_probe = flags & PHB_FLAG_UPDATE_PROBE;
+    float *illum = (mode == MODE_LSQML && (upd_obj || e->new_probe_mag)) ? w.illum : nullptr;
 
     FinArgs f{};
     f.mode = mode;
@@ -1418,7 +1443,7 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     k_finalize<<<1, 256, 0, st>>>(f);
     if ((rc = check_launch())) return rc;
 
-    if (mode != MODE_GRAD && (upd_obj || a.illum)) {
+    if (mode != MODE_GRAD && (upd_obj || illum)) {
         ObjApplyArgs o{};
         o.mode = mode;
         o.S = e->S;
@@ -1427,7 +1452,7 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
         o.eps = 1e-16f;
         o.object = (float2 *)e->object;
         o.acc = w.acc_obj;
-        o.illum = a.illum;
+        o.illum = illum;
         o.new_probe_mag = e->new_probe_mag;
         o.coef = w.coef;
         o.status = sp->status;
@@ -1523,6 +1548,27 @@ int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, flo
     return e->N == 128 ? simulate<128>(e, group, B, intensity, st) : simulate<64>(e, group, B, intensity, st);
 }
 
+int phb_solver_group_finish(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B, void *stream) {
+    int rc = validate(e);
+    if (rc) return rc;
+    if (!st || !group || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
+    if (st->solver < PHB_SOLVER_LSQML || st->solver > PHB_SOLVER_GRAD) return PHB_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    return e->N == 128 ? solver_finish<128>(e, st, group, B, s) : solver_finish<64>(e, st, group, B, s);
+}
+
+int phb_engine_reduce_layout(int32_t N, int32_t M, int32_t S, int32_t B_max, int64_t H, int64_t W, int64_t *out4) {
+    if (!out4 || N <= 0 || M <= 0 || S <= 0 || B_max <= 0 || H <= 0 || W <= 0) return PHB_ERR_INVALID_ARG;
+    // carve at a stand-in base address (never dereferenced) to read the offsets
+    char *const origin = reinterpret_cast<char *>(uintptr_t(1) << 20);
+    const Workspace w = carve(origin, N, M, S, B_max, H, W);
+    out4[0] = (int64_t)(reinterpret_cast<char *>(w.acc_obj) - origin);
+    out4[1] = (int64_t)(reinterpret_cast<char *>(w.gom + (size_t)N * N) - reinterpret_cast<char *>(w.acc_obj));
+    out4[2] = (int64_t)(reinterpret_cast<char *>(w.sums) - origin);
+    out4[3] = (int64_t)SumIdx(B_max, S, M).total * (int64_t)sizeof(double);
+    return PHB_OK;
+}
+
 int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B, void *stream) {
     int rc = validate(e);
     if (rc) return rc;
@@ -1536,6 +1582,8 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
     if (st->solver == PHB_SOLVER_GRAD && (st->flags & PHB_FLAG_UPDATE_POSITION) && !st->grad_pos)
         return PHB_ERR_INVALID_ARG;
     if ((st->flags & PHB_FLAG_UPDATE_POSITION) && st->solver != PHB_SOLVER_GRAD && !st->pos_update)
+        return PHB_ERR_INVALID_ARG;
+    if ((st->flags & PHB_FLAG_PARTIAL) && (st->b_begin < 0 || st->b_end > B || st->b_begin >= st->b_end))
         return PHB_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     return e->N == 128 ? solver_group<128>(e, st, group, B, s) : solver_group<64>(e, st, group, B, s);

@@ -184,7 +184,36 @@ class DeviceEngine:
              grad_object: t.Optional[torch.Tensor] = None, grad_probe: t.Optional[torch.Tensor] = None,
              grad_pos: t.Optional[torch.Tensor] = None, loss: t.Optional[torch.Tensor] = None,
              group_patterns: t.Optional[torch.Tensor] = None, events: t.Optional[t.Tuple[int, int]] = None,
-             grad_pos_scale: float = 1.0, group_loss: t.Optional[torch.Tensor] = None) -> None:
+             grad_pos_scale: float = 1.0, group_loss: t.Optional[torch.Tensor] = None,
+             rows: t.Optional[t.Tuple[int, int]] = None) -> None:
+        """One mini-batch step (phb_solver_group).  With `rows` = (b0, b1) only those
+        rows of the group run (PHB_FLAG_PARTIAL): sum reduce_views() over ranks, then
+        call finish()."""
+        st = self._step_struct(solver, flags, beta_object, beta_probe, illum_reg_object, illum_reg_probe, gamma,
+                               group_index, grad_object, grad_probe, grad_pos, loss, group_patterns, events,
+                               grad_pos_scale, group_loss, rows)
+        self._last_step = st
+        _lib.call('phb_solver_group', self._eref, ctypes.byref(st), group.data_ptr(), int(B), _stream())
+
+    def finish(self, group: torch.Tensor, B: int) -> None:
+        """Apply the mini-batch updates from the (rank-summed) accumulators of the last
+        partial step (phb_solver_group_finish)."""
+        st = _lib.PhbStep.from_buffer_copy(self._last_step)
+        st.flags = int(st.flags) & ~_lib.PHB_FLAG_PARTIAL
+        _lib.call('phb_solver_group_finish', self._eref, ctypes.byref(st), group.data_ptr(), int(B), _stream())
+
+    def reduce_views(self) -> t.Tuple[torch.Tensor, torch.Tensor]:
+        """float32 and float64 views of the workspace accumulators a partial step fills
+        (phb_engine_reduce_layout): the buffers ranks sum before `finish`."""
+        out = (ctypes.c_int64 * 4)()
+        _lib.call('phb_engine_reduce_layout', self.N, self.M, self.S, self.group_max, self.H, self.W, out)
+        f32 = self.workspace[out[0]:out[0] + out[1]].view(torch.float32)
+        f64 = self.workspace[out[2]:out[2] + out[3]].view(torch.float64)
+        return f32, f64
+
+    def _step_struct(self, solver, flags, beta_object, beta_probe, illum_reg_object, illum_reg_probe, gamma,
+                     group_index, grad_object, grad_probe, grad_pos, loss, group_patterns, events, grad_pos_scale,
+                     group_loss, rows) -> _lib.PhbStep:
         st = _lib.PhbStep()
         st.solver, st.flags = SOLVERS[solver], int(flags)
         st.beta_object, st.beta_probe = float(beta_object), float(beta_probe)
@@ -198,7 +227,10 @@ class DeviceEngine:
         st.grad_pos_scale, st.group_loss = float(grad_pos_scale), _ptr(group_loss)
         if events is not None:
             st.event_begin, st.event_end = events
-        _lib.call('phb_solver_group', self._eref, ctypes.byref(st), group.data_ptr(), int(B), _stream())
+        if rows is not None:
+            st.flags = int(st.flags) | _lib.PHB_FLAG_PARTIAL
+            st.b_begin, st.b_end = int(rows[0]), int(rows[1])
+        return st
 
     def simulate(self, group: torch.Tensor, B: int, out: t.Optional[torch.Tensor] = None) -> torch.Tensor:
         """Far-field intensity of the forward model for one group, (B, N, N)."""

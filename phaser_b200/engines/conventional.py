@@ -171,7 +171,7 @@ class ConventionalEngine:
             if self.fused_events is not None:
                 ev = _new_event_pair()
                 self.fused_events.append(ev)
-            eng.step(self.solver_kind, gt[gi], B, flags=f, group_index=gi, events=ev, **sched)
+            self._group_step(gt[gi], B, f, gi, ev, sched)
             for con in self.group_cons:
                 con.apply_group()
         for con in self.iter_cons:
@@ -186,11 +186,19 @@ class ConventionalEngine:
             eng.position_update(self.mom_state, step, maxs, float(P.get(pp, 'momentum', 0.9)))
         # one device->host status block per iteration
         eng.iteration_report(eng.report)
+        self._combine_report(eng.report)
         self.status_host.copy_(eng.report, non_blocking=True)
         if not sync:
             return None
         torch.cuda.current_stream().synchronize()
         return self.check(i, it_pos, it_err)
+
+    def _group_step(self, group: torch.Tensor, B: int, flags: int, gi: int, events, sched) -> None:
+        """One mini-batch on this device (the data-parallel engine splits it over ranks)."""
+        self.eng.step(self.solver_kind, group, B, flags=flags, group_index=gi, events=events, **sched)
+
+    def _combine_report(self, report: torch.Tensor) -> None:
+        """Hook for combining the iteration report over ranks (single device: nothing)."""
 
     def check(self, i: int, it_pos: bool = True, it_err: bool = True) -> t.Optional[float]:
         state, eng = self.state, self.eng
