@@ -113,6 +113,7 @@ int phb_fourier_mask_c64(void *arr, int64_t batch, int64_t N, const float *mask,
 #define PHB_FLAG_UPDATE_OBJECT   1
 #define PHB_FLAG_UPDATE_PROBE    2
 #define PHB_FLAG_UPDATE_POSITION 4
+#define PHB_FLAG_UPDATE_TILT   32   /* gradient solver: per-position tilt gradient (needs phb_engine.tilt) */
 #define PHB_FLAG_CALC_ERROR      8
 
 #define PHB_STATUS_INTERNAL (1 << 30)   /* flag bit in phb_step.status: kernel aborted its program */
@@ -175,6 +176,8 @@ typedef struct phb_step {
     float grad_pos_scale; /* gradient solver: grad_pos = grad_pos_scale * dL/d(y, x) (0 means 1) */
     double *group_loss;   /* gradient solver: optional device double, += the group's summed loss */
     int32_t b_begin, b_end; /* with PHB_FLAG_PARTIAL: the rows [b_begin, b_end) of the group this call runs */
+    float *grad_tilt;     /* gradient solver with PHB_FLAG_UPDATE_TILT: (n_pos, 2) dL/d(tilt y, tilt x) [1/mrad] */
+    float grad_tilt_scale;/* grad_tilt = grad_tilt_scale * dL/dtilt (0 means 1) */
 } phb_step;
 
 /* Bytes of workspace the engine needs for groups of up to B_max positions. */

@@ -681,7 +681,8 @@ def noise_dloss_dI(noise: NoiseModel, intensity, patterns, mask):
     return -2. * mask * (numpy.sqrt(pat + noise.offset) - sI - noise.eps) / (var * sI)
 
 
-def grad_model_grads(geom, probe, obj, group_scan, patterns, mask, props, tilts, noise: NoiseModel):
+def grad_model_grads(geom, probe, obj, group_scan, patterns, mask, props, tilts, noise: NoiseModel,
+                     with_tilt: bool = False):
     """Loss and gradients of the gradient-engine model (the adjoint of
     phaser/engines/gradient/run.py:357-405 that jax.value_and_grad evaluates).
 
@@ -700,17 +701,29 @@ def grad_model_grads(geom, probe, obj, group_scan, patterns, mask, props, tilts,
     g_wave = 2. * noise_dloss_dI(noise, intensity, patterns, mask)[:, None] * wave
     g = ifft2c(g_wave)
     g_obj = numpy.zeros_like(obj)
+    g_tilt = numpy.zeros((len(group_scan), 2))
     for s in range(S - 1, -1, -1):
         add_cutouts(g_obj[s], starts, numpy.sum(g * numpy.conj(psi[s]), axis=1))
         g = g * numpy.conj(cuts[:, s, None])
         if s > 0:
-            g = ifft2c(fft2c(g) * numpy.conj(props_t[s - 1])[:, None])
+            G = fft2c(g)
+            if with_tilt and tilts is not None:
+                # psi_s = ifft2c(fft2c(psi_{s-1} O_{s-1}) P_{s-1} T), dT/dtheta = T 2 pi i dz k (1 + tan^2) 1e-3
+                Y = fft2c(psi[s])
+                dz = float(geom.thicknesses[s - 1])
+                for j, k in enumerate((geom.ky, geom.kx)):
+                    d = numpy.real(numpy.conj(G) * Y * (2j * numpy.pi * dz * k))
+                    sec2 = 1.0 + numpy.tan(tilts[:, j] * 1e-3) ** 2
+                    g_tilt[:, j] += numpy.sum(d, axis=(1, -1, -2)) * sec2 * 1e-3
+            g = ifft2c(G * numpy.conj(props_t[s - 1])[:, None])
     g_probe = ifft2c(numpy.sum(fft2c(g) * numpy.conj(filt), axis=0))
     pf = fft2c(probe)[None] * filt
     g_pos = []
     for k in (geom.ky, geom.kx):
         d = ifft2c(pf * -2.j * numpy.pi * k)
         g_pos.append(numpy.sum(numpy.real(numpy.conj(g) * d), axis=(1, -1, -2)))
+    if with_tilt:
+        return loss, g_obj, g_probe, numpy.stack(g_pos, axis=-1), g_tilt
     return loss, g_obj, g_probe, numpy.stack(g_pos, axis=-1)
 
 
@@ -789,6 +802,7 @@ class GradientRun:
     update_object: bool = True
     update_probe: bool = True
     update_positions: bool = False
+    update_tilt: bool = False
     bwlim_frac: t.Optional[float] = 2. / 3.
     regularizers: t.Dict[str, float] = dataclasses.field(default_factory=dict)   # name -> cost
     tv_eps: float = 1e-8
@@ -798,7 +812,7 @@ _PER_ITER = ('positions', 'tilt')
 
 
 def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sampling, corner,
-                 obj_sampling, thicknesses, wavelength, tilt=None):
+                 obj_sampling, thicknesses, wavelength, tilt=None, return_tilt: bool = False):
     """Rescale + `niter` iterations of the gradient engine with sparse groupings
     (phaser/engines/gradient/run.py:156-349): per group the model's gradients,
     the descent directions -g / B (probe) and -g / (B sum|P|^2) (others), the
@@ -829,24 +843,27 @@ def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sa
     probe = probe * numpy.sqrt(numpy.mean(numpy.concatenate(factors)))
     probe_int = numpy.sum(abs2(probe))
 
-    params = {'object': obj, 'probe': probe, 'positions': flat_scan}
+    flat_tilt = (numpy.zeros_like(flat_scan) if (flat_tilt is None and any('tilt' in vs for vs in run.solvers))
+                 else flat_tilt)
+    params = {'object': obj, 'probe': probe, 'positions': flat_scan, 'tilt': flat_tilt}
     group_solvers, iter_solvers = [], []
     for (vs, (kind, sp)) in run.solvers.items():
         sol = (frozenset(vs), OptaxNP(kind, sp, {v: params[v] for v in vs}))
         (iter_solvers if set(vs) <= set(_PER_ITER) else group_solvers).append(sol)
-    enabled = {'object': run.update_object, 'probe': run.update_probe, 'positions': run.update_positions}
+    enabled = {'object': run.update_object, 'probe': run.update_probe, 'positions': run.update_positions,
+               'tilt': run.update_tilt}
     iter_vars = {v for sol in group_solvers + iter_solvers for v in sol[0] if enabled.get(v, False)}
 
     losses_out = []
     for it in range(1, run.niter + 1):
-        iter_d = {'positions': numpy.zeros_like(flat_scan)} if 'positions' in iter_vars else {}
+        iter_d = {k: numpy.zeros_like(flat_scan) for k in ('positions', 'tilt') if k in iter_vars}
         losses = []
         for gi, g in enumerate(sparse_groupings(scan_shape, run.grouping, run.seed, it)):
             idx = flat(g)
             B = len(idx)
             tl = None if flat_tilt is None else flat_tilt[idx]
-            L, g_obj, g_probe, g_pos = grad_model_grads(geom, probe, obj, flat_scan[idx], flat_pat[idx], mask,
-                                                        props, tl, run.noise)
+            L, g_obj, g_probe, g_pos, g_tilt = grad_model_grads(geom, probe, obj, flat_scan[idx], flat_pat[idx],
+                                                                mask, props, tl, run.noise, with_tilt=True)
             if run.regularizers:
                 # cost regularisers join the loss and the gradients (gradient/run.py:398-403)
                 regs = run.regularizers
@@ -863,10 +880,11 @@ def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sa
                     L = L + r_cost
                     g_probe = g_probe + r_grad
             d = {'object': -g_obj / (probe_int * B), 'probe': -g_probe / B,
-                 'positions': -g_pos / (probe_int * B)}
+                 'positions': -g_pos / (probe_int * B), 'tilt': -g_tilt / (probe_int * B)}
             d = {k: v.astype(params[k].dtype) for (k, v) in d.items() if k in iter_vars}
-            if 'positions' in d:
-                iter_d['positions'][idx] = d['positions']
+            for k in ('positions', 'tilt'):
+                if k in d:
+                    iter_d[k][idx] = d[k]
             for (vs, sol) in group_solvers:
                 dd = {k: v for (k, v) in d.items() if k in vs}
                 if not dd:
@@ -888,7 +906,11 @@ def run_gradient(run: GradientRun, *, probe, obj, scan, patterns, mask, probe_sa
             if 'positions' in upd:
                 u = upd['positions']
                 flat_scan = flat_scan + (u - numpy.mean(u, axis=0))
+            if 'tilt' in upd:
+                flat_tilt = flat_tilt + upd['tilt']   # no mean subtraction (run.py:119-123)
         losses_out.append(loss)
+    if return_tilt:
+        return probe, obj, flat_scan.reshape(scan.shape), numpy.array(losses_out), flat_tilt
     return probe, obj, flat_scan.reshape(scan.shape), numpy.array(losses_out)
 
 

@@ -32,6 +32,7 @@ PHB_FLAG_UPDATE_PROBE = 2
 PHB_FLAG_UPDATE_POSITION = 4
 PHB_FLAG_CALC_ERROR = 8
 PHB_FLAG_PARTIAL = 16
+PHB_FLAG_UPDATE_TILT = 32
 PHB_STATUS_INTERNAL = 1 << 30
 
 c_void_p = ctypes.c_void_p
@@ -69,6 +70,7 @@ class PhbStep(ctypes.Structure):
         ('status', c_void_p), ('group_index', c_i32),
         ('group_patterns', c_void_p), ('event_begin', c_void_p), ('event_end', c_void_p),
         ('grad_pos_scale', c_f32), ('group_loss', c_void_p), ('b_begin', c_i32), ('b_end', c_i32),
+        ('grad_tilt', c_void_p), ('grad_tilt_scale', c_f32),
     ]
 
 

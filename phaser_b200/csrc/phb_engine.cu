@@ -74,7 +74,7 @@ struct Workspace {
 };
 
 struct SumIdx {
-    int64_t numO, denO, numP, denP, pnum, pden, pnorm, loss, total;
+    int64_t numO, denO, numP, denP, pnum, pden, pnorm, loss, tilt, total;
     __host__ __device__ SumIdx(int B, int S, int M) {
         numO = 0;
         denO = numO + (int64_t)B * S;
@@ -84,7 +84,8 @@ struct SumIdx {
         pden = pnum + 2 * (int64_t)B;
         pnorm = pden + 2 * (int64_t)B;
         loss = pnorm + B;
-        total = loss + B;
+        tilt = loss + B;
+        total = tilt + 2 * (int64_t)B;
     }
 };
 
@@ -133,7 +134,7 @@ struct GroupArgs {
     int32_t *status;       // optional sticky status of the step (see phb_step.status)
     int32_t group_index;
     // float64 accumulator offsets (SumIdx for B_max), precomputed on the host
-    int64_t o_numO, o_denO, o_numP, o_denP, o_pnum, o_pden, o_pnorm, o_loss;
+    int64_t o_numO, o_denO, o_numP, o_denP, o_pnum, o_pden, o_pnorm, o_loss, o_tilt;
     const float *fy, *fx;
     float2 *psi, *acc_obj, *acc_probe;
     float *illum;
@@ -143,7 +144,6 @@ struct GroupArgs {
     float *sim_out;
     const float *group_patterns;
     const uint16_t *patterns16;   // resident uint16 counts (patterns == nullptr then)
-    int b_off;                    // first group row of this launch (partial launches)
 };
 
 // One position's measured pattern: host-streamed float32 rows (group_patterns),
@@ -218,6 +218,7 @@ enum Phase : int {
     PH_BPROP = 4,   // K: adjoint propagation to slice s-1
     PH_PROBE = 5,   // K: probe-update accumulation
     PH_POS = 6,     // R: position-gradient dot products (direction `dir`)
+    PH_TILT = 7,    // K: tilt-gradient dot products of gap s-1 (gradient engine), then BPROP
 };
 
 // MC > 0: the number of probe modes (cluster size) is the compile-time constant MC,
@@ -236,7 +237,6 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     const int S = a.S;
     const int m = (int)cl.block_rank();
     const int b = blockIdx.x / M;
-    const int bs = b + a.b_off;   // this position's row in the group-wide sums (partial launches)
     const int tid = threadIdx.x;
 
     extern __shared__ float4 smem_raw[];
@@ -255,6 +255,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     const bool upd_obj = !presolve && (a.flags & PHB_FLAG_UPDATE_OBJECT);
     const bool upd_probe = !presolve && (a.flags & PHB_FLAG_UPDATE_PROBE);
     const bool upd_pos = !presolve && (a.flags & PHB_FLAG_UPDATE_POSITION);
+    const bool upd_tilt = grad && (a.flags & PHB_FLAG_UPDATE_TILT) && a.tilt != nullptr;
     const bool calc_err = !presolve && !grad && (a.flags & PHB_FLAG_CALC_ERROR) && a.errors;
     const bool do_illum = a.illum && (mode == MODE_LSQML || mode == MODE_PRE_LSQML);
     const bool tilted = a.tilt != nullptr;
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     // The program is 4 S + 2 transforms at most (forward, adjoint, probe, two
     // position directions); the bound turns a logic error into a recorded error
     // (info[3] and the step's status word) instead of a kernel that never ends.
-    const int max_steps = 4 * S + 8;
+    const int max_steps = 5 * S + 8;
     PHB_T_BEGIN();
     for (int step = 0;; ++step) {
         if (step >= max_steps) {
@@ -375,9 +376,9 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int u = 0; u < U; ++u)
 #pragma unroll
                     for (int q = 0; q < E; ++q) n0 += cabs2(v[u][q]);
-                warp_atomic_sum(sums + a.o_pnorm + bs, (double)n0);
+                warp_atomic_sum(sums + a.o_pnorm + b, (double)n0);
             }
-            if (upd_obj) {
+            if (upd_obj || upd_tilt) {   // stored for the adjoint (the tilt gradient transforms it)
                 float2 *dst = psi_b + (size_t)s * NN;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
@@ -532,7 +533,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
                     if (tid == 0) {
                         if (calc_err) a.errors[pos] = (float)sqrt(t[0]);
-                        if (grad) sums[a.o_loss + bs] = t[1];
+                        if (grad) sums[a.o_loss + b] = t[1];
                     }
                 }
                 fwd = false;
@@ -598,11 +599,11 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 PHB_T_MARK(9);
                 if (lsqml) {
                     if (upd_obj) {
-                        warp_atomic_sum(sums + a.o_numO + (int64_t)bs * S + s, (double)t4[0]);
+                        warp_atomic_sum(sums + a.o_numO + (int64_t)b * S + s, (double)t4[0]);
                         warp_atomic_sum(sums + a.o_denO + s, (double)t4[1]);
                     }
                     if (s == 0 && upd_probe) {
-                        warp_atomic_sum(sums + a.o_numP + (int64_t)bs * M + m, (double)t4[2]);
+                        warp_atomic_sum(sums + a.o_numP + (int64_t)b * M + m, (double)t4[2]);
                         warp_atomic_sum(sums + a.o_denP, (double)t4[3]);
                     }
                 }
@@ -678,6 +679,57 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             } else {
                 return;
             }
+        } else if (grad && (phase == PH_TILT || (phase == PH_BPROP && upd_tilt))) {
+            if (phase == PH_BPROP) {
+                // tilt gradient of gap s-1 (gradient/run.py:357-400 through tilt_propagators,
+                // engines/common/simulation.py:193-222): sum_k conj(G) Y 2 pi i dz k (1 + tan^2) 1e-3 / N^2
+                // with G = FFT(adjoint of psi_s) (in v) and Y = FFT(psi_s).  Swap G into psi_s's
+                // stack slot (no longer needed) and transform psi_s.
+                float2 *slot = psi_b + (size_t)s * NN;
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        const int f = I::flat(u, e);
+                        const float2 w = slot[f];
+                        slot[f] = v[u][e];
+                        v[u][e] = w;
+                    }
+                fwd = true;
+                phase = PH_TILT;
+                continue;
+            }
+            const float2 *slot = psi_b + (size_t)s * NN;
+            double ty = 0.0, tx = 0.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const float2 G = slot[I::flat(u, e)];
+                    const float im = G.x * v[u][e].y - G.y * v[u][e].x;   // Im(conj(G) Y)
+                    ty += (double)(im * a.fy[I::ky(u, e)]);
+                    tx += (double)(im * a.fx[I::kx(u, e)]);
+                    v[u][e] = G;
+                }
+            {
+                const double dz = (double)a.thick[s - 1];
+                const double t0 = tan((double)a.tilt[2 * pos] * 1e-3), t1 = tan((double)a.tilt[2 * pos + 1] * 1e-3);
+                const double c = -2.0 * 3.141592653589793 * dz * 1e-3 / (double)NN;   // Re(i z) = -Im z
+                warp_atomic_sum(sums + a.o_tilt + 2 * b, ty * c * (1.0 + t0 * t0));
+                warp_atomic_sum(sums + a.o_tilt + 2 * b + 1, tx * c * (1.0 + t1 * t1));
+            }
+            const uint64_t kband = s_bits[FFT_THREADS + tid];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int ky = I::ky(u, e), kx = I::kx(u, e);
+                    const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
+                    v[u][e] = cscale(cmulc(v[u][e], p), inv_nn);
+                }
+            fwd = false;
+            phase = PH_BACK;
+            --s;
         } else if (phase == PH_BPROP) {
             // ------------------------------------------- adjoint propagation (K layout)
             const uint64_t kband = s_bits[FFT_THREADS + tid];
@@ -729,8 +781,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         t2[1] += cabs2(pr);
                     }
                 }
-            warp_atomic_sum(sums + a.o_pnum + 2 * bs + dir, (double)t2[0]);
-            warp_atomic_sum(sums + a.o_pden + 2 * bs + dir, (double)t2[1]);
+            warp_atomic_sum(sums + a.o_pnum + 2 * b + dir, (double)t2[0]);
+            warp_atomic_sum(sums + a.o_pden + 2 * b + dir, (double)t2[1]);
             if (dir == 1) return;
             dir = 1;
             load_probe_spectrum(1);
@@ -768,6 +820,8 @@ struct FinArgs {
     float *pos_update, *grad_pos, *loss;
     float grad_pos_scale;
     double *group_loss;
+    float *grad_tilt;
+    float grad_tilt_scale;
 };
 
 __global__ void k_finalize(const FinArgs f) {
@@ -827,6 +881,11 @@ __global__ void k_finalize(const FinArgs f) {
             }
             if (f.loss) f.loss[p] = (float)sums[SI.loss + b];
             lsum += sums[SI.loss + b];
+            if (f.grad_tilt && (f.flags & PHB_FLAG_UPDATE_TILT)) {
+                const double ts = f.grad_tilt_scale != 0.f ? (double)f.grad_tilt_scale : 1.0;
+                f.grad_tilt[2 * p] = (float)(ts * sums[SI.tilt + 2 * b]);
+                f.grad_tilt[2 * p + 1] = (float)(ts * sums[SI.tilt + 2 * b + 1]);
+            }
         }
         if (f.group_loss) {
             for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
@@ -1240,6 +1299,7 @@ static GroupArgs make_args(const phb_engine *e, const Workspace &w, int mode, in
     a.o_pden = SI.pden;
     a.o_pnorm = SI.pnorm;
     a.o_loss = SI.loss;
+    a.o_tilt = SI.tilt;
     a.probe_k = w.probe_k;
     a.fy = e->ky;
     a.fx = e->kx;
@@ -1386,7 +1446,15 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     const bool partial = flags & PHB_FLAG_PARTIAL;
     const int b0 = partial ? sp->b_begin : 0, b1 = partial ? sp->b_end : B;
     GroupArgs a = make_args(e, w, mode, flags, group + b0, b1 - b0);
-    a.b_off = b0;
+    if (b0) {   // per-position sums of this launch's rows sit at group rows b0.. (group-wide layout)
+        a.o_numO += (int64_t)b0 * e->S;
+        a.o_numP += (int64_t)b0 * e->M;
+        a.o_pnum += 2 * (int64_t)b0;
+        a.o_pden += 2 * (int64_t)b0;
+        a.o_pnorm += b0;
+        a.o_loss += b0;
+        a.o_tilt += 2 * (int64_t)b0;
+    }
     a.errors = sp->errors;
     a.beta_object = sp->beta_object;
     if (mode == MODE_LSQML) {
@@ -1440,6 +1508,8 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
     f.loss = sp->loss;
     f.grad_pos_scale = sp->grad_pos_scale;
     f.group_loss = sp->group_loss;
+    f.grad_tilt = sp->grad_tilt;
+    f.grad_tilt_scale = sp->grad_tilt_scale;
     k_finalize<<<1, 256, 0, st>>>(f);
     if ((rc = check_launch())) return rc;
 
@@ -1580,6 +1650,8 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
     if (st->solver == PHB_SOLVER_GRAD && (st->flags & PHB_FLAG_UPDATE_PROBE) && !st->grad_probe)
         return PHB_ERR_INVALID_ARG;
     if (st->solver == PHB_SOLVER_GRAD && (st->flags & PHB_FLAG_UPDATE_POSITION) && !st->grad_pos)
+        return PHB_ERR_INVALID_ARG;
+    if ((st->flags & PHB_FLAG_UPDATE_TILT) && (st->solver != PHB_SOLVER_GRAD || !st->grad_tilt || !e->tilt))
         return PHB_ERR_INVALID_ARG;
     if ((st->flags & PHB_FLAG_UPDATE_POSITION) && st->solver != PHB_SOLVER_GRAD && !st->pos_update)
         return PHB_ERR_INVALID_ARG;

@@ -185,13 +185,15 @@ class DeviceEngine:
              grad_pos: t.Optional[torch.Tensor] = None, loss: t.Optional[torch.Tensor] = None,
              group_patterns: t.Optional[torch.Tensor] = None, events: t.Optional[t.Tuple[int, int]] = None,
              grad_pos_scale: float = 1.0, group_loss: t.Optional[torch.Tensor] = None,
-             rows: t.Optional[t.Tuple[int, int]] = None) -> None:
+             rows: t.Optional[t.Tuple[int, int]] = None, grad_tilt: t.Optional[torch.Tensor] = None,
+             grad_tilt_scale: float = 1.0) -> None:
         """One mini-batch step (phb_solver_group).  With `rows` = (b0, b1) only those
         rows of the group run (PHB_FLAG_PARTIAL): sum reduce_views() over ranks, then
         call finish()."""
         st = self._step_struct(solver, flags, beta_object, beta_probe, illum_reg_object, illum_reg_probe, gamma,
                                group_index, grad_object, grad_probe, grad_pos, loss, group_patterns, events,
                                grad_pos_scale, group_loss, rows)
+        st.grad_tilt, st.grad_tilt_scale = _ptr(grad_tilt), float(grad_tilt_scale)
         self._last_step = st
         _lib.call('phb_solver_group', self._eref, ctypes.byref(st), group.data_ptr(), int(B), _stream())
 

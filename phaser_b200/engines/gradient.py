@@ -18,7 +18,10 @@ the reference:
 Every cost regulariser of the reference (object: obj_l1, obj_l2, obj_phase_l1,
 obj_recip_l1, obj_tv, obj_tikh, layers_tv, layers_tikh; probe: probe_phase_tikh,
 probe_recip_tikh, probe_recip_tv) adds its value to each group's loss and its
-gradient to the object / probe gradient; tilt updates raise NotImplementedError.
+gradient to the object / probe gradient.  Tilts (per position, mrad) are
+per-iteration variables like positions: their gradient comes from the fused
+kernel's adjoint through the tilted propagators, and their update is added
+without removing its mean (run.py:119-123).
 """
 from __future__ import annotations
 
@@ -266,6 +269,11 @@ class GradientEngine:
         probe0 = numpy.asarray(state.probe.data)
         obj0 = numpy.asarray(state.object.data)
         self.scan0 = numpy.asarray(state.scan)
+        if 'tilt' in self.all_vars and state.tilt is None:
+            # a zeroed tilt map, as phaser/execute.py:396-400 creates before the engine runs
+            state.tilt = numpy.zeros_like(self.scan0)
+        if 'tilt' in self.all_vars and len(numpy.asarray(state.object.thicknesses)) < 2:
+            raise ValueError("tilt updates need a multislice object")
         if probe0.dtype != numpy.complex64 or obj0.dtype != numpy.complex64:
             raise TypeError("object and probe must be complex64")
         self.eng = eng = DeviceEngine(
@@ -289,6 +297,8 @@ class GradientEngine:
         self.grad_object = torch.zeros_like(eng.object) if 'object' in self.all_vars else None
         self.grad_probe = torch.zeros_like(eng.probe) if 'probe' in self.all_vars else None
         self.grad_pos = torch.zeros_like(eng.scan) if 'positions' in self.all_vars else None
+        self.grad_tilt = torch.zeros_like(eng.tilt) if 'tilt' in self.all_vars else None
+        self.tilt_step = torch.zeros_like(eng.tilt) if 'tilt' in self.all_vars else None
         self.pos_step = torch.zeros_like(eng.scan)
         self.losses = torch.zeros((len(self.groups),), dtype=torch.float64, device=dev)
         self.loss_mean = torch.zeros((1,), dtype=torch.float64, device=dev)
@@ -320,13 +330,12 @@ class GradientEngine:
         state.iter.total_iter = self.start_i + i
         fargs = {'state': state, 'niter': self.niter}
         iter_vars = self.all_vars & {k for (k, f) in self.flags.items() if f(fargs)}
-        if 'tilt' in iter_vars:
-            raise NotImplementedError("tilt updates are not implemented by the B200 backend")
         for sol in self.group_solvers + self.iter_solvers:
             sol.update_for_iter(fargs)
         flags = ((_lib.PHB_FLAG_UPDATE_OBJECT if 'object' in iter_vars else 0)
                  | (_lib.PHB_FLAG_UPDATE_PROBE if 'probe' in iter_vars else 0)
-                 | (_lib.PHB_FLAG_UPDATE_POSITION if 'positions' in iter_vars else 0))
+                 | (_lib.PHB_FLAG_UPDATE_POSITION if 'positions' in iter_vars else 0)
+                 | (_lib.PHB_FLAG_UPDATE_TILT if 'tilt' in iter_vars else 0))
         scan_host = eng.scan.cpu().numpy().reshape(self.scan0.shape) if self.compact else None
         glist = self.groups.iter(scan_host, i, self.shuffle_groups(fargs))
         gt, sizes = eng.group_tensor([self.groups.flat(g) for g in glist])
@@ -349,7 +358,9 @@ class GradientEngine:
                      grad_object=self.grad_object if 'object' in iter_vars else None,
                      grad_probe=self.grad_probe if 'probe' in iter_vars else None,
                      grad_pos=self.grad_pos if 'positions' in iter_vars else None,
-                     grad_pos_scale=-1.0 / (probe_int * B), group_loss=losses[gi:gi + 1])
+                     grad_pos_scale=-1.0 / (probe_int * B), group_loss=losses[gi:gi + 1],
+                     grad_tilt=self.grad_tilt if 'tilt' in iter_vars else None,
+                     grad_tilt_scale=-1.0 / (probe_int * B))
             self.regularizers.apply(eng, B, self.grad_object if 'object' in iter_vars else None, losses[gi:gi + 1],
                                     self.grad_probe if 'probe' in iter_vars else None)
             dirs = {}
@@ -367,11 +378,19 @@ class GradientEngine:
                 con.apply_group()
         torch.mean(losses, dim=0, keepdim=True, out=self.loss_mean)
         for sol in self.iter_solvers:
-            d = {k: (self.grad_pos, 1.0) for k in sol.params if k == 'positions' and 'positions' in iter_vars}
+            d = {}
+            if 'positions' in sol.params and 'positions' in iter_vars:
+                d['positions'] = (self.grad_pos, 1.0)
+            if 'tilt' in sol.params and 'tilt' in iter_vars:
+                d['tilt'] = (self.grad_tilt, 1.0)
             if not d:
                 continue
-            sol.update(self.params, d, self.loss_mean, update_out={'positions': self.pos_step})
-            _lib.call('phb_add_centred', eng.scan.data_ptr(), self.pos_step.data_ptr(), eng.n_pos, _stream())
+            sol.update(self.params, d, self.loss_mean,
+                       update_out={'positions': self.pos_step, 'tilt': self.tilt_step})
+            if 'positions' in d:
+                _lib.call('phb_add_centred', eng.scan.data_ptr(), self.pos_step.data_ptr(), eng.n_pos, _stream())
+            if 'tilt' in d:   # the tilt update keeps its mean (run.py:119-123)
+                eng.tilt.add_(self.tilt_step)
         for con in self.iter_cons:
             con.apply_iter()
         self.loss_host[:1].copy_(self.loss_mean, non_blocking=True)
@@ -405,6 +424,8 @@ class GradientEngine:
         self.state.probe.data = probe
         self.state.object.data = obj
         self.state.scan = scan.astype(self.scan0.dtype)
+        if self.eng.tilt is not None and 'tilt' in self.all_vars:
+            self.state.tilt = self.eng.tilt.cpu().numpy().reshape(self.scan0.shape).astype(self.scan0.dtype)
         _call(self.observer, 'finish_engine', self.state)
         return self.state
 

@@ -207,3 +207,50 @@ def test_autograd_function_matches_oracle_adjoint():
     obj2 = eng.object.clone().requires_grad_()
     (g,) = torch.autograd.grad(multislice_loss(obj2, eng.probe, eng.scan, eng, gt[0], sizes[0]), (obj2,))
     assert rel_l2(g.cpu().numpy(), r_obj) < 1e-4
+
+
+@pytest.mark.parametrize('cfg', [dict(seed=87, N=64, M=2, S=3), dict(seed=88, N=128, M=2, S=4, scan_shape=(3, 3))],
+                         ids=['N64M2S3', 'N128M2S4'])
+def test_tilt_gradient_matches_oracle_adjoint(cfg):
+    c = make_case(tilt=True, **cfg)
+    n = c.scan.shape[0] * c.scan.shape[1]
+    idx = numpy.random.default_rng(9).permutation(n)[: max(2, (2 * n) // 3)].astype(numpy.int64)
+    onoise, spec = NOISES['poisson']
+    eng = DeviceEngine(probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+                       probe_sampling=c.probe_sampling, obj_sampling=c.osamp, thicknesses=c.thick,
+                       wavelength=c.wavelength, tilt=c.tilt, noise=spec, group_max=len(idx))
+    gt, sizes = eng.group_tensor([idx])
+    g_tilt = torch.zeros_like(eng.scan)
+    loss = torch.zeros((1,), dtype=torch.float64, device='cuda')
+    eng.status.fill_(-1)
+    eng.step('grad', gt[0], sizes[0], flags=_lib.PHB_FLAG_UPDATE_TILT, grad_tilt=g_tilt, group_loss=loss)
+    torch.cuda.synchronize()
+    assert int(eng.status.cpu()[0]) == -1
+    tl = c.tilt.reshape(-1, 2)[idx]
+    L, _, _, _, r_tilt = P.grad_model_grads(
+        c.geom(), c.probe, c.obj, c.scan.reshape(-1, 2)[idx], c.patterns.reshape(-1, *c.probe.shape[-2:])[idx],
+        c.mask, c.props(), tl, onoise, with_tilt=True)
+    assert float(loss.cpu()[0]) == pytest.approx(float(L), rel=1e-5)
+    assert rel_l2(g_tilt.cpu().numpy()[idx], r_tilt) < 1e-3
+
+
+def test_run_engine_with_tilt_updates_matches_oracle():
+    c = make_case(seed=95, N=64, M=1, S=3, scan_shape=(4, 4))
+    props = PL.GradientEnginePlan(
+        solvers={'object': {'type': 'sgd', 'learning_rate': 2.0},
+                 'tilt': {'type': 'adam', 'learning_rate': 0.5}},
+        noise_model={'type': 'poisson', 'eps': 1e-3}, niter=3, grouping=8, update_tilt=True)
+    state = run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                        'seed': 'tilt-seed', 'recons_name': 't'}, props)
+    run = P.GradientRun(solvers={('object',): ('sgd', dict(learning_rate=2.0)),
+                                 ('tilt',): ('adam', dict(learning_rate=0.5))},
+                        niter=3, grouping=8, seed='tilt-seed', noise=P.NoiseModel(kind='poisson', eps=1e-3),
+                        update_tilt=True)
+    probe, obj, scan, losses, tilt = P.run_gradient(
+        run, probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+        probe_sampling=c.probe_sampling, corner=c.osamp.corner, obj_sampling=c.osamp.sampling,
+        thicknesses=c.thick, wavelength=c.wavelength, return_tilt=True)
+    assert numpy.allclose(state.progress.detector_errors, losses, rtol=1e-4)
+    assert rel_l2(state.object.data, obj) < 1e-4
+    assert numpy.max(numpy.abs(state.tilt.reshape(-1, 2) - tilt)) < 1e-3 * max(1.0, numpy.max(numpy.abs(tilt)))
+    assert numpy.max(numpy.abs(tilt)) > 0.1   # the tilts moved

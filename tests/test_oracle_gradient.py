@@ -73,3 +73,26 @@ def test_adjoint_matches_finite_differences(noise):
             if (P.cutout_starts(sp[b], g.corner, g.obj_sampling, probe.shape) ==
                     P.cutout_starts(sm[b], g.corner, g.obj_sampling, probe.shape)).all():
                 assert fd == pytest.approx(g_pos[b, d], rel=1e-4, abs=1e-6 * max(1.0, abs(L)))
+
+
+def test_tilt_adjoint_matches_finite_differences():
+    c, probe, obj, pats = f64_case(73, N=32, M=2, S=3, scan_shape=(2, 2), samp=0.3, dz=15.0)
+    g, ky, kx = geom64(c)
+    props = P.make_propagators(ky, kx, c.probe_sampling, c.wavelength, c.thick)
+    scan = c.scan.reshape(-1, 2).astype(numpy.float64)
+    mask = c.mask.astype(numpy.float64)
+    tilts = numpy.random.default_rng(4).normal(0, 3.0, (4, 2))
+    noise = P.NoiseModel(kind='poisson', eps=1e-3)
+
+    def loss(t_):
+        return float(P.grad_model_loss(g, probe, obj, scan, pats, mask, props, t_, noise))
+
+    *_, g_tilt = P.grad_model_grads(g, probe, obj, scan, pats, mask, props, tilts, noise, with_tilt=True)
+    h = 1e-3
+    for i in range(4):
+        for j in range(2):
+            tp, tm = tilts.copy(), tilts.copy()
+            tp[i, j] += h
+            tm[i, j] -= h
+            fd = (loss(tp) - loss(tm)) / (2 * h)
+            assert fd == pytest.approx(g_tilt[i, j], rel=1e-4, abs=1e-8)
