@@ -312,6 +312,16 @@ int phb_object_filter_c64(void *obj, int64_t S, int64_t H, int64_t W, const floa
 int phb_remove_phase_ramp_c64(void *obj, int64_t S, int64_t H, int64_t W, int64_t y0, int64_t y1, int64_t x0,
                               int64_t x1, double *sums, void *stream);
 
+/* UnstructuredGaussian for per-position (n, 2) values such as tilts
+ * (regularizers.py:430-497, 'tilt_gaussian'): nearest-position image on the object
+ * grid, blurred with `filter` (H, W) (exp(-2 pi^2 sigma^2 k^2), fftfreq order), sampled
+ * back at each position's rounded pixel, blended with `weight`.
+ * `scratch`: phb_smooth_positions_scratch_bytes(H, W). */
+size_t phb_smooth_positions_scratch_bytes(int64_t H, int64_t W);
+int phb_smooth_position_values(float *vals, const float *scan, int64_t n, int64_t H, int64_t W, double corner_y,
+                               double corner_x, double samp_y, double samp_x, const float *filter, float weight,
+                               void *scratch, void *stream);
+
 /* Cost regularisers of the gradient engine on the object (regularizers.py:195-351):
  * obj_l1 sum|O-1|, obj_l2 sum|O-1|^2, obj_phase_l1 sum|angle O|, obj_tikh
  * sum|diff_x O|^2 + |diff_y O|^2, obj_tv sum sqrt(|g_y|^2 + |g_x|^2 + tv_eps)

@@ -1122,3 +1122,26 @@ def probe_regularizer_costs(probe, costs: t.Mapping[str, float], tv_eps: float =
         gRs += c('probe_recip_tv') * g
     gR += numpy.fft.ifftshift(gRs, axes=(-1, -2))
     return total, ifft2c(gR).astype(probe.dtype)
+
+
+def unstructured_gaussian(vals, scan, shape, corner, sampling, sigma: float, weight: float):
+    """UnstructuredGaussian (regularizers.py:430-497) for per-position values
+    (n, C): every object-grid pixel takes the value of its nearest scan position,
+    the image is blurred with exp(-2 pi^2 sigma^2 k^2) (k from fftfreq of the
+    object sampling), sampled back at each position's rounded pixel, and blended:
+    weight * blurred + (1 - weight) * vals."""
+    from scipy.spatial import cKDTree
+    pts = scan.reshape(-1, 2).astype(numpy.float64)
+    ys = corner[0] + numpy.arange(shape[0]) * sampling[0]
+    xs = corner[1] + numpy.arange(shape[1]) * sampling[1]
+    grid = numpy.stack(numpy.meshgrid(ys, xs, indexing='ij'), axis=-1)
+    near = cKDTree(pts).query(grid)[1]
+    v = vals.reshape(len(pts), -1)
+    img = v[near]                                     # (H, W, C)
+    ky, kx = numpy.meshgrid(numpy.fft.fftfreq(shape[0], sampling[0]), numpy.fft.fftfreq(shape[1], sampling[1]),
+                            indexing='ij')
+    filt = numpy.exp(-(2 * numpy.pi ** 2 * sigma ** 2) * (ky ** 2 + kx ** 2))
+    blur = numpy.real(ifft2c(fft2c(numpy.moveaxis(img, -1, 0)) * filt))
+    idx = numpy.round((pts - numpy.asarray(corner)) / numpy.asarray(sampling)).astype(int)
+    out = numpy.moveaxis(blur, 0, -1)[idx[:, 0], idx[:, 1]]
+    return (weight * out + (1 - weight) * v).reshape(vals.shape)

@@ -169,6 +169,9 @@ _SIGNATURES = {
     'phb_engine_reduce_layout': (c_i32, [c_i32, c_i32, c_i32, c_i32, c_i64, c_i64, ctypes.POINTER(c_i64)]),
     'phb_solver_group_finish': (c_i32, [ctypes.POINTER(PhbEngine), ctypes.POINTER(PhbStep), c_void_p, c_i32,
                                         c_void_p]),
+    'phb_smooth_positions_scratch_bytes': (ctypes.c_size_t, [c_i64, c_i64]),
+    'phb_smooth_position_values': (c_i32, [c_void_p, c_void_p, c_i64, c_i64, c_i64, c_f64, c_f64, c_f64, c_f64,
+                                           c_void_p, c_f32, c_void_p, c_void_p]),
     'phb_position_update': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_i32, c_f32, c_f32, c_f32,
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),

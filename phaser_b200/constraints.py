@@ -9,6 +9,7 @@ phaser/engines/common/regularizers.py).  Implemented here:
   obj_low_pass            (regularizers.py:135-161) -> phb_object_filter_c64
   obj_gaussian            (regularizers.py:164-192) -> phb_object_filter_c64
   remove_phase_ramp       (regularizers.py:67-83)   -> phb_remove_phase_ramp_c64
+  tilt_gaussian           (regularizers.py:430-497) -> phb_smooth_position_values (iteration only)
 Any other constraint name raises NotImplementedError (no silent skip).
 """
 from __future__ import annotations
@@ -138,11 +139,32 @@ class RemovePhaseRamp:
                   self.rows[0], self.rows[1], self.cols[0], self.cols[1], self.sums.data_ptr(), _stream())
 
 
-_KNOWN = {'clamp_object_amplitude': ClampObjectAmplitude, 'limit_probe_support': LimitProbeSupport,
+class TiltGaussian:
+    """Gaussian smoothing of the per-position tilts over the scan (iteration constraint)."""
+
+    def __init__(self, eng, state, props):
+        if eng.tilt is None:
+            raise ValueError("tilt_gaussian needs a tilt map (state.tilt)")
+        self.eng = eng
+        sigma, self.weight = float(P.get(props, 'sigma')), float(P.get(props, 'weight', 0.9))
+        samp = numpy.asarray(eng.obj_sampling.sampling, numpy.float64)
+        ky, kx = numpy.meshgrid(numpy.fft.fftfreq(eng.H, samp[0]), numpy.fft.fftfreq(eng.W, samp[1]), indexing='ij')
+        filt = numpy.exp(-(2 * numpy.pi ** 2 * sigma ** 2) * (ky ** 2 + kx ** 2)).astype(numpy.float32)
+        self.filt = torch.from_numpy(filt).to(eng.device)
+        self.scratch = torch.empty((2 * eng.H * eng.W,), dtype=torch.complex64, device=eng.device)
+
+    def apply_iter(self) -> None:
+        e, os_ = self.eng, self.eng.obj_sampling
+        _lib.call('phb_smooth_position_values', e.tilt.data_ptr(), e.scan.data_ptr(), e.n_pos, e.H, e.W,
+                  float(os_.corner[0]), float(os_.corner[1]), float(os_.sampling[0]), float(os_.sampling[1]),
+                  self.filt.data_ptr(), self.weight, self.scratch.data_ptr(), _stream())
+
+
+_KNOWN = {'clamp_object_amplitude': ClampObjectAmplitude, 'tilt_gaussian': TiltGaussian, 'limit_probe_support': LimitProbeSupport,
           'layers': RegularizeLayers, 'obj_low_pass': ObjLowPass, 'obj_gaussian': ObjGaussian,
           'remove_phase_ramp': RemovePhaseRamp}
 # the reference's GroupConstraintHook has no 'layers' (phaser/hooks/regularization.py:83-91)
-_GROUP_ONLY_EXCLUDED = {'layers'}
+_GROUP_ONLY_EXCLUDED = {'layers', 'tilt_gaussian'}
 
 
 def build_constraints(hooks: t.Sequence[t.Any], eng, state, per_group: bool) -> t.List[t.Any]:

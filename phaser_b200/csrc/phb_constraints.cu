@@ -353,6 +353,48 @@ __global__ void k_recip_grad(const float2 *obj, int64_t S, int64_t HW, const flo
     }
 }
 
+// ------------------------------------------------ per-position value smoothing
+// UnstructuredGaussian (regularizers.py:430-497): object pixel (r, c) at
+// corner + (r, c) * sampling takes the (2-component) value of its nearest scan
+// position (brute force; the lowest index wins an exact tie), packed as a complex.
+__global__ void __launch_bounds__(256) k_nearest_fill(const float *scan, int64_t n, const float *vals, int64_t H,
+                                                      int64_t W, double cy, double cx, double sy, double sx,
+                                                      float2 *img) {
+    __shared__ float2 sp[1024];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = i < H * W;
+    const double py = cy + (double)(i / W) * sy, px = cx + (double)(i % W) * sx;
+    double best = 1e300;
+    int64_t arg = 0;
+    for (int64_t p0 = 0; p0 < n; p0 += 1024) {
+        const int64_t cnt = n - p0 < 1024 ? n - p0 : 1024;
+        __syncthreads();
+        for (int64_t k = threadIdx.x; k < cnt; k += blockDim.x)
+            sp[k] = make_float2(scan[2 * (p0 + k)], scan[2 * (p0 + k) + 1]);
+        __syncthreads();
+        if (ok)
+            for (int64_t k = 0; k < cnt; ++k) {
+                const double dy = (double)sp[k].x - py, dx = (double)sp[k].y - px;
+                const double d = dy * dy + dx * dx;
+                if (d < best) { best = d; arg = p0 + k; }
+            }
+    }
+    if (ok) img[i] = make_float2(vals[2 * arg], vals[2 * arg + 1]);
+}
+
+// vals[p] = weight * img[round((pos - corner) / sampling)] + (1 - weight) * vals[p]
+__global__ void k_sample_blend(const float2 *img, const float *scan, int64_t n, int64_t H, int64_t W, double cy,
+                               double cx, double sy, double sx, float weight, float *vals) {
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = (int64_t)rint(((double)scan[2 * p] - cy) / sy), c = (int64_t)rint(((double)scan[2 * p + 1] - cx) / sx);
+        r = r < 0 ? 0 : (r >= H ? H - 1 : r);
+        c = c < 0 ? 0 : (c >= W ? W - 1 : c);
+        const float2 b = img[r * W + c];
+        vals[2 * p] = weight * b.x + (1.f - weight) * vals[2 * p];
+        vals[2 * p + 1] = weight * b.y + (1.f - weight) * vals[2 * p + 1];
+    }
+}
+
 __global__ void k_add_c(float2 *dst, const float2 *src, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = cadd(dst[i], src[i]);
@@ -481,6 +523,26 @@ int phb_object_recip_l1(const void *obj, int64_t S, int64_t H, int64_t W, float 
     k_dft_t<<<grid(W, H), 256, 0, st>>>(b, a, W, H, +1, sc, nullptr);
     if ((rc = check_launch())) return rc;
     k_recip_grad<<<flat_grid(HW), 256, 0, st>>>((const float2 *)obj, S, HW, a, cost, pre, (float2 *)grad);
+    return check_launch();
+}
+
+size_t phb_smooth_positions_scratch_bytes(int64_t H, int64_t W) {
+    return (H < 1 || W < 1) ? 0 : (size_t)2 * H * W * sizeof(float2);
+}
+
+int phb_smooth_position_values(float *vals, const float *scan, int64_t n, int64_t H, int64_t W, double corner_y,
+                               double corner_x, double samp_y, double samp_x, const float *filter, float weight,
+                               void *scratch, void *stream) {
+    if (!vals || !scan || !filter || !scratch || n < 1 || H < 1 || W < 1) return PHB_ERR_INVALID_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    float2 *img = (float2 *)scratch, *tmp = img + H * W;
+    k_nearest_fill<<<(unsigned)((H * W + 255) / 256), 256, 0, st>>>(scan, n, vals, H, W, corner_y, corner_x, samp_y,
+                                                                   samp_x, img);
+    int rc = check_launch();
+    if (rc) return rc;
+    // a real, k-symmetric filter keeps the two packed components apart
+    if ((rc = phb_object_filter_c64(img, 1, H, W, filter, tmp, stream))) return rc;
+    k_sample_blend<<<flat_grid(n), 256, 0, st>>>(img, scan, n, H, W, corner_y, corner_x, samp_y, samp_x, weight, vals);
     return check_launch();
 }
 

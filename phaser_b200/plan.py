@@ -160,7 +160,7 @@ _REF_CLASS_NAMES = {
     'ClampObjectAmplitude': 'clamp_object_amplitude', 'LimitProbeSupport': 'limit_probe_support',
     'SGDSolver': 'sgd', 'AdamSolver': 'adam', 'PolyakSGDSolver': 'polyak_sgd',
     'RegularizeLayers': 'layers', 'ObjLowPass': 'obj_low_pass', 'ObjGaussian': 'obj_gaussian',
-    'RemovePhaseRamp': 'remove_phase_ramp',
+    'RemovePhaseRamp': 'remove_phase_ramp', 'UnstructuredGaussian': 'tilt_gaussian',
     'ObjL1': 'obj_l1', 'ObjL2': 'obj_l2', 'ObjPhaseL1': 'obj_phase_l1', 'ObjRecipL1': 'obj_recip_l1',
     'ObjTotalVariation': 'obj_tv', 'ObjTikhonov': 'obj_tikh', 'LayersTotalVariation': 'layers_tv',
     'LayersTikhonov': 'layers_tikh', 'ProbePhaseTikhonov': 'probe_phase_tikh',

@@ -304,6 +304,23 @@ def constraints_case():
     apply(R.RemovePhaseRamp(None, {}), 'phase_ramp')
     apply(R.ClampObjectAmplitude(None, ClampObjectAmplitudeProps(amplitude=1.1)), 'clamp')
     apply(R.LimitProbeSupport(None, LimitProbeSupportProps(max_angle=20.0)), 'probe_support', 'probe')
+    # tilt_gaussian: nearest-position image of the tilts, Gaussian blur, sampled back
+    from phaser.hooks.regularization import TiltGaussianProps
+    tilts = rng.normal(0, 2.0, c['scan'].shape).astype(F32)
+    s_ = st()
+
+    class _Values(numpy.ndarray):
+        # UnstructuredGaussian reads `getattr(values, 'data', values)` (regularizers.py:470),
+        # which for a numpy array is its memoryview; jax arrays have no `.data`.  Emulate that.
+        @property
+        def data(self):
+            return numpy.asarray(self)
+
+    s_.tilt = tilts.copy().view(_Values)
+    hook = R.UnstructuredGaussian(None, TiltGaussianProps(sigma=0.8, weight=0.7))
+    s_, _ = hook.apply_iter(s_, hook.init_state(s_))
+    out['tilt_in'] = tilts
+    out['tilt_gaussian'] = numpy.asarray(s_.tilt)
 
     group = numpy.indices((3, 4)).reshape(2, -1)[:, :7]
     costs = {}

@@ -150,3 +150,14 @@ def test_gradient_run_with_fourier_regularizers_matches_oracle():
     assert numpy.allclose(state.progress.detector_errors, losses, rtol=1e-4)
     assert rel_l2(state.object.data, obj) < 1e-4
     assert rel_l2(state.probe.data, probe) < 1e-4
+
+
+def test_tilt_gaussian_matches_reference(g):
+    eng, state = fake_engine(g)
+    eng.tilt = torch.from_numpy(g['tilt_in'].reshape(-1, 2).astype(numpy.float32)).cuda()
+    eng.scan = torch.from_numpy(g['scan'].reshape(-1, 2).astype(numpy.float32)).cuda()
+    eng.n_pos = eng.scan.shape[0]
+    (con,) = build_constraints([{'type': 'tilt_gaussian', 'sigma': 0.8, 'weight': 0.7}], eng, state, per_group=False)
+    con.apply_iter()
+    out = eng.tilt.cpu().numpy().reshape(g['tilt_gaussian'].shape)
+    assert numpy.max(numpy.abs(out - g['tilt_gaussian'])) < 1e-5 * numpy.max(numpy.abs(g['tilt_gaussian']))

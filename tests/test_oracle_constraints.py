@@ -114,3 +114,9 @@ def test_fourier_and_probe_cost_gradients_match_finite_differences():
                 xm[i] -= h * unit
                 fd = (f(xp)[0] - f(xm)[0]) / (2 * h)
                 assert fd == pytest.approx(part[i], rel=1e-4, abs=1e-6)
+
+
+def test_tilt_gaussian_matches_reference(g):
+    out = P.unstructured_gaussian(g['tilt_in'].astype(numpy.float64), g['scan'], g['obj'].shape[-2:], g['corner'],
+                                  g['obj_sampling'], 0.8, 0.7)
+    assert numpy.max(numpy.abs(out - g['tilt_gaussian'])) < 1e-6 * numpy.max(numpy.abs(g['tilt_gaussian']))
