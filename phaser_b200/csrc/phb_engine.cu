@@ -621,6 +621,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         if (upd_obj) xf[I::flat(u, q)] = cabs2(ps[I::flat(u, q)]);
                     }
                 omax = block_max_float<FFT_THREADS>(omax, fred);
+                float scl = 0.f;
                 if (upd_obj) {
                     cl.sync();
                     float lmax = 0.f;
@@ -642,23 +643,31 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     // last remote access of the program: no rank may leave (and release its
                     // shared memory) before every rank has read the slice-0 maxima
                     if (s == 0) cl.sync();
-                    const float scl = a.beta_object / (float)S / wmax;
-                    float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
-#pragma unroll
-                    for (int u = 0; u < U; ++u)
-#pragma unroll
-                        for (int q = 0; q < E; ++q)
-                            if (cv.ok(u, q))
-                                atomic_add_c(dst + cv.off(u, q), cscale(cmulc(v[u][q], ps[I::flat(u, q)]), scl));
+                    scl = a.beta_object / (float)S / wmax;
                 }
+                // one pass: object update (atomics), exit-wave update and the next adjoint,
+                // loads of a chunk issued together
                 const float inv = 1.0f / omax;
+                float2 *dst = a.acc_obj + (size_t)s * a.H * a.W;
+                constexpr int CH = 8;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int q = 0; q < E; ++q) {
-                        const float2 c = v[u][q];
-                        if (s == 0 && upd_pos) ps[I::flat(u, q)] = c;
-                        v[u][q] = cscale(cmulc(c, cv.at(Os, u, q)), inv);
+                    for (int q0 = 0; q0 < E; q0 += CH) {
+                        float2 oo[CH], pp[CH];
+#pragma unroll
+                        for (int j = 0; j < CH; ++j) {
+                            oo[j] = cv.at(Os, u, q0 + j);
+                            pp[j] = upd_obj ? ps[I::flat(u, q0 + j)] : make_float2(0.f, 0.f);
+                        }
+#pragma unroll
+                        for (int j = 0; j < CH; ++j) {
+                            const int q = q0 + j;
+                            const float2 c = v[u][q];
+                            if (upd_obj && cv.ok(u, q)) atomic_add_c(dst + cv.off(u, q), cscale(cmulc(c, pp[j]), scl));
+                            if (s == 0 && upd_pos) ps[I::flat(u, q)] = c;
+                            v[u][q] = cscale(cmulc(c, oo[j]), inv);
+                        }
                     }
             }
             if (s > 0) {
