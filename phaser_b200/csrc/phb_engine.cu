@@ -378,13 +378,34 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     for (int q = 0; q < E; ++q) n0 += cabs2(v[u][q]);
                 warp_atomic_sum(sums + a.o_pnorm + b, (double)n0);
             }
-            if (upd_obj || upd_tilt) {   // stored for the adjoint (the tilt gradient transforms it)
+            if constexpr (!presolve) {
+                // one chunked pass: the object loads of a chunk are issued first, then the
+                // wavefield store (for the adjoint; the tilt gradient transforms it), the
+                // illumination scatter group_probe_mag[s] += |psi_s,m|^2 and the transmission
+                const bool store = upd_obj || upd_tilt;
                 float2 *dst = psi_b + (size_t)s * NN;
+                float *ill = do_illum ? a.illum + (size_t)s * a.H * a.W : nullptr;
+                constexpr int CH = 8;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int q = 0; q < E; ++q) dst[I::flat(u, q)] = v[u][q];
-            }
+                    for (int q0 = 0; q0 < E; q0 += CH) {
+                        float2 oo[CH];
+#pragma unroll
+                        for (int j = 0; j < CH; ++j) oo[j] = cv.at(Os, u, q0 + j);
+#pragma unroll
+                        for (int j = 0; j < CH; ++j) {
+                            const int q = q0 + j;
+                            if (store) dst[I::flat(u, q)] = v[u][q];
+                            if (ill && cv.ok(u, q)) atomicAdd(ill + cv.off(u, q), cabs2(v[u][q]));
+                            v[u][q] = cmul(v[u][q], oo[j]);
+                        }
+                    }
+                PHB_T_MARK(11);
+                if (s != S - 1) load_prop(s);
+                fwd = true;
+                phase = s == S - 1 ? PH_FAR : PH_PROP;
+            } else {
             if (do_illum) {   // group_probe_mag[s] += scatter(|psi_s,m|^2): one red per pixel and mode
                 float *dst = a.illum + (size_t)s * a.H * a.W;
 #pragma unroll
@@ -444,6 +465,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             if (!last) load_prop(s);
             fwd = true;
             phase = last ? PH_FAR : PH_PROP;
+            }
         } else if (phase == PH_PROP) {
             // ------------------------------------------- propagate (K layout)
             const uint64_t kband = s_bits[FFT_THREADS + tid];
