@@ -144,6 +144,15 @@ class DeviceEngine:
         self.report = torch.zeros((4,), dtype=torch.float64, device=dev)
 
     # ---------------------------------------------------------------- helpers
+    def set_patterns(self, patterns: torch.Tensor) -> None:
+        """Point the engine at another resident pattern array of the same shape and
+        type (e.g. the other half of a double-buffered host->device stream)."""
+        if patterns.shape != self.patterns.shape or patterns.dtype != self.patterns.dtype \
+                or not patterns.is_contiguous() or patterns.device != self.patterns.device:
+            raise ValueError("patterns must match the engine's resident pattern array")
+        self.patterns = patterns
+        self.desc.patterns = patterns.data_ptr()
+
     def probe_changed(self) -> None:
         _lib.call('phb_engine_probe_changed', self._eref, _stream())
 

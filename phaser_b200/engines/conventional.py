@@ -132,7 +132,8 @@ class ConventionalEngine:
         if self.pos_solver is not None and self.pos_solver[0] == 'momentum':
             self.mom_state = torch.zeros_like(eng.scan)
         self.start_i = int(state.iter.total_iter)
-        self.status_host = torch.empty((4,), dtype=torch.float64).pin_memory()
+        # two pinned report blocks: iteration i+1 may run while iteration i's report is read
+        self.status_hosts = [torch.empty((4,), dtype=torch.float64).pin_memory() for _ in range(2)]
         self.fused_events: t.Optional[t.List[t.Tuple[int, int]]] = None
         _call(self.observer, 'init_engine', state, recons_name=args.get('recons_name', ''), plan=props,
               noise_model=self.noise.kind)
@@ -187,7 +188,7 @@ class ConventionalEngine:
         # one device->host status block per iteration
         eng.iteration_report(eng.report)
         self._combine_report(eng.report)
-        self.status_host.copy_(eng.report, non_blocking=True)
+        self.status_hosts[i % 2].copy_(eng.report, non_blocking=True)
         if not sync:
             return None
         torch.cuda.current_stream().synchronize()
@@ -201,8 +202,10 @@ class ConventionalEngine:
         """Hook for combining the iteration report over ranks (single device: nothing)."""
 
     def check(self, i: int, it_pos: bool = True, it_err: bool = True) -> t.Optional[float]:
+        """Read iteration i's report (after the device has finished iteration i)."""
         state, eng = self.state, self.eng
-        bad_group, n_out, err = int(self.status_host[0]), int(self.status_host[1]), float(self.status_host[2])
+        rep = self.status_hosts[i % 2]
+        bad_group, n_out, err = int(rep[0]), int(rep[1]), float(rep[2])
         if bad_group >= _lib.PHB_STATUS_INTERNAL:
             raise RuntimeError(f"internal error: fused kernel aborted in group {bad_group - _lib.PHB_STATUS_INTERNAL}")
         if bad_group >= 0:
