@@ -54,6 +54,14 @@ def algorithmic_bytes_per_pos_slice(N: int, M: int, S: int, pattern_bytes: int =
     return N * N * (28 + 16 * M) + pattern_bytes * N * N // S
 
 
+def measured_sm_max_mhz():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            return float(json.load(f)['sm_max_mhz'])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def measured_peaks():
     path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     try:
@@ -376,6 +384,14 @@ def run_b200(args, world, rank, local):
             "traffic": traffic if (args.scan == 64 and args.batch == 256) else None, "traffic_unit": "GB per launch (ncu)", "kernel": "k_group<128> (fused LSQ-ML mini-batch)",
             "launch_ms": avg_ms, "launches_timed": len(fused), "bytes_per_launch": bytes_launch,
             "peak_source": f"{peak_kind} hbm_gbs", "share_of_step": sum(fused) / t_ms if t_ms else None}
+    # the kernel's other bound: FP32 FFT work (5 N^2 log2 N^2 per transform, M (4 + 4/S) transforms
+    # and ~60 M N^2 elementwise FLOP per position-slice) against the FP32 pipe's peak
+    # (148 SMs x 128 FMA lanes x 2 FLOP x max SM clock, an estimate: not in MEASURED_PEAKS.json)
+    flop_ps = 5 * N * N * numpy.log2(N * N) * M * (4 + 4 / S) + 60 * M * N * N
+    fp32_peak = 148 * 128 * 2 * (measured_sm_max_mhz() or 1965.0) * 1e6
+    flops = flop_ps * B * S / (avg_ms / 1e3)
+    roof["fp32_pipe"] = {"achieved_tflops": flops / 1e12, "peak_tflops_estimate": fp32_peak / 1e12,
+                         "frac": flops / fp32_peak, "flop_per_pos_slice": flop_ps}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
