@@ -373,20 +373,21 @@ int phb_upsample2_bwd(const float *gout, float *gin, int64_t planes, int32_t H, 
 /* *loss += mean (pred - target)^2 (float64), grad = d/dpred (either may be NULL) */
 int phb_mse(const float *pred, const float *target, float *grad, int64_t n, double *loss, void *stream);
 int phb_to_bf16(const float *x, void *y, int64_t n, void *stream);
-/* network input: log(1 + I) of each pattern (rows `index`, or 0..B-1 when NULL), zero
- * frequency centred, binned bin x bin, scaled to a maximum of 1: (B, N/bin, N/bin) */
-int phb_pattern_features(const float *patterns, const int64_t *index, int32_t B, int32_t N, int32_t bin, float *out,
-                         void *stream);
+/* network input: log(1 + I) of each pattern (rows `index`, or 0..B-1 when NULL) over the
+ * crop x crop detector window centred on zero frequency, binned bin x bin, mirrored through
+ * zero frequency (k -> -k) when flip != 0, scaled to a maximum of 1: (B, crop/bin, crop/bin) */
+int phb_pattern_features(const float *patterns, const int64_t *index, int32_t B, int32_t N, int32_t crop,
+                         int32_t bin, int32_t flip, float *out, void *stream);
 /* training targets: centred P x P patch of the projected object `proj` (H, W) under each
  * position's cutout (exact reference cutout start), as (Re - 1, Im): (B, 2, P, P) */
 int phb_patch_targets(const void *proj, int64_t H, int64_t W, const float *scan, const int64_t *index, int32_t B,
                       double corner_y, double corner_x, double samp_y, double samp_x, int32_t N, int32_t P,
                       float *out, void *stream);
-/* stitching: accumulate predicted (B, 2, P, P) patches into acc (H, W complex) and wgt (H, W);
- * then obj = acc / wgt where covered, 1 elsewhere */
+/* stitching: accumulate predicted (B, 2, P, P) patches, each pixel weighted by window (P x P,
+ * NULL = 1), into acc (H, W complex) and wgt (H, W); then obj = acc / wgt where covered, 1 elsewhere */
 int phb_stitch_patches(const float *pred, const float *scan, const int64_t *index, int32_t B, double corner_y,
-                       double corner_x, double samp_y, double samp_x, int32_t N, int32_t P, void *acc, float *wgt,
-                       int64_t H, int64_t W, void *stream);
+                       double corner_x, double samp_y, double samp_x, int32_t N, int32_t P, const float *window,
+                       void *acc, float *wgt, int64_t H, int64_t W, void *stream);
 int phb_stitch_finish(const void *acc, const float *wgt, void *obj, int64_t n, void *stream);
 /* product over the S slices of an (S, HW) complex64 object */
 int phb_project_slices(const void *obj, int64_t S, int64_t HW, void *out, void *stream);

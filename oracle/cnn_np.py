@@ -105,3 +105,40 @@ def loss_and_grads(params, x, target, quantize: bool = True):
         g = gx
         k -= 1
     return loss, grads[::-1]
+
+
+def pattern_features(pats, crop: int, bin: int, flip: bool):
+    """log(1 + I) over the crop x crop window centred on zero frequency of patterns
+    (B, N, N) stored with zero frequency at [0, 0], binned bin x bin, mirrored k -> -k
+    when flip, scaled to a maximum of 1 per pattern: (B, crop/bin, crop/bin)."""
+    B, N = pats.shape[0], pats.shape[-1]
+    k = numpy.arange(crop) - crop // 2          # frequency of each window pixel
+    if flip:
+        k = -k
+    rows = (k + N) % N
+    win = numpy.maximum(pats, 0)[:, rows][:, :, rows].astype(numpy.float64)
+    F = crop // bin
+    binned = win.reshape(B, F, bin, F, bin).sum(axis=(2, 4))
+    v = numpy.log1p(binned)
+    mx = v.max(axis=(1, 2), keepdims=True)
+    return numpy.where(mx > 0, v / numpy.where(mx > 0, mx, 1), 0).astype(numpy.float32)
+
+
+def stitch(pred, starts, N: int, H: int, W: int, window=None):
+    """Patches pred (B, 2, P, P) = (Re - 1, Im) placed at the centred P x P of each
+    N x N cutout (top-left `starts` (B, 2)), averaged with per-pixel weights `window`
+    (P, P; uniform when None); 1 where no patch lands."""
+    B, _, P, _ = pred.shape
+    off = (N - P) // 2
+    w = numpy.ones((P, P)) if window is None else numpy.asarray(window, numpy.float64)
+    acc = numpy.zeros((H, W), numpy.complex128)
+    wgt = numpy.zeros((H, W))
+    for b in range(B):
+        y0, x0 = int(starts[b, 0]) + off, int(starts[b, 1]) + off
+        ys, xs = numpy.arange(y0, y0 + P), numpy.arange(x0, x0 + P)
+        my, mx = (ys >= 0) & (ys < H), (xs >= 0) & (xs < W)
+        v = (pred[b, 0] + 1.0) + 1j * pred[b, 1]
+        sub = numpy.ix_(ys[my], xs[mx])
+        acc[sub] += (w * v)[numpy.ix_(my, mx)]
+        wgt[sub] += w[numpy.ix_(my, mx)]
+    return numpy.where(wgt > 0, acc / numpy.where(wgt > 0, wgt, 1), 1.0).astype(numpy.complex64)

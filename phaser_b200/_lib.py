@@ -154,11 +154,11 @@ _SIGNATURES = {
     'phb_upsample2_bwd': (c_i32, [c_void_p, c_void_p, c_i64, c_i32, c_i32, c_void_p]),
     'phb_mse': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p, c_void_p]),
     'phb_to_bf16': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
-    'phb_pattern_features': (c_i32, [c_void_p, c_void_p, c_i32, c_i32, c_i32, c_void_p, c_void_p]),
+    'phb_pattern_features': (c_i32, [c_void_p, c_void_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_void_p, c_void_p]),
     'phb_patch_targets': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p, c_i32, c_f64, c_f64, c_f64, c_f64,
                                   c_i32, c_i32, c_void_p, c_void_p]),
     'phb_stitch_patches': (c_i32, [c_void_p, c_void_p, c_void_p, c_i32, c_f64, c_f64, c_f64, c_f64, c_i32, c_i32,
-                                   c_void_p, c_void_p, c_i64, c_i64, c_void_p]),
+                                   c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_void_p]),
     'phb_stitch_finish': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p]),
     'phb_project_slices': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p]),
     'phb_probe_regularizers_scratch_bytes': (ctypes.c_size_t, [c_i32, c_i32]),

@@ -225,9 +225,9 @@ __global__ void k_to_bf16(const float *x, __nv_bfloat16 *y, int64_t n) {
 // ------------------------------------------------------- data preparation
 // Network input of pattern b: log(1 + max(I, 0)) with the zero frequency moved to
 // the centre, binned by `bin` x `bin`, divided by its maximum.  One CTA per pattern.
-__global__ void __launch_bounds__(256) k_pattern_features(const float *pat, const int64_t *index, int N, int bin,
-                                                          float *out) {
-    const int b = blockIdx.x, F = N / bin;
+__global__ void __launch_bounds__(256) k_pattern_features(const float *pat, const int64_t *index, int N, int crop,
+                                                          int bin, int flip, float *out) {
+    const int b = blockIdx.x, F = crop / bin, c0 = N / 2 - crop / 2;
     const float *p = pat + (size_t)(index ? index[b] : b) * N * N;
     float *o = out + (size_t)b * F * F;
     __shared__ float smax[32];
@@ -237,8 +237,11 @@ __global__ void __launch_bounds__(256) k_pattern_features(const float *pat, cons
         float s = 0.f;
         for (int dy = 0; dy < bin; ++dy)
             for (int dx = 0; dx < bin; ++dx) {
-                const int ky = (fy * bin + dy + N / 2) % N, kx = (fx * bin + dx + N / 2) % N;   // fftshift
-                s += fmaxf(p[ky * N + kx], 0.f);
+                // spatial frequency of this detector pixel (zero at the crop's centre), mirrored
+                // through zero when flip is set; stored patterns hold zero frequency at [0, 0]
+                int ky = c0 + fy * bin + dy - N / 2, kx = c0 + fx * bin + dx - N / 2;
+                if (flip) ky = -ky, kx = -kx;
+                s += fmaxf(p[((ky + N) % N) * N + (kx + N) % N], 0.f);
             }
         const float v = log1pf(s);
         o[i] = v;
@@ -268,10 +271,12 @@ __global__ void __launch_bounds__(256) k_patch_targets(const float2 *proj, int64
     }
 }
 
-// Stitch predicted patches (B, 2, P, P) = (Re - 1, Im) into sum / weight grids.
+// Stitch predicted patches (B, 2, P, P) = (Re - 1, Im) into sum / weight grids, each
+// patch pixel weighted by window[P * P] (1 when window is NULL).
 __global__ void __launch_bounds__(256) k_stitch(const float *pred, const float *scan, const int64_t *index,
                                                 double cy, double cx, double sy, double sx, int N, int P,
-                                                float2 *acc, float *wgt, int64_t H, int64_t W) {
+                                                const float *window, float2 *acc, float *wgt, int64_t H,
+                                                int64_t W) {
     const int b = blockIdx.x;
     const int64_t pos = index ? index[b] : b;
     const CutoutIndex ci = cutout_index(scan, pos, cy, cx, sy, sx, N, N);
@@ -280,8 +285,9 @@ __global__ void __launch_bounds__(256) k_stitch(const float *pred, const float *
     for (int i = threadIdx.x; i < P * P; i += blockDim.x) {
         const int64_t y = ci.y0 + off + i / P, x = ci.x0 + off + i % P;
         if (y < 0 || y >= H || x < 0 || x >= W) continue;
-        atomic_add_c(acc + y * W + x, make_float2(p[i] + 1.f, p[P * P + i]));
-        atomicAdd(wgt + y * W + x, 1.f);
+        const float w = window ? window[i] : 1.f;
+        atomic_add_c(acc + y * W + x, make_float2(w * (p[i] + 1.f), w * p[P * P + i]));
+        atomicAdd(wgt + y * W + x, w);
     }
 }
 
@@ -403,10 +409,11 @@ int phb_to_bf16(const float *x, void *y, int64_t n, void *stream) {
     return check_launch();
 }
 
-int phb_pattern_features(const float *patterns, const int64_t *index, int32_t B, int32_t N, int32_t bin, float *out,
-                         void *stream) {
-    if (!patterns || !out || B < 1 || N < 1 || bin < 1 || N % bin) return PHB_ERR_INVALID_ARG;
-    k_pattern_features<<<B, 256, 0, (cudaStream_t)stream>>>(patterns, index, N, bin, out);
+int phb_pattern_features(const float *patterns, const int64_t *index, int32_t B, int32_t N, int32_t crop,
+                         int32_t bin, int32_t flip, float *out, void *stream) {
+    if (!patterns || !out || B < 1 || N < 2 || N % 2 || crop < 2 || crop > N || crop % 2 || bin < 1 || crop % bin)
+        return PHB_ERR_INVALID_ARG;
+    k_pattern_features<<<B, 256, 0, (cudaStream_t)stream>>>(patterns, index, N, crop, bin, flip ? 1 : 0, out);
     return check_launch();
 }
 
@@ -420,11 +427,11 @@ int phb_patch_targets(const void *proj, int64_t H, int64_t W, const float *scan,
 }
 
 int phb_stitch_patches(const float *pred, const float *scan, const int64_t *index, int32_t B, double corner_y,
-                       double corner_x, double samp_y, double samp_x, int32_t N, int32_t P, void *acc, float *wgt,
-                       int64_t H, int64_t W, void *stream) {
+                       double corner_x, double samp_y, double samp_x, int32_t N, int32_t P, const float *window,
+                       void *acc, float *wgt, int64_t H, int64_t W, void *stream) {
     if (!pred || !scan || !acc || !wgt || B < 1 || P < 1 || P > N || H < 1 || W < 1) return PHB_ERR_INVALID_ARG;
     k_stitch<<<B, 256, 0, (cudaStream_t)stream>>>(pred, scan, index, corner_y, corner_x, samp_y, samp_x, N, P,
-                                                  (float2 *)acc, wgt, H, W);
+                                                  window, (float2 *)acc, wgt, H, W);
     return check_launch();
 }
 

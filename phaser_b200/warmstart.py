@@ -1,12 +1,22 @@
 """Learned warm start for the iterative solvers.
 
-A small convolutional network maps each diffraction pattern (64 x 64, log
-scale, zero frequency centred) to the 32 x 32 complex object patch under the
-centre of the probe; the patches are stitched into an initial object that
-LSQ-ML / ePIE / the gradient engine then refine.  The reference has no such
-component; the solvers stay the authority and the fallback: the warm start is
-used only when its simulated patterns fit the measurements better than the
-flat object does.
+A small convolutional network maps each diffraction pattern to the 32 x 32
+complex object patch under the centre of the probe; the patches are stitched
+into an initial object that LSQ-ML / ePIE / the gradient engine then refine.
+The reference has no such component; the solvers stay the authority and the
+fallback: the warm start is used only when its simulated patterns fit the
+measurements better than the flat object does.
+
+Input (FeatureSpec): log(1 + I) of the 64 x 64 detector window around zero
+frequency of the 128^2 patterns (the bright-field disk of the 25 mrad probe at
+full resolution), mirrored k -> -k and scaled to a maximum of 1.  The probe is
+200 A out of focus, so the disk holds a shadow image of the illuminated object
+(about 1.3 detector px per object px); mirrored, that image has the output
+patch's orientation, and the residual offset between an output pixel and its
+source (at most ~11 input px at the patch edge) lies inside the network's
+receptive field.  Binning the whole pattern 2 x 2 instead halves the shadow
+image and pushes the offsets past the receptive field: the stitched phase then
+correlates 0.2 with the truth instead of 0.5-0.7 (measured).
 
 Network: 3x3 convolutions with bfloat16 weights and float32 accumulation
 (libphaser_b200 phb_conv3x3_*):
@@ -16,11 +26,13 @@ Network: 3x3 convolutions with bfloat16 weights and float32 accumulation
     conv 64->32, ReLU            32^2
     conv 32->2                   32^2 x (Re - 1, Im)
 trained with mean squared error and Adam (phb_optimizer_update) on patterns the
-B200 forward model simulates from random Gaussian-atom lattices.
+B200 forward model simulates from random Gaussian-atom lattices in the
+multislice LSQ-ML configuration's geometry (lattice_geometry).
 """
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import math
 import time
 import typing as t
@@ -35,6 +47,22 @@ LAYERS = ((1, 32, 2, True, False), (32, 64, 2, True, False), (64, 64, 1, True, T
 IN_SIDE, PATCH = 64, 32
 
 
+@dataclasses.dataclass(frozen=True)
+class FeatureSpec:
+    """Which detector pixels feed the network: the crop x crop window centred on zero
+    frequency, binned bin x bin (crop / bin = 64), mirrored k -> -k when flip is set.
+    The default keeps the bright-field disk of the 128^2 patterns at full resolution
+    and mirrors it, so that the shadow image the defocused probe casts of the object
+    under it lies on the output patch's grid (no mirror across the patch), within the
+    network's ~30 px receptive field."""
+    crop: int = 64
+    bin: int = 1
+    flip: bool = True
+
+
+DEFAULT_FEATURES = FeatureSpec()
+
+
 def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
@@ -43,8 +71,10 @@ class WarmStartNet:
     """The network's parameters (float32 master copies, bfloat16 working copies),
     gradients, Adam state and activation buffers, all on one device."""
 
-    def __init__(self, seed: int = 0, device: t.Union[str, torch.device] = 'cuda'):
+    def __init__(self, seed: int = 0, device: t.Union[str, torch.device] = 'cuda',
+                 features: FeatureSpec = DEFAULT_FEATURES):
         self.device = torch.device(device)
+        self.features = features
         rng = numpy.random.default_rng(seed)
         self.w, self.b, self.wq, self.gw, self.gb, self.m, self.v = [], [], [], [], [], [], []
         for (ci, co, *_r) in LAYERS:
@@ -191,35 +221,53 @@ def lattice_phase_fast(shape: t.Tuple[int, int], spacing: float, sigma: float, p
     return numpy.bincount((ys * W + xs)[ok], weights=vals[ok], minlength=H * W).reshape(H, W)
 
 
-def random_lattice_dataset(rng: numpy.random.Generator, *, scan: int = 32, N: int = 64, counts: float = 1e5,
-                           slices: t.Tuple[int, int] = (4, 12)):
-    """One training object of the single-slice configuration's geometry (64^2 probe,
-    20 mrad, 200 kV, 100 A defocus, 0.2 A/px, scan at 4 px) with 4-12 slices of
-    random lattices (spacing 6-14 px, peak phase 0.1-0.5 rad, 2 nm slices)."""
+def lattice_geometry(scan: int = 32, seed: int = 0):
+    """The multislice LSQ-ML configuration's optics and scan geometry (128^2 probe at
+    0.2 A/px, 25 mrad, 300 kV, 200 A defocus, 4 Hermite modes holding 70/15/10/5 %,
+    6 px steps, 1e6 e- per pattern) on a scan x scan raster: a Dataset whose object
+    the training loop replaces."""
     from .synthetic import make_dataset
-    S = int(rng.integers(slices[0], slices[1] + 1))
-    ds = make_dataset(N=N, M=1, S=1, scan_shape=(scan, scan), step_px=4.0, sampling=0.2, kv=200e3,
-                      conv_mrad=20.0, defocus=100.0, slice_thickness=0.0, spacing_px=10.0, sigma_px=1.5,
-                      peak_rad=0.0, counts=counts, scan_jitter_px=0.5, seed=int(rng.integers(1 << 31)))
+    return make_dataset(N=128, M=4, S=1, scan_shape=(scan, scan), step_px=6.0, sampling=0.2, kv=300e3,
+                        conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
+                        peak_rad=0.0, counts=1e6, mode_powers=(0.70, 0.15, 0.10, 0.05), seed=seed)
+
+
+def random_lattice_objects(n: int, *, seed: int = 0, scan: int = 32, slices: t.Tuple[int, int] = (4, 12),
+                           peak: t.Tuple[float, float] = (0.1, 0.5), spacing: t.Tuple[float, float] = (6., 14.)):
+    """Yield n training datasets on lattice_geometry(scan): each with 4-12 slices of 2 nm,
+    every slice an independently shifted Gaussian-atom lattice (sigma 1.5 px) of one
+    random spacing (6-14 px) and peak phase (0.1-0.5 rad).  The same Dataset object is
+    reused: consume each before drawing the next."""
+    rng = numpy.random.default_rng(seed)
+    ds = lattice_geometry(scan, seed)
     H, W = ds.true_object.shape[-2:]
-    spacing, peak = float(rng.uniform(6, 14)), float(rng.uniform(0.1, 0.5))
-    phase = numpy.stack([lattice_phase_fast((H, W), spacing, 1.5, peak, rng) for _ in range(S)])
-    ds.true_object = numpy.exp(1j * phase).astype(numpy.complex64)
-    ds.init_object = numpy.ones((S, H, W), numpy.complex64)
-    ds.thicknesses = numpy.full(S, 20.0, numpy.float32)
-    return ds
+    for _ in range(n):
+        S = int(rng.integers(slices[0], slices[1] + 1))
+        sp, pk = float(rng.uniform(*spacing)), float(rng.uniform(*peak))
+        phase = numpy.stack([lattice_phase_fast((H, W), sp, 1.5, pk, rng) for _ in range(S)])
+        ds.true_object = numpy.exp(1j * phase).astype(numpy.complex64)
+        ds.init_object = numpy.ones((S, H, W), numpy.complex64)
+        ds.thicknesses = numpy.full(S, 20.0, numpy.float32)
+        yield ds
 
 
-def features_and_targets(ds, pats: torch.Tensor, *, with_targets: bool = True):
-    """Network inputs (n, 1, 64, 64) of the dataset's patterns and, optionally, the
-    training targets (n, 2, 32, 32) from its true object."""
+def pattern_features(pats: torch.Tensor, spec: FeatureSpec = DEFAULT_FEATURES) -> torch.Tensor:
+    """Network inputs (n, 1, 64, 64) of patterns (n, N, N) (zero frequency at [0, 0])."""
+    n, N = pats.shape[0], pats.shape[-1]
+    side = spec.crop // spec.bin
+    if side != IN_SIDE or spec.crop > N:
+        raise ValueError(f"feature window {spec} does not give {IN_SIDE}^2 inputs from {N}^2 patterns")
+    feats = torch.empty((n, 1, IN_SIDE, IN_SIDE), dtype=torch.float32, device=pats.device)
+    _lib.call('phb_pattern_features', pats.data_ptr(), None, n, N, spec.crop, spec.bin, int(spec.flip),
+              feats.data_ptr(), _stream())
+    return feats
+
+
+def patch_targets(ds, pats: torch.Tensor) -> torch.Tensor:
+    """Training targets (n, 2, 32, 32): the projected true object under each probe centre."""
     dev = pats.device
     n, N = pats.shape[0], pats.shape[-1]
     st = _stream()
-    feats = torch.empty((n, 1, IN_SIDE, IN_SIDE), dtype=torch.float32, device=dev)
-    _lib.call('phb_pattern_features', pats.data_ptr(), None, n, N, N // IN_SIDE, feats.data_ptr(), st)
-    if not with_targets:
-        return feats, None
     S, H, W = ds.true_object.shape
     obj = torch.from_numpy(ds.true_object).to(dev)
     proj = torch.empty((H, W), dtype=torch.complex64, device=dev)
@@ -229,105 +277,125 @@ def features_and_targets(ds, pats: torch.Tensor, *, with_targets: bool = True):
     os_ = ds.obj_sampling
     _lib.call('phb_patch_targets', proj.data_ptr(), H, W, scan.data_ptr(), None, n, float(os_.corner[0]),
               float(os_.corner[1]), float(os_.sampling[0]), float(os_.sampling[1]), N, PATCH, targets.data_ptr(), st)
-    return feats, targets
+    return targets
 
 
 def training_set(n_objects: int, *, seed: int = 0, scan: int = 32, slices: t.Tuple[int, int] = (4, 12),
-                 device='cuda'):
-    """(features, targets) of n_objects random-lattice objects x scan^2 positions."""
+                 spec: FeatureSpec = DEFAULT_FEATURES, device='cuda', **objects):
+    """(features, targets) of n_objects random-lattice objects x scan^2 positions, the
+    patterns simulated by the fused forward kernel with Poisson noise."""
     from .synthetic import simulate_patterns
-    rng = numpy.random.default_rng(seed)
     fs, ts = [], []
-    for k in range(n_objects):
-        ds = random_lattice_dataset(rng, scan=scan, slices=slices)
+    for k, ds in enumerate(random_lattice_objects(n_objects, seed=seed, scan=scan, slices=slices, **objects)):
         pats = simulate_patterns(ds, seed=seed * 100003 + k, device=device)
-        f, tg = features_and_targets(ds, pats)
-        fs.append(f)
-        ts.append(tg)
+        fs.append(pattern_features(pats, spec))
+        ts.append(patch_targets(ds, pats))
     return torch.cat(fs), torch.cat(ts)
 
 
-def stitch(net: WarmStartNet, feats: torch.Tensor, scan: numpy.ndarray, obj_sampling, shape, N: int) -> torch.Tensor:
-    """Predicted patches stitched into an (H, W) complex64 object (1 outside the patches)."""
+def stitch_window(sigma: t.Optional[float]) -> t.Optional[torch.Tensor]:
+    """Gaussian weight (PATCH, PATCH) centred on the patch (None: uniform weights)."""
+    if sigma is None:
+        return None
+    r = numpy.arange(PATCH, dtype=numpy.float64) - (PATCH - 1) / 2
+    w = numpy.exp(-(r[:, None] ** 2 + r[None, :] ** 2) / (2 * sigma ** 2))
+    return torch.from_numpy(w.astype(numpy.float32))
+
+
+def stitch(net: WarmStartNet, feats: torch.Tensor, scan: numpy.ndarray, obj_sampling, shape, N: int,
+           window_sigma: t.Optional[float] = None) -> torch.Tensor:
+    """Predicted patches stitched into an (H, W) complex64 object (1 outside the patches),
+    each patch weighted by a Gaussian of window_sigma px (uniform when None)."""
     dev = feats.device
     H, W = shape
     pred = net.predict(feats)
     acc = torch.zeros((H, W), dtype=torch.complex64, device=dev)
     wgt = torch.zeros((H, W), dtype=torch.float32, device=dev)
     sc = torch.from_numpy(numpy.ascontiguousarray(scan.reshape(-1, 2), numpy.float32)).to(dev)
+    win = stitch_window(window_sigma)
+    win = None if win is None else win.to(dev)
     st = _stream()
     _lib.call('phb_stitch_patches', pred.data_ptr(), sc.data_ptr(), None, pred.shape[0],
               float(obj_sampling.corner[0]), float(obj_sampling.corner[1]), float(obj_sampling.sampling[0]),
-              float(obj_sampling.sampling[1]), N, PATCH, acc.data_ptr(), wgt.data_ptr(), H, W, st)
+              float(obj_sampling.sampling[1]), N, PATCH, None if win is None else win.data_ptr(), acc.data_ptr(),
+              wgt.data_ptr(), H, W, st)
     out = torch.empty_like(acc)
     _lib.call('phb_stitch_finish', acc.data_ptr(), wgt.data_ptr(), out.data_ptr(), H * W, st)
     return out
 
 
-def pattern_residual(eng, obj: torch.Tensor) -> float:
-    """sum (sqrt(I_model) - sqrt(I_measured))^2 over all positions for the object
-    `obj` (S, H, W) with the engine's current probe (the fallback criterion)."""
+def pattern_residual(eng, obj: torch.Tensor, stride: int = 1) -> float:
+    """sum (sqrt(I_model) - sqrt(I_measured))^2 over every stride-th position for the
+    object `obj` (S, H, W) with the engine's current probe (the fallback criterion)."""
     saved = eng.object.clone()
     eng.object.copy_(obj)
-    n, G = eng.n_pos, eng.group_max
-    idx = numpy.arange(n, dtype=numpy.int64)
-    gt, sizes = eng.group_tensor([idx[i:i + G] for i in range(0, n, G)])
+    G = eng.group_max
+    idx = numpy.arange(0, eng.n_pos, stride, dtype=numpy.int64)
+    chunks = [idx[i:i + G] for i in range(0, len(idx), G)]
+    gt, sizes = eng.group_tensor(chunks)
+    rows = torch.from_numpy(idx).to(eng.device)
     total = torch.zeros((), dtype=torch.float64, device=eng.device)
     for g, B in enumerate(sizes):
         sim = eng.simulate(gt[g], B)
-        meas = eng.patterns[g * G:g * G + B]
+        meas = eng.patterns[rows[g * G:g * G + B]].to(torch.float32)
         total += torch.sum((torch.sqrt(sim) - torch.sqrt(torch.clamp(meas, min=0))) ** 2, dtype=torch.float64)
     eng.object.copy_(saved)
     return float(total)
 
 
-def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.ndarray) -> t.Tuple[torch.Tensor, dict]:
-    """The stitched warm-start object for the engine's geometry (each of the S slices
-    gets the S-th root of the predicted transmission), or the engine's current
-    object when the prediction fits the patterns worse.  Returns (object, info)."""
+def phase_candidate(proj: torch.Tensor, S: int, scale: float) -> torch.Tensor:
+    """(S, H, W) pure-phase object whose slices share the stitched projection's phase
+    (times `scale`) equally."""
+    ph = torch.angle(proj) * (scale / S)
+    return torch.polar(torch.ones_like(ph), ph).unsqueeze(0).expand(S, *proj.shape).contiguous()
+
+
+def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.ndarray, *,
+                      window_sigma: t.Optional[float] = None, scales: t.Sequence[float] = (1.0, 1.25, 1.5),
+                      residual_stride: int = 4) -> t.Tuple[torch.Tensor, dict]:
+    """The stitched warm-start object for the engine's geometry: every slice gets an equal
+    share of the predicted projected phase, times the scale in `scales` whose simulated
+    patterns fit the measurements best (on every residual_stride-th position); the
+    engine's current object is kept instead when that fit is worse than its own.
+    Returns (object, info)."""
     S, H, W = eng.object.shape
-    feats, _ = features_and_targets(None, pats, with_targets=False)
-    proj = stitch(net, feats, scan, eng.obj_sampling, (H, W), eng.N)
-    cand = torch.exp(torch.log(proj) / S).unsqueeze(0).expand(S, H, W).contiguous()
-    r_warm = pattern_residual(eng, cand)
-    r_flat = pattern_residual(eng, eng.object)
-    use = r_warm < r_flat
-    return (cand if use else eng.object.clone()), {"residual_warm": r_warm, "residual_flat": r_flat,
-                                                   "used": bool(use)}
+    feats = pattern_features(pats, net.features)
+    proj = stitch(net, feats, scan, eng.obj_sampling, (H, W), eng.N, window_sigma)
+    r_flat = pattern_residual(eng, eng.object, residual_stride)
+    best = None
+    tried = {}
+    for sc in scales:
+        cand = phase_candidate(proj, S, sc)
+        r = pattern_residual(eng, cand, residual_stride)
+        tried[float(sc)] = r
+        if best is None or r < best[0]:
+            best = (r, float(sc), cand)
+    use = best[0] < r_flat
+    return (best[2] if use else eng.object.clone()), {"residual_warm": best[0], "residual_flat": r_flat,
+                                                      "scale": best[1], "residuals": tried, "used": bool(use)}
 
 
-def compare_with_plain(net: WarmStartNet, ds, pats: torch.Tensor, *, iters: int = 20, solver: str = 'lsqml',
-                       grouping: int = 64) -> dict:
-    """Warm start against the plain method on one dataset: NRMSE of the projected
-    object after every iteration (against ds.true_object) and the device time to
-    reach the plain run's final NRMSE.  The warm arm's time includes the network
-    inference, the stitching and the fallback test."""
+def compare_with_plain(net: WarmStartNet, make_engine: t.Callable[[], t.Any], true_object: numpy.ndarray,
+                       pats: torch.Tensor, scan: numpy.ndarray, *, iters: int = 20, **warm) -> dict:
+    """Warm start against the plain method on one dataset: `make_engine()` returns a
+    presolved engine (ConventionalEngine or GradientEngine) started from the flat
+    object.  NRMSE of the projected object after every iteration (against
+    true_object) and the device time to reach the plain run's final NRMSE; the warm
+    arm's time includes the feature extraction, inference, stitching and the
+    residual tests."""
     from .constraints import RemovePhaseRamp
-    from .engines.conventional import ConventionalEngine
     from .metrics import object_nrmse
-    from .plan import ConventionalEnginePlan
-    from .sampling import Sampling
-    from .state import IterState, ObjectState, Patterns, ProbeState, ReconsState
-    N = ds.probe.shape[-1]
-    ref = torch.from_numpy(ds.true_object).to(pats.device)
-    props = ConventionalEnginePlan(noise_model={'type': 'amplitude'}, solver={'type': solver}, niter=iters,
-                                   grouping=grouping)
+    ref = torch.from_numpy(true_object).to(pats.device)
     out = {}
     for arm in ('plain', 'warm'):
-        state = ReconsState(iter=IterState(), wavelength=ds.wavelength,
-                            probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
-                            object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
-                            scan=ds.scan.copy())
-        eng = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
-                                  'seed': 'warm-start', 'recons_name': arm}, props, patterns_on_device=pats)
-        eng.presolve()
+        eng = make_engine()
         crop = RemovePhaseRamp(eng.eng, None, None)
         info = None
         t_prep = 0.0
         if arm == 'warm':
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            obj, info = warm_start_object(net, eng.eng, pats, ds.scan)
+            obj, info = warm_start_object(net, eng.eng, pats, scan, **warm)
             eng.eng.object.copy_(obj)
             torch.cuda.synchronize()
             t_prep = time.perf_counter() - t0
@@ -343,6 +411,7 @@ def compare_with_plain(net: WarmStartNet, ds, pats: torch.Tensor, *, iters: int 
             times.append(times[-1] + e0.elapsed_time(e1) / 1e3)
             curve.append(object_nrmse(eng.eng.object, ref, crop.rows, crop.cols))
         out[arm] = {"curve": curve, "seconds": times, "fallback_test": info}
+        del eng
     target = out['plain']['curve'][-1]
     for arm in ('plain', 'warm'):
         hit = next((i for i, v in enumerate(out[arm]['curve']) if v <= target), None)

@@ -92,3 +92,52 @@ def test_upsample_and_relu_kernels():
     g2 = g.clone()
     _lib.call('phb_relu_bwd', g2.data_ptr(), up.data_ptr(), g2.numel(), st())
     assert torch.equal(g2.cpu(), (g * (up > 0)).cpu())
+
+
+@pytest.mark.parametrize('N,crop,bin,flip', [(128, 64, 1, True), (128, 64, 1, False), (128, 128, 2, False),
+                                             (64, 64, 1, True), (128, 96, 3, True)])
+def test_pattern_features_match_oracle(N, crop, bin, flip):
+    rng = numpy.random.default_rng(N + crop + bin + flip)
+    B = 5
+    pats = rng.poisson(50.0, (B + 2, N, N)).astype(numpy.float32)
+    pats[0, :3, :3] = -1.0                          # negative counts are clamped to zero
+    index = numpy.array([6, 0, 3, 3, 1], numpy.int64)
+    F = crop // bin
+    out = torch.empty((B, F, F), dtype=torch.float32, device='cuda')
+    p = torch.from_numpy(pats).cuda()
+    it = torch.from_numpy(index).cuda()
+    _lib.call('phb_pattern_features', p.data_ptr(), it.data_ptr(), B, N, crop, bin, int(flip), out.data_ptr(), st())
+    ref = C.pattern_features(pats[index], crop, bin, flip)
+    assert rel_l2(out.cpu().numpy(), ref) < 1e-6
+
+
+def test_pattern_features_reject_bad_windows():
+    p = torch.zeros((1, 64, 64), dtype=torch.float32, device='cuda')
+    out = torch.empty((1, 64, 64), dtype=torch.float32, device='cuda')
+    for crop, bin in ((128, 1), (63, 1), (64, 3), (0, 1)):
+        with pytest.raises(_lib.PhbError):
+            _lib.call('phb_pattern_features', p.data_ptr(), None, 1, 64, crop, bin, 0, out.data_ptr(), st())
+
+
+@pytest.mark.parametrize('windowed', [False, True])
+def test_stitch_matches_oracle(windowed):
+    from oracle import phaser_np as O
+    from phaser_b200.warmstart import stitch_window
+    rng = numpy.random.default_rng(7 + windowed)
+    N, P, H, W, B = 64, 32, 90, 100, 40
+    corner, samp = numpy.array([-9.0, -10.0]), numpy.array([0.2, 0.2])
+    # positions spread past every edge of the object: patches are clipped there
+    scan = rng.uniform([-14.0, -15.0], [14.0, 15.0], (B, 2)).astype(numpy.float32)
+    pred = rng.normal(0, 0.2, (B, 2, P, P)).astype(numpy.float32)
+    win = stitch_window(4.0).numpy() if windowed else None
+    acc = torch.zeros((H, W), dtype=torch.complex64, device='cuda')
+    wgt = torch.zeros((H, W), dtype=torch.float32, device='cuda')
+    pt, sc = torch.from_numpy(pred).cuda(), torch.from_numpy(scan).cuda()
+    wt = None if win is None else torch.from_numpy(win).cuda()
+    _lib.call('phb_stitch_patches', pt.data_ptr(), sc.data_ptr(), None, B, corner[0], corner[1], samp[0], samp[1],
+              N, P, None if wt is None else wt.data_ptr(), acc.data_ptr(), wgt.data_ptr(), H, W, st())
+    obj = torch.empty_like(acc)
+    _lib.call('phb_stitch_finish', acc.data_ptr(), wgt.data_ptr(), obj.data_ptr(), H * W, st())
+    starts = O.cutout_starts(scan.astype(numpy.float64), corner, samp, (N, N))
+    ref = C.stitch(pred, starts, N, H, W, win)
+    assert rel_l2(obj.cpu().numpy(), ref) < 1e-6

@@ -53,3 +53,37 @@ def test_bf16_rounding_matches_torch():
     x = numpy.random.default_rng(0).normal(size=10000).astype(numpy.float32) * 10
     ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy()
     assert numpy.array_equal(C.bf16(x), ref)
+
+
+def test_feature_window_is_the_centred_crop_and_flip_mirrors_k():
+    rng = numpy.random.default_rng(3)
+    p = rng.random((2, 16, 16)).astype(numpy.float32)
+    f = C.pattern_features(p, 8, 1, False)
+    sh = numpy.fft.fftshift(p, axes=(-2, -1))[:, 4:12, 4:12]
+    ref = numpy.log1p(sh.astype(numpy.float64))
+    assert numpy.allclose(f, ref / ref.max(axis=(1, 2), keepdims=True), atol=1e-7)
+    # the mirror k -> -k of the stored pattern, read without flip, is the flipped read
+    mirrored = p[:, (-numpy.arange(16)) % 16][:, :, (-numpy.arange(16)) % 16]
+    assert numpy.allclose(C.pattern_features(p, 8, 1, True), C.pattern_features(mirrored, 8, 1, False))
+    # 2x2 binning sums the counts before the log
+    fb = C.pattern_features(p, 16, 2, False)
+    sb = numpy.log1p(numpy.fft.fftshift(p, axes=(-2, -1)).astype(numpy.float64).reshape(2, 8, 2, 8, 2).sum((2, 4)))
+    assert numpy.allclose(fb, sb / sb.max(axis=(1, 2), keepdims=True), atol=1e-7)
+
+
+def test_stitch_averages_overlaps_and_leaves_the_rest_at_one():
+    P, N = 4, 8
+    pred = numpy.zeros((2, 2, P, P), numpy.float32)
+    pred[0, 1] = 0.2
+    pred[1, 1] = 0.4
+    starts = numpy.array([[0, 0], [1, 0]])
+    out = C.stitch(pred, starts, N, 12, 12)
+    # patch rows 2..5 (first) and 3..6 (second), columns 2..5
+    assert numpy.allclose(out[2, 2], 1 + 0.2j) and numpy.allclose(out[6, 2], 1 + 0.4j)
+    assert numpy.allclose(out[3:6, 2:6], 1 + 0.3j)
+    assert numpy.allclose(out[0], 1) and numpy.allclose(out[:, 8:], 1)
+    w = numpy.zeros((P, P))
+    w[0] = 1.0            # only each patch's first row counts
+    outw = C.stitch(pred, starts, N, 12, 12, w)
+    assert numpy.allclose(outw[2, 2], 1 + 0.2j) and numpy.allclose(outw[3, 2], 1 + 0.4j)
+    assert numpy.allclose(outw[4, 2], 1)    # weight zero everywhere there
