@@ -392,6 +392,30 @@ int phb_stitch_finish(const void *acc, const float *wgt, void *obj, int64_t n, v
 /* product over the S slices of an (S, HW) complex64 object */
 int phb_project_slices(const void *obj, int64_t S, int64_t HW, void *out, void *stream);
 
+/* ---- state preparation in front of the engines (phaser/execute.py:334-402) ----
+ * Resampling of a stack of batch (H, W) planes onto (Ho, Wo): output pixel (i, j) is
+ * the bilinear interpolation, at (my * i + oy, mx * j + ox), of the input extended by
+ * cval beyond its edges -- scipy.ndimage.affine_transform with a diagonal matrix,
+ * order 1, mode 'grid-constant' (phaser/utils/image.py:151-195), as called by
+ * Sampling.resample (num.py:713-733) and ObjectSampling.resample (object.py:430-467).
+ * recip != 0 reads the input through fftshift and writes through ifftshift
+ * (Sampling.resample_recip, num.py:735-750) for patterns and masks stored with the
+ * zero frequency in the corner. */
+int phb_resample_c64(const void *in, int64_t batch, int32_t H, int32_t W, void *out, int32_t Ho, int32_t Wo,
+                     double my, double mx, double oy, double ox, float cval_re, float cval_im, int32_t recip,
+                     void *stream);
+int phb_resample_f32(const float *in, int64_t batch, int32_t H, int32_t W, float *out, int32_t Ho, int32_t Wo,
+                     double my, double mx, double oy, double ox, float cval, int32_t recip, void *stream);
+/* Reslicing along z (resample_slices, phaser/utils/object.py:56-157): out[i] =
+ * exp(new_t[i] * (wa[i] L(ja[i]) + wb[i] L(jb[i]))) per pixel, with L(k) =
+ * log(obj[k-1]) / old_t[k-1] for 1 <= k <= S_old and the padding slice for k = 0 and
+ * k = S_old + 1 (pad_mode 0 vacuum = 0, 1 edge = L(1) / L(S_old), 2 average = nanmean
+ * of L over the slices).  Tables are host arrays of S_new entries (S_old, S_new <= 128);
+ * the caller computes them from the slice centres (_interp1d, object.py:160-185). */
+int phb_resample_slices_c64(const void *obj, int32_t S_old, int64_t HW, const float *old_t, void *out,
+                            int32_t S_new, const float *new_t, const int32_t *ja, const int32_t *jb,
+                            const float *wa, const float *wb, int32_t pad_mode, void *stream);
+
 /* Per-iteration position update (phaser/engines/conventional/run.py:95-110 with
  * phaser/engines/common/position_correction.py): subtract mean, momentum or
  * steepest-descent step with norm clipping, subtract mean, scan += update, and

@@ -161,6 +161,12 @@ _SIGNATURES = {
                                    c_void_p, c_void_p, c_void_p, c_i64, c_i64, c_void_p]),
     'phb_stitch_finish': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p]),
     'phb_project_slices': (c_i32, [c_void_p, c_i64, c_i64, c_void_p, c_void_p]),
+    'phb_resample_c64': (c_i32, [c_void_p, c_i64, c_i32, c_i32, c_void_p, c_i32, c_i32, c_f64, c_f64, c_f64, c_f64,
+                                 c_f32, c_f32, c_i32, c_void_p]),
+    'phb_resample_f32': (c_i32, [c_void_p, c_i64, c_i32, c_i32, c_void_p, c_i32, c_i32, c_f64, c_f64, c_f64, c_f64,
+                                 c_f32, c_i32, c_void_p]),
+    'phb_resample_slices_c64': (c_i32, [c_void_p, c_i32, c_i64, c_void_p, c_void_p, c_i32, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_i32, c_void_p]),
     'phb_probe_regularizers_scratch_bytes': (ctypes.c_size_t, [c_i32, c_i32]),
     'phb_probe_regularizers': (c_i32, [c_void_p, c_i32, c_i32, ctypes.POINTER(PhbProbeReg), c_void_p, c_void_p,
                                        c_void_p, c_void_p]),

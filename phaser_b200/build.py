@@ -17,7 +17,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / 'csrc'
 LIB = PKG / 'libphaser_b200.so'
-SOURCES = ['phb_runtime.cu', 'phb_ops.cu', 'phb_engine.cu', 'phb_optim.cu', 'phb_constraints.cu', 'phb_cnn.cu']
+SOURCES = ['phb_runtime.cu', 'phb_ops.cu', 'phb_engine.cu', 'phb_optim.cu', 'phb_constraints.cu', 'phb_cnn.cu',
+           'phb_prepare.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

@@ -35,6 +35,10 @@ class NoiseSpec(t.NamedTuple):
     gaussian_variance: float = 0.1
 
 
+def _is_complex64(a) -> bool:
+    return a.dtype == (torch.complex64 if torch.is_tensor(a) else numpy.complex64)
+
+
 class DeviceEngine:
     """Device-resident state + workspace of one reconstruction.
 
@@ -55,13 +59,14 @@ class DeviceEngine:
             raise RuntimeError("the B200 backend needs a CUDA device")
         dev = torch.device(device)
         self.device = dev
-        probe = numpy.asarray(probe)
+        # probe and object: host arrays, or device tensors (e.g. from prepare_for_engine)
+        probe = probe if torch.is_tensor(probe) else numpy.asarray(probe)
         if probe.ndim == 2:
             probe = probe[None]
-        obj = numpy.asarray(obj)
+        obj = obj if torch.is_tensor(obj) else numpy.asarray(obj)
         if obj.ndim == 2:
             obj = obj[None]
-        if probe.dtype != numpy.complex64 or obj.dtype != numpy.complex64:
+        if not (_is_complex64(probe) and _is_complex64(obj)):
             raise TypeError("the B200 backend computes in complex64 (plan dtype float32)")
         M, N, N2 = probe.shape
         if N != N2 or N not in (64, 128):
@@ -85,6 +90,8 @@ class DeviceEngine:
             raise ValueError(f"{len(thick)} thicknesses for an object of {S} slices")
 
         def up(a, dt):
+            if torch.is_tensor(a):
+                return a.detach().to(dev).contiguous().clone()
             return torch.from_numpy(numpy.ascontiguousarray(a, dtype=dt)).to(dev)
 
         self.probe = up(probe, numpy.complex64)

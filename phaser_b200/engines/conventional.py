@@ -19,12 +19,21 @@ import torch
 from .. import plan as P
 from .. import _lib
 from ..constraints import build_constraints
-from ..device import DeviceEngine, NoiseSpec
+from ..device import DeviceEngine, NoiseSpec, _is_complex64
 from ..groups import GroupManager, mask_fraction_of_groups
 from ..sampling import ObjectSampling
 
 logger = logging.getLogger(__name__)
 
+
+
+def _array(a):
+    """A state array as given: a device tensor stays one, anything else becomes numpy."""
+    return a if torch.is_tensor(a) else numpy.asarray(a)
+
+
+def _host(a) -> numpy.ndarray:
+    return a.detach().cpu().numpy() if torch.is_tensor(a) else numpy.asarray(a)
 
 def _object_sampling(s) -> ObjectSampling:
     if isinstance(s, ObjectSampling):
@@ -108,17 +117,19 @@ class ConventionalEngine:
         self.calc_error = P.process_flag(P.get(props, 'calc_error', P.Flag(every=1)))
         self.shuffle_groups = P.process_flag(P.get(props, 'shuffle_groups', None) or not self.compact)
 
-        probe0 = numpy.asarray(state.probe.data)
-        obj0 = numpy.asarray(state.object.data)
+        probe0 = _array(state.probe.data)
+        obj0 = _array(state.object.data)
         self.scan0 = numpy.asarray(state.scan)
-        if probe0.dtype != numpy.complex64 or obj0.dtype != numpy.complex64:
+        if not (_is_complex64(probe0) and _is_complex64(obj0)):
             raise TypeError("object and probe must be complex64")
+        if patterns_on_device is None and torch.is_tensor(data.patterns):
+            patterns_on_device = data.patterns   # device-resident patterns (e.g. from prepare_for_engine)
         osamp = _object_sampling(state.object.sampling)
         thick = numpy.asarray(state.object.thicknesses)
         self.eng = eng = DeviceEngine(
             probe=probe0, obj=obj0, scan=self.scan0,
             patterns=None if patterns_on_device is not None else numpy.asarray(data.patterns),
-            mask=numpy.asarray(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
+            mask=_host(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
             obj_sampling=osamp, thicknesses=thick, wavelength=float(state.wavelength),
             tilt=None if state.tilt is None else numpy.asarray(state.tilt), noise=self.noise,
             bwlim_frac=P.get(props, 'bwlim_frac', 2 / 3), group_max=grouping,

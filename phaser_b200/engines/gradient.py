@@ -35,7 +35,7 @@ import torch
 from .. import plan as P
 from .. import _lib
 from ..constraints import build_constraints
-from ..device import DeviceEngine
+from ..device import DeviceEngine, _is_complex64
 from ..groups import GroupManager
 from .conventional import _call, _noise, _object_sampling
 
@@ -44,6 +44,15 @@ logger = logging.getLogger(__name__)
 _PER_ITER_VARS = frozenset({'positions', 'tilt'})
 _KINDS = {'sgd': _lib.PHB_OPTIM_SGD, 'adam': _lib.PHB_OPTIM_ADAM, 'polyak_sgd': _lib.PHB_OPTIM_POLYAK}
 
+
+
+def _array(a):
+    """A state array as given: a device tensor stays one, anything else becomes numpy."""
+    return a if torch.is_tensor(a) else numpy.asarray(a)
+
+
+def _host(a) -> numpy.ndarray:
+    return a.detach().cpu().numpy() if torch.is_tensor(a) else numpy.asarray(a)
 
 def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
@@ -266,20 +275,22 @@ class GradientEngine:
         }
         self.shuffle_groups = P.process_flag(P.get(props, 'shuffle_groups', None) or not self.compact)
 
-        probe0 = numpy.asarray(state.probe.data)
-        obj0 = numpy.asarray(state.object.data)
+        probe0 = _array(state.probe.data)
+        obj0 = _array(state.object.data)
         self.scan0 = numpy.asarray(state.scan)
         if 'tilt' in self.all_vars and state.tilt is None:
             # a zeroed tilt map, as phaser/execute.py:396-400 creates before the engine runs
             state.tilt = numpy.zeros_like(self.scan0)
         if 'tilt' in self.all_vars and len(numpy.asarray(state.object.thicknesses)) < 2:
             raise ValueError("tilt updates need a multislice object")
-        if probe0.dtype != numpy.complex64 or obj0.dtype != numpy.complex64:
+        if not (_is_complex64(probe0) and _is_complex64(obj0)):
             raise TypeError("object and probe must be complex64")
+        if patterns_on_device is None and torch.is_tensor(data.patterns):
+            patterns_on_device = data.patterns   # device-resident patterns (e.g. from prepare_for_engine)
         self.eng = eng = DeviceEngine(
             probe=probe0, obj=obj0, scan=self.scan0,
             patterns=None if patterns_on_device is not None else numpy.asarray(data.patterns),
-            mask=numpy.asarray(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
+            mask=_host(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
             obj_sampling=_object_sampling(state.object.sampling), thicknesses=numpy.asarray(state.object.thicknesses),
             wavelength=float(state.wavelength), tilt=None if state.tilt is None else numpy.asarray(state.tilt),
             noise=self.noise, bwlim_frac=P.get(props, 'bwlim_frac', 2 / 3), group_max=grouping,

@@ -105,9 +105,57 @@ class HookSpec:
     props: t.Any = None
 
 
+@dataclasses.dataclass
+class SliceList:
+    """Slice thicknesses listed (phaser/types.py:95-96)."""
+    thicknesses: t.List[float]
+
+
+@dataclasses.dataclass
+class SliceStep:
+    """n slices of one thickness (phaser/types.py:98-108)."""
+    n: int
+    slice_thickness: float
+
+    @property
+    def thicknesses(self) -> t.List[float]:
+        return [float(self.slice_thickness)] * int(self.n)
+
+
+@dataclasses.dataclass
+class SliceTotal:
+    """n equal slices of a total thickness (phaser/types.py:110-120)."""
+    n: int
+    total_thickness: float
+
+    @property
+    def thicknesses(self) -> t.List[float]:
+        return [float(self.total_thickness) / int(self.n)] * int(self.n)
+
+
+def slice_thicknesses(spec: t.Any) -> t.Optional[t.List[float]]:
+    """Thicknesses of a `slices` plan entry: a SliceList / SliceStep / SliceTotal (or an
+    object with a `thicknesses` attribute), the equivalent dict, a plain list, or None."""
+    if spec is None:
+        return None
+    if isinstance(spec, dict):
+        if 'thicknesses' in spec:
+            return [float(v) for v in spec['thicknesses']]
+        if 'slice_thickness' in spec:
+            return SliceStep(int(spec['n']), float(spec['slice_thickness'])).thicknesses
+        if 'total_thickness' in spec:
+            return SliceTotal(int(spec['n']), float(spec['total_thickness'])).thicknesses
+        raise ValueError(f"unknown slices specification {spec!r}")
+    if hasattr(spec, 'thicknesses'):
+        return [float(v) for v in spec.thicknesses]
+    return [float(v) for v in spec]
+
+
 @dataclasses.dataclass(eq=False)
 class ConventionalEnginePlan:
-    """Fields of phaser's ConventionalEnginePlan that the engine reads."""
+    """Fields of phaser's ConventionalEnginePlan that the engine reads (the EnginePlan
+    fields of phaser/plan.py:43-73 included: prepare_for_engine reads sim_shape,
+    resize_method, probe_modes, base_mode_power, obj_pad_px and slices)."""
     noise_model: t.Any = dataclasses.field(default_factory=lambda: HookSpec('amplitude', AmplitudeNoisePlan()))
     solver: t.Any = dataclasses.field(default_factory=lambda: HookSpec('lsqml', LSQMLSolverPlan()))
     position_solver: t.Any = None
@@ -126,6 +174,12 @@ class ConventionalEnginePlan:
     calc_error_fraction: float = 0.1
     bwlim_frac: t.Optional[float] = 2 / 3
     send_every_group: bool = False
+    sim_shape: t.Optional[t.Tuple[int, int]] = None
+    resize_method: str = 'pad_crop'
+    probe_modes: int = 1
+    base_mode_power: float = 0.7
+    obj_pad_px: float = 5.0
+    slices: t.Any = None
 
 
 @dataclasses.dataclass(eq=False)
@@ -147,6 +201,12 @@ class GradientEnginePlan:
     update_tilt: t.Any = False
     bwlim_frac: t.Optional[float] = 2 / 3
     send_every_group: bool = False
+    sim_shape: t.Optional[t.Tuple[int, int]] = None
+    resize_method: str = 'pad_crop'
+    probe_modes: int = 1
+    base_mode_power: float = 0.7
+    obj_pad_px: float = 5.0
+    slices: t.Any = None
 
 
 _NOISE_DEFAULTS = {'amplitude': AmplitudeNoisePlan, 'anscombe': AnscombeNoisePlan, 'poisson': PoissonNoisePlan}

@@ -75,6 +75,50 @@ class ObjectSampling:
         idx = self.pos_to_object_idx(pos, cutout_shape)
         return (idx - numpy.round(idx)).astype(numpy.float64) * self.sampling
 
+    @property
+    def min(self) -> numpy.ndarray:
+        return self.corner
+
+    @property
+    def max(self) -> numpy.ndarray:
+        """Position of the last pixel (object.py:205-208)."""
+        return (self.corner + (self.shape - 1) * self.sampling).astype(numpy.float64)
+
+    def __eq__(self, other: t.Any) -> bool:
+        """Same shape, sampling and corner (object.py:222-230)."""
+        if type(self) is not type(other):
+            return False
+        return (numpy.array_equal(self.shape, other.shape) and numpy.array_equal(self.sampling, other.sampling)
+                and numpy.array_equal(self.corner, other.corner))
+
+    __hash__ = object.__hash__
+
+    def with_sampling(self, sampling) -> 'ObjectSampling':
+        """The grid at pixel size `sampling` covering at least this one, half the growth on
+        each side (object.py:469-480)."""
+        sampling = numpy.broadcast_to(numpy.asarray(sampling, numpy.float64), (2,))
+        new_shape = numpy.ceil(self.sampling / sampling * self.shape).astype(int)
+        growth = sampling * new_shape - self.sampling * self.shape
+        if not numpy.all(growth / self.sampling >= -1e-4):
+            raise ValueError("resampled object grid would shrink")
+        return ObjectSampling(tuple(new_shape), sampling, self.corner - growth / 2. + (sampling - self.sampling) / 2.,
+                              self.region_min, self.region_max)
+
+    def expand_to_scan(self, scan, pad=0.) -> 'ObjectSampling':
+        """This grid padded (whole pixels) to cover every scan position plus `pad`
+        (object.py:257-275)."""
+        pad = numpy.broadcast_to(pad, (2,)).astype(numpy.float64)
+        smin = numpy.array([float(numpy.nanmin(scan[..., i])) for i in range(2)])
+        smax = numpy.array([float(numpy.nanmax(scan[..., i])) for i in range(2)])
+        pad_min = numpy.ceil(numpy.maximum(0, self.min - smin + pad) / self.sampling).astype(numpy.int_)
+        pad_max = numpy.ceil(numpy.maximum(0, smax - self.max + pad) / self.sampling).astype(numpy.int_)
+        if numpy.all(pad_min == 0) and numpy.all(pad_max == 0):
+            return self
+        rmin = numpy.minimum(self.region_min, smin) if self.region_min is not None else None
+        rmax = numpy.maximum(self.region_max, smax) if self.region_max is not None else None
+        return ObjectSampling(tuple(self.shape + pad_min + pad_max), self.sampling, self.corner - pad_min * self.sampling,
+                              rmin, rmax)
+
     def check_bounds(self, pad=0.) -> t.Tuple[numpy.ndarray, numpy.ndarray]:
         """(min, max) corner of the region in which probe positions overlap the object
         (object.py:277-289)."""

@@ -343,8 +343,65 @@ def constraints_case():
     save('constraints.npz', **out)
 
 
+def prepare_case():
+    """phaser.execute.prepare_for_engine (execute.py:334-402) on one small state under
+    several engine plans: detector/probe resizing (pad_crop and resample, up and
+    down), object resampling to the probe's pixel size and padding to the scan,
+    probe-mode truncation and creation, and z reslicing (multi->multi with each
+    alignment's default, single->multi, multi->single)."""
+    from phaser.execute import prepare_for_engine
+    from phaser.types import SliceList, SliceStep, SliceTotal
+    from phaser.utils.object import resample_slices
+    c = make_case(seed=31, N=32, M=2, S=3, scan_shape=(4, 4), step=2.0)
+    plans = {
+        'pad_crop_up': dict(sim_shape=(40, 40), resize_method='pad_crop', probe_modes=2),
+        'pad_crop_down': dict(sim_shape=(24, 24), resize_method='pad_crop', probe_modes=2),
+        'resample_up': dict(sim_shape=(36, 36), resize_method='resample', probe_modes=2),
+        'resample_down': dict(sim_shape=(28, 28), resize_method='resample', probe_modes=2, obj_pad_px=9.0),
+        'modes_down': dict(probe_modes=1),
+        'modes_up': dict(probe_modes=4, base_mode_power=0.6),
+        'reslice': dict(probe_modes=2, slices=SliceStep(n=5, slice_thickness=10.0)),
+        'reslice_total': dict(probe_modes=2, slices=SliceTotal(n=2, total_thickness=40.0)),
+        'to_single': dict(probe_modes=2, slices=SliceList(thicknesses=[])),
+    }
+    out = dict(case_arrays(c), osamp_shape=numpy.asarray(c['osamp'].shape),
+               region_min=numpy.asarray(c['osamp'].region_min), region_max=numpy.asarray(c['osamp'].region_max))
+    names = []
+    for name, kw in plans.items():
+        st = c['state'](c['est_obj'], c['probe'])
+        plan = ConventionalEnginePlan(
+            noise_model=NoiseModelHook('phaser.engines.common.noise_models:AmplitudeNoiseModel',
+                                       AmplitudeNoisePlan(), 'amplitude'),
+            solver=ConventionalSolverHook('phaser.engines.conventional.solvers:LSQMLSolver', LSQMLSolverPlan(),
+                                          'lsqml'),
+            group_constraints=[], iter_constraints=[], **kw)
+        pats, st2 = prepare_for_engine(Patterns(c['pats'].copy(), c['mask'].copy()), st, numpy, plan)
+        names.append(name)
+        os2 = st2.object.sampling
+        out.update({f'{name}__probe': st2.probe.data, f'{name}__probe_sampling': numpy.asarray(st2.probe.sampling.sampling),
+                    f'{name}__obj_shape': numpy.asarray(os2.shape),
+                    f'{name}__obj_sampling': numpy.asarray(os2.sampling), f'{name}__corner': numpy.asarray(os2.corner),
+                    f'{name}__region_min': numpy.asarray(os2.region_min), f'{name}__region_max': numpy.asarray(os2.region_max),
+                    f'{name}__thicknesses': numpy.asarray(st2.object.thicknesses)})
+        if st2.object.data.shape != c['est_obj'].shape or not numpy.array_equal(st2.object.data, c['est_obj']):
+            out[f'{name}__object'] = st2.object.data
+        if 'sim_shape' in kw:   # the other plans leave the patterns untouched
+            out.update({f'{name}__patterns': pats.patterns, f'{name}__mask': pats.pattern_mask})
+        else:
+            assert pats.patterns.shape == c['pats'].shape and numpy.array_equal(pats.patterns, c['pats'])
+    # resample_slices' other alignment and padding modes, on the same object
+    obj = c['est_obj'][:, 20:32, 24:36]
+    for align in ('top', 'middle', 'bottom'):
+        for pad in ('vacuum', 'edge', 'average'):
+            key = f'slices_{align}_{pad}'
+            out[key] = resample_slices(obj, c['thick'], [12.0, 9.0, 14.0, 11.0], align=align, pad_mode=pad)
+    out['plan_names'] = numpy.array(names)
+    save('prepare.npz', **out)
+
+
 CASES = {'numerics': numerics_case, 'cutouts': cutout_case, 'groupings': grouping_case,
-         'groups': group_cases, 'engines': engine_cases, 'constraints': constraints_case}
+         'groups': group_cases, 'engines': engine_cases, 'constraints': constraints_case,
+         'prepare': prepare_case}
 
 if __name__ == '__main__':
     for name in (sys.argv[1:] or list(CASES)):
