@@ -9,7 +9,9 @@ replaces jax.value_and_grad.  The kernel evaluates loss and adjoint in one
 launch, so the forward pass already holds the gradients and the backward pass
 only scales them by the incoming gradient.  Every slice's incident wavefield
 is kept (the per-slice checkpoints) in the engine's workspace for the adjoint:
-B_max x M x S x N^2 complex values, bounded by the group size.
+B_max x M x S x N^2 complex values, bounded by the group size.  From them the
+adjoint recomputes each slice's transmitted wave, its propagation and the
+object cutouts; no other forward intermediate is stored.
 
 Complex gradients follow torch's convention, dL/dRe + i dL/dIm, so
 `obj.grad` is what torch.autograd gives for a real loss of a complex leaf;
