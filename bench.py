@@ -449,7 +449,10 @@ def time_to_target(ds, pats, new_engine, iters: int, stream, warm: bool = True):
       warm_gradient: the gradient engine (hand-written adjoint kernel, Adam on object
                      and probe, amplitude noise model, grouping 256) from the warm start;
       plain_gradient: the gradient engine from the flat object (separates the warm
-                     start's share of the gain from the adjoint engine's).
+                     start's share of the gain from the adjoint engine's);
+      warm_gradient_lsqml: warm start, 3 gradient-engine iterations, then LSQ-ML
+                     polish for the remaining iterations (state handed over on the
+                     device; the hand-over time is counted).
     A warm arm's clock starts with the feature extraction, inference, stitching and
     residual tests (prep_seconds).  The network is trained first, once, on 200,704
     simulated patterns; its training time is reported beside, not inside, the race."""
@@ -505,6 +508,11 @@ def time_to_target(ds, pats, new_engine, iters: int, stream, warm: bool = True):
         "training_loss_per_epoch": [round(v, 5) for v in losses],
         "held_out_patch_mse": float(torch.mean((pred - th) ** 2)), "flat_patch_mse": float(torch.mean(th ** 2))}
     del fh, th, pred
+    # one untimed warm-start pass first: the first launch of each kernel loads its module
+    e = new_engine()
+    WS.warm_start_object(net, e.eng, pats, ds.scan)
+    torch.cuda.synchronize()
+    del e
     for arm, make in (("warm_lsqml", new_engine), ("warm_gradient", gradient_engine)):
         eng = make()
         torch.cuda.synchronize()
@@ -517,8 +525,36 @@ def time_to_target(ds, pats, new_engine, iters: int, stream, warm: bool = True):
         out[arm] = r
         del eng
     out["plain_gradient"] = nrmse_race(gradient_engine(), ref, iters, stream, target=target)
+    # the three forms chained: warm start, 3 gradient-engine iterations, LSQ-ML polish for the rest
+    n_grad = 3
+    g = gradient_engine()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    init, info = WS.warm_start_object(net, g.eng, pats, ds.scan)
+    torch.cuda.synchronize()
+    prep = time.perf_counter() - t0
+    first = nrmse_race(g, ref, n_grad, stream, init=init, prep_seconds=prep)
+    t0 = time.perf_counter()
+    polish = new_engine()
+    polish.eng.take_state(g.eng)
+    torch.cuda.synchronize()
+    handoff = time.perf_counter() - t0
+    del g
+    second = nrmse_race(polish, ref, iters - n_grad, stream, prep_seconds=first["seconds"][-1] + handoff)
+    curve = first["curve"] + second["curve"][1:]
+    secs = first["seconds"] + second["seconds"][1:]
+    hit = next((i for i, v in enumerate(curve) if v <= target), None)
+    out["warm_gradient_lsqml"] = {
+        "method": f"warm start, {n_grad} gradient-engine iterations, then LSQ-ML", "curve": curve, "seconds": secs,
+        "prep_seconds": prep, "handoff_seconds": handoff, "iterations_to_target": hit,
+        "seconds_to_target": None if hit is None else secs[hit], "final_nrmse": curve[-1], "fallback_test": info}
+    del polish
     out["seconds_to_target"] = {arm: out[arm].get("seconds_to_target")
-                                for arm in ("plain_lsqml", "warm_lsqml", "warm_gradient", "plain_gradient")}
+                                for arm in ("plain_lsqml", "warm_lsqml", "warm_gradient", "plain_gradient",
+                                            "warm_gradient_lsqml")}
+    out["final_nrmse"] = {arm: out[arm]["curve"][-1]
+                          for arm in ("plain_lsqml", "warm_lsqml", "warm_gradient", "plain_gradient",
+                                      "warm_gradient_lsqml")}
     return out
 
 

@@ -163,6 +163,19 @@ class DeviceEngine:
     def probe_changed(self) -> None:
         _lib.call('phb_engine_probe_changed', self._eref, _stream())
 
+    def take_state(self, other: 'DeviceEngine') -> None:
+        """Continue from another engine's reconstruction of the same dataset (e.g. the
+        gradient engine's result handed to LSQ-ML): object, probe, scan positions and
+        tilts are copied on the device."""
+        for name in ('object', 'probe', 'scan'):
+            mine, theirs = getattr(self, name), getattr(other, name)
+            if mine.shape != theirs.shape:
+                raise ValueError(f"{name} shapes differ: {tuple(mine.shape)} vs {tuple(theirs.shape)}")
+            mine.copy_(theirs)
+        if self.tilt is not None and other.tilt is not None:
+            self.tilt.copy_(other.tilt)
+        self.probe_changed()
+
     def group_tensor(self, flat_groups: t.Sequence[numpy.ndarray]) -> t.Tuple[torch.Tensor, t.List[int]]:
         """Upload a list of flat position-index arrays as one (G, B_max) int64 tensor."""
         G = len(flat_groups)

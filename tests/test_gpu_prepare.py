@@ -144,3 +144,51 @@ def test_engine_runs_on_the_prepared_device_state():
         results.append((out.object.data.copy(), out.probe.data.copy()))
     assert rel_l2(results[0][0], results[1][0]) < 1e-5 and rel_l2(results[0][1], results[1][1]) < 1e-5
     assert numpy.all(numpy.isfinite(results[0][0]))
+
+
+def test_take_state_continues_another_engines_reconstruction():
+    """The gradient engine's result handed to LSQ-ML on the device equals starting
+    LSQ-ML from host copies of that result."""
+    from phaser_b200.engines.conventional import ConventionalEngine
+    from phaser_b200.engines.gradient import GradientEngine
+    from phaser_b200.plan import GradientEnginePlan
+    from phaser_b200.synthetic import epie_single_slice_config, simulate_patterns
+    ds = epie_single_slice_config(seed=6)
+    pats = simulate_patterns(ds, seed=6, device='cuda', group=64)
+    N = ds.probe.shape[-1]
+
+    def state(probe=None, obj=None):
+        return ReconsState(iter=IterState(), wavelength=ds.wavelength,
+                           probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling),
+                                            ds.probe.copy() if probe is None else probe),
+                           object=ObjectState(ds.obj_sampling, ds.init_object.copy() if obj is None else obj,
+                                              ds.thicknesses.copy()),
+                           scan=ds.scan.copy())
+
+    args = dict(dtype=numpy.float32, seed='handoff', recons_name='h')
+    g = GradientEngine(dict(args, data=Patterns(None, ds.mask), state=state()),
+                       # Anscombe: with one mode and a flat start some far-field intensities are exactly
+                       # zero, where the amplitude model's d sqrt(I)/dI (jax's too) is infinite
+                       GradientEnginePlan(solvers={'object': {'type': 'adam', 'learning_rate': 1e-2}},
+                                          noise_model={'type': 'anscombe'}, niter=2, grouping=64),
+                       patterns_on_device=pats)
+    g.presolve()
+    g.iteration(1)
+    g.iteration(2)
+    plan = ConventionalEnginePlan(noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'}, niter=1, grouping=64)
+    a = ConventionalEngine(dict(args, data=Patterns(None, ds.mask), state=state()), plan, patterns_on_device=pats)
+    a.presolve()
+    a.eng.take_state(g.eng)
+    b = ConventionalEngine(dict(args, data=Patterns(None, ds.mask),
+                                state=state(g.eng.probe.cpu().numpy(), g.eng.object.cpu().numpy())), plan,
+                           patterns_on_device=pats)
+    b.eng.take_state(g.eng)     # same probe scale: skip b's own presolve
+    for e in (a, b):
+        e.iteration(1)
+    assert rel_l2(a.eng.object.cpu().numpy(), b.eng.object.cpu().numpy()) < 1e-5
+    assert rel_l2(a.eng.probe.cpu().numpy(), b.eng.probe.cpu().numpy()) < 1e-5
+    two_modes = numpy.concatenate([ds.probe, 0.1 * ds.probe]).astype(numpy.complex64)
+    other = ConventionalEngine(dict(args, data=Patterns(None, ds.mask), state=state(probe=two_modes)), plan,
+                               patterns_on_device=pats)
+    with pytest.raises(ValueError):
+        other.eng.take_state(g.eng)
