@@ -1,7 +1,7 @@
 """CPU oracle for the phaser multislice hot path -- TEST INFRASTRUCTURE ONLY.
 
 Nothing in the product (`phaser_b200`) imports this package.  It is used by
-`tests/` as the parity checker, by `__graft_entry__.smoke()` to check one
+`tests/` as the parity reference, by `__graft_entry__.smoke()` to check one
 small GPU invocation, and by `bench.py` for its CPU-baseline leg (the timed
 numpy implementation of the same algorithm, reported beside the GPU number).
 

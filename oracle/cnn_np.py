@@ -1,5 +1,5 @@
 """numpy restatement of the warm-start network's layers and of its training
-step: the checker the GPU kernels are tested against.  TEST INFRASTRUCTURE:
+step, which the GPU kernels are tested against.  TEST INFRASTRUCTURE:
 only tests/ and the benchmark's baseline code import this module.
 
 The warm start has no counterpart in the reference (it is this backend's
