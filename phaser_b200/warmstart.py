@@ -352,15 +352,24 @@ def phase_candidate(proj: torch.Tensor, S: int, scale: float) -> torch.Tensor:
 
 def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.ndarray, *,
                       window_sigma: t.Optional[float] = None, scales: t.Sequence[float] = (1.0, 1.25, 1.5),
-                      residual_stride: int = 4) -> t.Tuple[torch.Tensor, dict]:
+                      position_stride: int = 2, residual_stride: int = 8) -> t.Tuple[torch.Tensor, dict]:
     """The stitched warm-start object for the engine's geometry: every slice gets an equal
     share of the predicted projected phase, times the scale in `scales` whose simulated
     patterns fit the measurements best (on every residual_stride-th position); the
     engine's current object is kept instead when that fit is worse than its own.
-    Returns (object, info)."""
+    The network sees every position_stride-th pattern: at the benchmark geometry
+    (6 px steps, 32 px patches) every object pixel still gets ~14 overlapping
+    predictions, and halving them cost 0.001 in the stitched object's NRMSE
+    (0.1060 -> 0.1070) while halving the inference time (16.5 -> 8.3 ms for 4096
+    patterns).  Returns (object, info)."""
     S, H, W = eng.object.shape
-    feats = pattern_features(pats, net.features)
-    proj = stitch(net, feats, scan, eng.obj_sampling, (H, W), eng.N, window_sigma)
+    flat_scan = numpy.asarray(scan).reshape(-1, 2)
+    idx = numpy.arange(0, flat_scan.shape[0], max(1, int(position_stride)))
+    sub = pats.reshape(-1, *pats.shape[-2:])
+    if len(idx) != flat_scan.shape[0]:
+        sub = sub[torch.from_numpy(idx).to(pats.device)]
+    feats = pattern_features(sub, net.features)
+    proj = stitch(net, feats, flat_scan[idx], eng.obj_sampling, (H, W), eng.N, window_sigma)
     r_flat = pattern_residual(eng, eng.object, residual_stride)
     best = None
     tried = {}
