@@ -41,6 +41,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "multislice pos*slice/s (LSQ-ML iteration, 1 B200)"
+METRIC_GRAD = "multislice pos*slice/s (gradient-engine iteration, 1 B200)"
 UNIT = "pos*slice/s"
 CONFIG = {"workload": "multislice LSQ-ML: 8 x 517^2 slices (2 nm), probe 128^2 x 4 modes, "
                       "scan 64x64=4096 @ 6 px, batch 256, position correction on",
@@ -48,10 +49,12 @@ CONFIG = {"workload": "multislice LSQ-ML: 8 x 517^2 slices (2 nm), probe 128^2 x
           "solver": "lsqml", "noise_model": "amplitude", "l2": "working set > L2 (1.07 GB psi scratch per batch)"}
 
 
-def algorithmic_bytes_per_pos_slice(N: int, M: int, S: int, pattern_bytes: int = 4) -> int:
+def algorithmic_bytes_per_pos_slice(N: int, M: int, S: int, pattern_bytes: int = 4, engine: str = 'lsqml') -> int:
     """O cutout read fwd + adj (16 N^2), psi store + reload (16 M N^2), object-update
-    scatter (8 N^2), illumination scatter (4 N^2), pattern read amortised over S."""
-    return N * N * (28 + 16 * M) + pattern_bytes * N * N // S
+    scatter (8 N^2), illumination scatter (4 N^2, LSQ-ML only), pattern read amortised
+    over S."""
+    illum = 4 if engine == 'lsqml' else 0
+    return N * N * (24 + illum + 16 * M) + pattern_bytes * N * N // S
 
 
 def measured_sm_max_mhz():
@@ -72,9 +75,9 @@ def measured_peaks():
         return 6650.0, 'fallback'
 
 
-def ncu_traffic_per_launch():
+def ncu_traffic_per_launch(engine: str = 'lsqml'):
     """dram bytes (read + write) per k_group launch from the committed ncu summary."""
-    path = os.path.join(ROOT, 'profiles', 'k_group_lsqml_c2.md')
+    path = os.path.join(ROOT, 'profiles', f'k_group_{"grad" if engine == "gradient" else "lsqml"}_c2.md')
     try:
         for line in open(path):
             if line.strip().startswith('traffic_bytes_per_full_launch:'):
@@ -226,6 +229,7 @@ def run_b200(args, world, rank, local):
     from phaser_b200 import _lib
     from phaser_b200.synthetic import lsqml_multislice_config, simulate_patterns
     from phaser_b200.engines.conventional import ConventionalEngine
+    from phaser_b200.engines.gradient import GradientEngine
     from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
     from phaser_b200.sampling import Sampling
     from phaser_b200 import plan as PL
@@ -246,6 +250,9 @@ def run_b200(args, world, rank, local):
         config.update(workload=f"reduced multislice LSQ-ML (scan {args.scan}x{args.scan}, batch {args.batch})",
                       positions=args.scan * args.scan, batch=args.batch,
                       object=[int(v) for v in ds.obj_sampling.shape])
+    if args.engine == 'gradient':
+        config.update(workload=config["workload"].replace("LSQ-ML", "gradient engine (hand-written adjoint, Adam)")
+                      .replace(", position correction on", ""), solver="gradient (adam: object 1e-2, probe 1e-3)")
     pats_host = pats.cpu().pin_memory()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -272,7 +279,20 @@ def run_b200(args, world, rank, local):
         e.presolve()
         return e
 
-    eng = new_engine()
+    def new_gradient_engine():
+        state = ReconsState(iter=IterState(), wavelength=ds.wavelength,
+                            probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
+                            object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
+                            scan=ds.scan.copy())
+        props = PL.GradientEnginePlan(
+            solvers={'object': {'type': 'adam', 'learning_rate': 1e-2}, 'probe': {'type': 'adam', 'learning_rate': 1e-3}},
+            noise_model={'type': 'amplitude'}, niter=10 ** 6, grouping=args.batch)
+        e = GradientEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
+                            'seed': 'bench', 'recons_name': 'bench-grad'}, props, patterns_on_device=pats)
+        e.presolve()
+        return e
+
+    eng = new_gradient_engine() if args.engine == 'gradient' else new_engine()
     stream = torch.cuda.current_stream()
     it = 0
     for _ in range(args.warmup):
@@ -376,12 +396,13 @@ def run_b200(args, world, rank, local):
     # ---------------- roofline of the fused kernel
     peak, peak_kind = measured_peaks()
     B = args.batch
-    bytes_launch = algorithmic_bytes_per_pos_slice(N, M, S) * B * S
+    bytes_launch = algorithmic_bytes_per_pos_slice(N, M, S, engine=args.engine) * B * S
     avg_ms = float(numpy.mean(fused)) if fused else float('nan')
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
-    traffic = ncu_traffic_per_launch()
+    traffic = ncu_traffic_per_launch(args.engine)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic if (args.scan == 64 and args.batch == 256) else None, "traffic_unit": "GB per launch (ncu)", "kernel": "k_group<128> (fused LSQ-ML mini-batch)",
+            "traffic": traffic if (args.scan == 64 and args.batch == 256) else None, "traffic_unit": "GB per launch (ncu)", "kernel": ("k_group<128> (fused gradient-engine mini-batch: loss + adjoint)" if args.engine == 'gradient'
+                       else "k_group<128> (fused LSQ-ML mini-batch)"),
             "launch_ms": avg_ms, "launches_timed": len(fused), "bytes_per_launch": bytes_launch,
             "peak_source": f"{peak_kind} hbm_gbs", "share_of_step": sum(fused) / t_ms if t_ms else None}
     # the kernel's other bound: FP32 FFT work (5 N^2 log2 N^2 per transform, M (4 + 4/S) transforms
@@ -394,7 +415,8 @@ def run_b200(args, world, rank, local):
                          "frac": flops / fp32_peak, "flop_per_pos_slice": flop_ps}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": METRIC if args.engine == 'lsqml' else METRIC_GRAD, "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
                 "config": dict(config, parallelism=f"replicas x{world}"),
@@ -642,6 +664,8 @@ def main():
     ap.add_argument('--no-extra', action='store_true', help='skip the single-slice ePIE and gradient-engine lines')
     ap.add_argument('--nrmse-iters', type=int, default=20, help='iterations of the NRMSE run (20 = the configuration)')
     ap.add_argument('--no-warm', action='store_true', help='time-to-NRMSE: plain LSQ-ML arm only (no network training)')
+    ap.add_argument('--engine', default='lsqml', choices=['lsqml', 'gradient'],
+                    help='engine timed for the throughput line (the benchmark configuration is lsqml)')
     ap.add_argument('--scan', type=int, default=64, help='scan side (64 = the benchmark configuration)')
     ap.add_argument('--batch', type=int, default=256, help='mini-batch size (256 = the benchmark configuration)')
     args = ap.parse_args()
