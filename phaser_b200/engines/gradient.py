@@ -365,13 +365,7 @@ class GradientEngine:
             if self.fused_events is not None:
                 ev = _new_event_pair()
                 self.fused_events.append(ev)
-            eng.step('grad', gt[gi], B, flags=flags, group_index=gi, events=ev,
-                     grad_object=self.grad_object if 'object' in iter_vars else None,
-                     grad_probe=self.grad_probe if 'probe' in iter_vars else None,
-                     grad_pos=self.grad_pos if 'positions' in iter_vars else None,
-                     grad_pos_scale=-1.0 / (probe_int * B), group_loss=losses[gi:gi + 1],
-                     grad_tilt=self.grad_tilt if 'tilt' in iter_vars else None,
-                     grad_tilt_scale=-1.0 / (probe_int * B))
+            self._grad_step(gt[gi], B, flags, gi, ev, iter_vars, losses[gi:gi + 1], probe_int)
             self.regularizers.apply(eng, B, self.grad_object if 'object' in iter_vars else None, losses[gi:gi + 1],
                                     self.grad_probe if 'probe' in iter_vars else None)
             dirs = {}
@@ -410,6 +404,20 @@ class GradientEngine:
             return None
         torch.cuda.current_stream().synchronize()
         return self.check(i, 'positions' in iter_vars)
+
+    def _grad_step(self, group: torch.Tensor, B: int, flags: int, gi: int, events, iter_vars, group_loss,
+                   probe_int: float) -> None:
+        """Loss and gradients of one mini-batch into the engine's gradient buffers."""
+        self.eng.step('grad', group, B, flags=flags, group_index=gi, events=events, **self._grad_kw(B, iter_vars,
+                                                                                                  group_loss, probe_int))
+
+    def _grad_kw(self, B: int, iter_vars, group_loss, probe_int: float) -> dict:
+        return dict(grad_object=self.grad_object if 'object' in iter_vars else None,
+                    grad_probe=self.grad_probe if 'probe' in iter_vars else None,
+                    grad_pos=self.grad_pos if 'positions' in iter_vars else None,
+                    grad_pos_scale=-1.0 / (probe_int * B), group_loss=group_loss,
+                    grad_tilt=self.grad_tilt if 'tilt' in iter_vars else None,
+                    grad_tilt_scale=-1.0 / (probe_int * B))
 
     def check(self, i: int, it_pos: bool = True) -> float:
         state, eng = self.state, self.eng

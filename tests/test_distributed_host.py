@@ -1,7 +1,8 @@
 """Host side of the data-parallel mini-batch split, on CPU with two gloo ranks:
 row ranges cover every mini-batch exactly once, the accumulator all-reduce sums
 the ranks' shares, and the iteration report combines NaN status and error
-means as one process would compute them."""
+means as one process would compute them, and the gradient engine's NaN status
+is the same on every rank."""
 import os
 import socket
 
@@ -10,7 +11,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from phaser_b200.distributed import allreduce_sum, combine_report, split_rows
+from phaser_b200.distributed import allreduce_sum, combine_report, combine_status, split_rows
 
 
 def test_split_rows_partitions_every_batch():
@@ -46,7 +47,13 @@ def _worker(rank: int, world: int, port: int, q):
         combine_report(rep)
         empty = torch.tensor([-1.0, 0.0, float('nan'), 0.0], dtype=torch.float64)
         combine_report(empty)
-        q.put((rank, f32.tolist(), f64.tolist(), rep.tolist(), empty.tolist()))
+        # gradient-engine status: rank 1 saw group 5 go non-finite, rank 0 nothing -> 5 on both;
+        # both fine -> -1
+        st = torch.tensor([[-1, 5][rank]], dtype=torch.int32)
+        combine_status(st)
+        ok = torch.tensor([-1], dtype=torch.int32)
+        combine_status(ok)
+        q.put((rank, f32.tolist(), f64.tolist(), rep.tolist(), empty.tolist(), int(st[0]), int(ok[0])))
     finally:
         dist.destroy_process_group()
 
@@ -62,7 +69,8 @@ def test_allreduce_and_report_over_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, f32, f64, rep, empty in out:
+    for rank, f32, f64, rep, empty, st, ok in out:
+        assert st == 5 and ok == -1
         assert f32 == [float(i + 1) for i in range(10)]
         assert f64 == [3.0] * 4
         assert rep[0] == 3.0 and rep[1] == 2.0

@@ -2,9 +2,11 @@
 here, so two ranks are emulated by two engines on the same device whose
 partial steps never wait on each other: rank 1's accumulators are added into
 rank 0's (what the all-reduce does), rank 0 finishes, and the result must
-match one full step (1e-5 relative L2; fp32 atomics reorder sums).  A whole
-run of DistributedConventionalEngine on a one-rank NCCL group must match
-ConventionalEngine."""
+match one full step (1e-5 relative L2; fp32 atomics reorder sums).  The same
+holds for the gradient engine's loss and gradients, where the object gradient
+buffer is summed too.  Whole runs of DistributedConventionalEngine and
+DistributedGradientEngine on a one-rank NCCL group must match the plain
+engines."""
 import os
 import socket
 
@@ -15,8 +17,10 @@ import torch.distributed as dist
 
 from phaser_b200 import _lib
 from phaser_b200 import plan as PL
-from phaser_b200.distributed import DistributedConventionalEngine
+from phaser_b200.distributed import DistributedConventionalEngine, DistributedGradientEngine
 from phaser_b200.engines.conventional import ConventionalEngine
+from phaser_b200.device import NoiseSpec
+from phaser_b200.engines.gradient import GradientEngine
 from phaser_b200.state import Patterns
 
 from .cases import make_case
@@ -79,6 +83,61 @@ def test_distributed_engine_on_one_rank_matches_engine():
     finally:
         dist.destroy_process_group()
     assert numpy.allclose(errs, errs_ref, rtol=1e-5)
+    assert rel_l2(st_d.object.data, st_r.object.data) < 1e-5
+    assert rel_l2(st_d.probe.data, st_r.probe.data) < 1e-5
+    assert numpy.max(numpy.abs(st_d.scan - st_r.scan)) < 1e-5
+
+
+def test_partial_gradient_steps_summed_match_one_step():
+    c = make_case(seed=73, N=64, M=2, S=3, scan_shape=(4, 4))
+    idx = numpy.random.default_rng(3).permutation(16)[:11].astype(numpy.int64)
+    flags = _lib.PHB_FLAG_UPDATE_OBJECT | _lib.PHB_FLAG_UPDATE_PROBE | _lib.PHB_FLAG_UPDATE_POSITION
+    engs = [engine_for(c, 11, noise=NoiseSpec('poisson', 1e-3, 0.0, 0.1)) for _ in range(3)]
+    bufs = []
+    for e, rows in zip(engs, (None, (0, 4), (4, 11))):
+        e.status.fill_(-1)
+        g = e.group_tensor([idx])[0][0]
+        b = dict(grad_object=torch.zeros_like(e.object), grad_probe=torch.zeros_like(e.probe),
+                 grad_pos=torch.zeros_like(e.scan), group_loss=torch.zeros(1, dtype=torch.float64, device='cuda'))
+        e.step('grad', g, 11, flags=flags, grad_pos_scale=-0.5, rows=rows, **b)
+        bufs.append((g, b))
+    (a32, a64), (b32, b64) = engs[1].reduce_views(), engs[2].reduce_views()
+    a32 += b32
+    a64 += b64
+    bufs[1][1]['grad_object'] += bufs[2][1]['grad_object']
+    engs[1].finish(bufs[1][0], 11)
+    torch.cuda.synchronize()
+    full, part = bufs[0][1], bufs[1][1]
+    for k in ('grad_object', 'grad_probe'):
+        assert rel_l2(part[k].cpu().numpy(), full[k].cpu().numpy()) < 1e-5, k
+    assert rel_l2(part['grad_pos'].cpu().numpy()[idx], full['grad_pos'].cpu().numpy()[idx]) < 1e-4
+    assert float(part['group_loss'][0]) == pytest.approx(float(full['group_loss'][0]), rel=1e-9)
+    assert int(engs[1].status.cpu()[0]) == -1
+
+
+def test_distributed_gradient_engine_on_one_rank_matches_engine():
+    c = make_case(seed=74, N=64, M=2, S=2, scan_shape=(5, 5))
+    props = PL.GradientEnginePlan(
+        solvers={'object': {'type': 'adam', 'learning_rate': 1e-2}, 'probe': {'type': 'adam', 'learning_rate': 1e-3},
+                 'positions': {'type': 'sgd', 'learning_rate': 1e-2}},
+        noise_model={'type': 'poisson', 'eps': 1e-3}, niter=2, grouping=10, update_positions=True)
+    args = dict(data=Patterns(c.patterns, c.mask), dtype=numpy.float32, seed='dist-grad', recons_name='t')
+    ref = GradientEngine(dict(args, state=make_state(c)), props)
+    ref.presolve()
+    loss_ref = [ref.iteration(i) for i in (1, 2)]
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+    dist.init_process_group('nccl', rank=0, world_size=1, device_id=torch.device('cuda', 0))
+    try:
+        eng = DistributedGradientEngine(dict(args, state=make_state(c)), props)
+        eng.presolve()
+        loss = [eng.iteration(i) for i in (1, 2)]
+        st_d, st_r = eng.finish(), ref.finish()
+    finally:
+        dist.destroy_process_group()
+    assert numpy.allclose(loss, loss_ref, rtol=1e-5)
     assert rel_l2(st_d.object.data, st_r.object.data) < 1e-5
     assert rel_l2(st_d.probe.data, st_r.probe.data) < 1e-5
     assert numpy.max(numpy.abs(st_d.scan - st_r.scan)) < 1e-5
