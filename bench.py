@@ -652,6 +652,53 @@ def extra_configs(dev, stream):
     return out
 
 
+def run_cnn(args):
+    """Throughput of the warm-start network's kernels alone: `args.cnn` random 64x64
+    inputs through inference (batch 256) and through training steps (forward,
+    backward, Adam; batch 256), CUDA events on the current stream, after warm-up.
+    FLOP per pattern: 2 x (multiply-adds of the five 3x3 convolutions) forward,
+    3 x that for a training step (forward, data and weight gradients)."""
+    import torch
+    from phaser_b200 import warmstart as WS
+    dev = torch.device('cuda', 0)
+    torch.cuda.set_device(dev)
+    n = int(args.cnn)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(0)
+    x = torch.rand((n, 1, 64, 64), generator=gen, device=dev)
+    tgt = torch.rand((n, 2, 32, 32), generator=gen, device=dev) * 0.1
+    net = WS.WarmStartNet(seed=0)
+    macs = 0
+    side = 64
+    for ci, co, st, relu, up in WS.LAYERS:
+        side //= st
+        macs += side * side * co * ci * 9
+        side *= 2 if up else 1
+    flop_fwd = 2 * macs
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for _ in range(max(1, args.warmup)):
+        net.predict(x)
+    ev[0].record()
+    for _ in range(args.steps):
+        net.predict(x)
+    ev[1].record()
+    net.train(x, tgt, epochs=1, batch=256)
+    ev[2].record()
+    net.train(x, tgt, epochs=max(1, args.steps // 2), batch=256)
+    ev[3].record()
+    torch.cuda.synchronize()
+    t_inf = ev[0].elapsed_time(ev[1]) / 1e3 / args.steps
+    t_train = ev[2].elapsed_time(ev[3]) / 1e3 / max(1, args.steps // 2)
+    fp32_peak = 148 * 128 * 2 * (measured_sm_max_mhz() or 1965.0) * 1e6
+    print(json.dumps({"metric": "warm-start network patterns/s", "unit": "patterns/s", "patterns": n,
+                      "inference": {"value": n / t_inf, "ms": t_inf * 1e3, "tflops": n * flop_fwd / t_inf / 1e12,
+                                    "fp32_frac": n * flop_fwd / t_inf / fp32_peak},
+                      "training": {"value": n / t_train, "ms_per_epoch": t_train * 1e3,
+                                   "tflops": 3 * n * flop_fwd / t_train / 1e12,
+                                   "fp32_frac": 3 * n * flop_fwd / t_train / fp32_peak},
+                      "flop_per_pattern_forward": flop_fwd}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -668,8 +715,13 @@ def main():
                     help='engine timed for the throughput line (the benchmark configuration is lsqml)')
     ap.add_argument('--scan', type=int, default=64, help='scan side (64 = the benchmark configuration)')
     ap.add_argument('--batch', type=int, default=256, help='mini-batch size (256 = the benchmark configuration)')
+    ap.add_argument('--cnn', type=int, default=0, metavar='PATTERNS',
+                    help='only time the warm-start network on this many patterns (training step and inference)')
     args = ap.parse_args()
     world, rank, local = setup_dist()
+    if args.cnn:
+        run_cnn(args)
+        return
     if args.impl == 'reference':
         run_reference(args, world, rank)
     else:

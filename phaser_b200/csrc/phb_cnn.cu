@@ -24,8 +24,13 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const float *in, const __nv_bf
                                                   float *out, int Ci, int Hi, int Wi, int Co, int Ho, int Wo,
                                                   int relu) {
     constexpr int PH = (CT - 1) * S + 3;
-    __shared__ float patch[CIB][PH][PH];
-    __shared__ float ws[CIB][9][COB];
+    // Row stride of the staged input: a warp reads two tile rows (16 threads each); at
+    // stride 1 a row stride of 48 words puts the second half-warp 16 banks after the
+    // first, so the two never share a bank.
+    constexpr int PW = S == 1 ? 48 : PH;
+    __shared__ float patch[CIB][PH][PW];
+    // weights [ci][tap][co], read as float4 broadcasts (4 output channels per load)
+    __shared__ __align__(16) float ws[CIB][9][COB];
     const int tiles_x = (Wo + CT - 1) / CT;
     const int ty0 = (blockIdx.x / tiles_x) * CT, tx0 = (blockIdx.x % tiles_x) * CT;
     const int co0 = blockIdx.y * COB, n = blockIdx.z;
@@ -54,8 +59,20 @@ __global__ void __launch_bounds__(256) k_conv_fwd(const float *in, const __nv_bf
 #pragma unroll
             for (int t = 0; t < 9; ++t) {
                 const float v = patch[c][ty * S + t / 3][tx * S + t % 3];
+                if constexpr (COB % 4 == 0) {
+                    const float4 *w4 = reinterpret_cast<const float4 *>(&ws[c][t][0]);
 #pragma unroll
-                for (int o = 0; o < COB; ++o) acc[o] = fmaf(v, ws[c][t][o], acc[o]);
+                    for (int o = 0; o < COB / 4; ++o) {
+                        const float4 q = w4[o];
+                        acc[4 * o + 0] = fmaf(v, q.x, acc[4 * o + 0]);
+                        acc[4 * o + 1] = fmaf(v, q.y, acc[4 * o + 1]);
+                        acc[4 * o + 2] = fmaf(v, q.z, acc[4 * o + 2]);
+                        acc[4 * o + 3] = fmaf(v, q.w, acc[4 * o + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int o = 0; o < COB; ++o) acc[o] = fmaf(v, ws[c][t][o], acc[o]);
+                }
             }
         __syncthreads();
     }
@@ -77,7 +94,7 @@ template <int CIO, int S>
 __global__ void __launch_bounds__(256) k_conv_bwd_data(const float *dout, const __nv_bfloat16 *w, float *din,
                                                        int Ci, int Hi, int Wi, int Co, int Ho, int Wo) {
     constexpr int COB2 = 8;
-    __shared__ float ws[COB2][9][CIO];
+    __shared__ __align__(16) float ws[COB2][9][CIO];   // read as float4 broadcasts
     const int tiles_x = (Wi + CT - 1) / CT;
     const int Y = (blockIdx.x / tiles_x) * CT + threadIdx.x / CT, X = (blockIdx.x % tiles_x) * CT + threadIdx.x % CT;
     const int ci0 = blockIdx.y * CIO, n = blockIdx.z;
@@ -105,8 +122,20 @@ __global__ void __launch_bounds__(256) k_conv_bwd_data(const float *dout, const 
                     const int co = co0 + o;
                     if (co >= Co) break;
                     const float g = dn[((size_t)co * Ho + yy) * Wo + xx];
+                    if constexpr (CIO % 4 == 0) {
+                        const float4 *w4 = reinterpret_cast<const float4 *>(&ws[o][t][0]);
 #pragma unroll
-                    for (int c = 0; c < CIO; ++c) acc[c] = fmaf(g, ws[o][t][c], acc[c]);
+                        for (int c = 0; c < CIO / 4; ++c) {
+                            const float4 q = w4[c];
+                            acc[4 * c + 0] = fmaf(g, q.x, acc[4 * c + 0]);
+                            acc[4 * c + 1] = fmaf(g, q.y, acc[4 * c + 1]);
+                            acc[4 * c + 2] = fmaf(g, q.z, acc[4 * c + 2]);
+                            acc[4 * c + 3] = fmaf(g, q.w, acc[4 * c + 3]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < CIO; ++c) acc[c] = fmaf(g, ws[o][t][c], acc[c]);
+                    }
                 }
             }
         }
