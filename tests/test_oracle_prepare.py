@@ -73,3 +73,29 @@ def test_resample_slices_matches_reference(align, pad):
     obj = g['object'][:, 20:32, 24:36]
     out = PR.resample_slices(obj, g['thicknesses'], [12.0, 9.0, 14.0, 11.0], align, pad)
     assert rel_l2(out, g[f'slices_{align}_{pad}']) < 1e-5
+
+
+def test_product_grid_arithmetic_matches_reference():
+    """The host grid steps of phaser_b200.prepare (ObjectSampling.with_sampling and
+    expand_to_scan, the slices specifications) give the reference's grids."""
+    from phaser_b200 import plan as PL
+    from phaser_b200.sampling import ObjectSampling
+    g = load('prepare.npz')
+    grid = ObjectSampling(tuple(g['osamp_shape']), g['obj_sampling'], g['corner'], g['region_min'], g['region_max'])
+    N = numpy.asarray(g['probe'].shape[-2:])
+    psamp = numpy.asarray(g['probe_sampling'])
+    for name, shape, method, pad in (('pad_crop_up', 40, 'pad_crop', 5.0), ('resample_down', 28, 'resample', 9.0)):
+        new_samp = psamp * N / shape if method == 'pad_crop' else psamp
+        g2 = grid.with_sampling(new_samp) if not numpy.allclose(new_samp, grid.sampling) else grid
+        g2 = g2.expand_to_scan(g['scan'], new_samp * shape / 2. + pad * new_samp)
+        p = name + '__'
+        assert numpy.array_equal(g2.shape, g[p + 'obj_shape'])
+        assert numpy.allclose(g2.corner, g[p + 'corner'], rtol=1e-12, atol=1e-12)
+        assert numpy.allclose(g2.region_min, g[p + 'region_min']) and numpy.allclose(g2.region_max, g[p + 'region_max'])
+    assert grid.expand_to_scan(g['scan'], psamp * N / 2. + 5.0 * psamp) == grid   # already covers the scan
+    assert PL.slice_thicknesses(PL.SliceStep(n=5, slice_thickness=10.0)) == [10.0] * 5
+    assert PL.slice_thicknesses({'n': 2, 'total_thickness': 40.0}) == [20.0, 20.0]
+    assert PL.slice_thicknesses({'thicknesses': [1, 2]}) == [1.0, 2.0]
+    assert PL.slice_thicknesses(PL.SliceList(thicknesses=[])) == [] and PL.slice_thicknesses(None) is None
+    with pytest.raises(ValueError):
+        PL.slice_thicknesses({'n': 3})
