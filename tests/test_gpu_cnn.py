@@ -29,7 +29,8 @@ def bf16_tensor(w):
 
 
 @pytest.mark.parametrize('ci,co,stride,H', [(1, 32, 2, 64), (32, 64, 2, 32), (64, 64, 1, 16), (64, 32, 1, 32),
-                                            (32, 2, 1, 32), (3, 5, 1, 20), (5, 17, 2, 18)])
+                                            (32, 2, 1, 32), (3, 5, 1, 20), (5, 17, 2, 18), (6, 20, 1, 40),
+                                            (7, 33, 1, 34)])
 def test_conv_layer_matches_oracle(ci, co, stride, H):
     rng = numpy.random.default_rng(ci * 100 + co)
     B = 3
