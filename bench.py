@@ -581,15 +581,18 @@ def time_to_target(ds, pats, new_engine, iters: int, stream, warm: bool = True):
 
 
 def extra_configs(dev, stream):
-    """The other two configurations of the benchmark description, measured on the
+    """The other configurations of the benchmark description, measured on the
     same GPU (device time of whole iterations, patterns resident):
       single-slice ePIE: 64^2 probe, 1 mode, 32x32 scan at 4 px (+-0.5 px jitter),
         1e5 e-/pattern, grouping 64, 10 iterations from the flat start;
       gradient engine: 16 x 2 nm slices of 774^2 (reference geometry of a 128x128 scan
         at 5 px), probe 128^2 x 2 modes, Poisson negative log-likelihood, Adam on object
-        and probe, grouping 64, 2 timed iterations after 1 warm-up."""
+        and probe, grouping 64, 2 timed iterations after 1 warm-up;
+      large multislice (detector binned 2x2 to 128^2, see large_multislice_config):
+        LSQ-ML and the gradient engine, 1 timed iteration each after 1 warm-up."""
     import torch
-    from phaser_b200.synthetic import epie_single_slice_config, gradient_multislice_config, simulate_patterns
+    from phaser_b200.synthetic import (epie_single_slice_config, gradient_multislice_config,
+                                       large_multislice_config, simulate_patterns)
     from phaser_b200.engines.conventional import ConventionalEngine
     from phaser_b200.engines.gradient import GradientEngine
     from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
@@ -649,6 +652,46 @@ def extra_configs(dev, stream):
                     "128x128 scan @ 5 px, Poisson NLL, Adam, grouping 64",
         "value": n_pos * S * 2 / secs, "unit": UNIT, "ms_per_iteration": secs / 2 * 1e3}
     del eng, pats
+    torch.cuda.empty_cache()
+    # the large configuration with its 256^2 detector binned to 128^2 (the reference's
+    # sim_shape path): 32 x 1033^2 slices, 8 modes, 65536 positions, uint16 counts resident
+    ds = large_multislice_config(seed=3)
+    pats = simulate_patterns(ds, seed=3, device=dev, group=256)
+    peak_count = float(pats.max())
+    if peak_count >= 65536:
+        raise RuntimeError(f"large configuration: {peak_count} counts do not fit uint16")
+    pats16 = pats.to(torch.uint16)
+    del pats
+    torch.cuda.empty_cache()
+    n_pos, S = int(numpy.prod(ds.scan.shape[:-1])), ds.true_object.shape[0]
+    large = {"workload": f"large multislice: {S} x {ds.obj_sampling.shape[0]}^2 slices, probe 256^2 x 8 modes with "
+                         "the detector binned 2x2 to 128^2 (sim_shape 128, 'resample'), 256x256 scan @ 3 px, "
+                         "5e5 e-/pattern as uint16 counts resident (2.1 GB), batch 256",
+             "unit": UNIT, "peak_count": peak_count}
+    for kind in ('lsqml', 'gradient'):
+        if kind == 'lsqml':
+            props = PL.ConventionalEnginePlan(
+                noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
+                position_solver={'type': 'momentum', 'step_size': 1e-3, 'max_step_size': 0.2, 'momentum': 0.9},
+                niter=10 ** 6, grouping=256, update_positions=True)
+            eng = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state_of(ds), 'dtype': numpy.float32,
+                                      'seed': 'bench-c5', 'recons_name': 'c5'}, props, patterns_on_device=pats16)
+        else:
+            props = PL.GradientEnginePlan(
+                solvers={'object': {'type': 'adam', 'learning_rate': 1e-2},
+                         'probe': {'type': 'adam', 'learning_rate': 1e-3}},
+                noise_model={'type': 'amplitude'}, niter=10 ** 6, grouping=256)
+            eng = GradientEngine({'data': Patterns(None, ds.mask), 'state': state_of(ds), 'dtype': numpy.float32,
+                                  'seed': 'bench-c5', 'recons_name': 'c5-grad'}, props, patterns_on_device=pats16)
+        eng.presolve()
+        timed(eng, 1, 1)
+        secs = timed(eng, 2, 1)
+        large[kind] = {"value": n_pos * S / secs, "seconds_per_iteration": secs}
+        del eng
+        torch.cuda.empty_cache()
+    out['large_multislice_binned'] = large
+    del pats16
+    torch.cuda.empty_cache()
     return out
 
 

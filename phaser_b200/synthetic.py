@@ -66,7 +66,11 @@ class Dataset:
 def make_dataset(*, N: int, M: int, S: int, scan_shape: t.Tuple[int, int], step_px: float, sampling: float,
                  kv: float, conv_mrad: float, defocus: float, slice_thickness: float, spacing_px: float,
                  sigma_px: float, peak_rad: float, counts: float, mode_powers: t.Sequence[float] = (),
-                 scan_jitter_px: float = 0.0, seed: int = 0) -> Dataset:
+                 scan_jitter_px: float = 0.0, seed: int = 0, grid_probe_px: t.Optional[int] = None) -> Dataset:
+    """A seeded dataset.  The object grid is the reference's for a probe of
+    grid_probe_px pixels (N when None): a dataset prepared for a larger detector
+    keeps its grid when the detector is binned down to N (prepare_for_engine only
+    pads objects)."""
     rng = numpy.random.default_rng(seed)
     lam = electron_wavelength(kv)
     psamp = Sampling((N, N), sampling=(sampling, sampling))
@@ -85,7 +89,8 @@ def make_dataset(*, N: int, M: int, S: int, scan_shape: t.Tuple[int, int], step_
     if scan_jitter_px:
         scan = scan + rng.uniform(-scan_jitter_px, scan_jitter_px, scan.shape) * sampling
     scan = scan.astype(numpy.float32)
-    osamp = ObjectSampling.from_scan(scan, psamp.sampling, psamp.extent / 2. + 5 * psamp.sampling)
+    grid_extent = psamp.sampling * (grid_probe_px or N)
+    osamp = ObjectSampling.from_scan(scan, psamp.sampling, grid_extent / 2. + 5 * psamp.sampling)
     H, W = (int(v) for v in osamp.shape)
     phase = numpy.stack([lattice_phase((H, W), spacing_px, sigma_px, peak_rad, rng) for _ in range(S)])
     true_obj = numpy.exp(1j * phase).astype(numpy.complex64)
@@ -103,6 +108,17 @@ def lsqml_multislice_config(seed: int = 0, scan: int = 64) -> Dataset:
     return make_dataset(N=128, M=4, S=8, scan_shape=(scan, scan), step_px=6.0, sampling=0.2, kv=300e3,
                         conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
                         peak_rad=0.2, counts=1e6, mode_powers=(0.70, 0.15, 0.10, 0.05), seed=seed)
+
+
+# the large multislice configuration (32 slices of 1032^2, 8 modes, 256 x 256 scan at 3 px,
+# 5e5 e-/pattern) with its 256^2 detector binned 2 x 2 to 128^2: the pixel size stays
+# 0.2 A, the probe window halves to 25.6 A (the 25 mrad probe at 200 A defocus is ~10 A
+# across), i.e. prepare_for_engine with sim_shape (128, 128), resize_method 'resample'.
+# The object grid is the one the reference builds for the 256^2 probe.
+def large_multislice_config(seed: int = 0, scan: int = 256) -> Dataset:
+    return make_dataset(N=128, M=8, S=32, scan_shape=(scan, scan), step_px=3.0, sampling=0.2, kv=300e3,
+                        conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
+                        peak_rad=0.2, counts=5e5, seed=seed, grid_probe_px=256)
 
 
 # the single-slice ePIE configuration (256^2-class object, 64^2 probe, 32^2 scan)
