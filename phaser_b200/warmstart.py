@@ -251,8 +251,22 @@ def random_lattice_objects(n: int, *, seed: int = 0, scan: int = 32, slices: t.T
         yield ds
 
 
+def _as_f32(pats: torch.Tensor, rows: t.Optional[torch.Tensor] = None) -> torch.Tensor:
+    """float32 copy of patterns (or of the given rows).  uint16 counts are read through
+    an int16 view, since torch has no CUDA indexing or arithmetic for uint16."""
+    if pats.dtype == torch.uint16:
+        x = pats.view(torch.int16)
+        x = x if rows is None else x[rows]
+        return (x.to(torch.int32) & 0xFFFF).to(torch.float32)
+    x = pats if rows is None else pats[rows]
+    return x.to(torch.float32)
+
+
 def pattern_features(pats: torch.Tensor, spec: FeatureSpec = DEFAULT_FEATURES) -> torch.Tensor:
     """Network inputs (n, 1, 64, 64) of patterns (n, N, N) (zero frequency at [0, 0])."""
+    if pats.dtype != torch.float32:   # e.g. uint16 counts held resident
+        pats = _as_f32(pats)
+    pats = pats.reshape(-1, *pats.shape[-2:]).contiguous()
     n, N = pats.shape[0], pats.shape[-1]
     side = spec.crop // spec.bin
     if side != IN_SIDE or spec.crop > N:
@@ -337,7 +351,7 @@ def pattern_residual(eng, obj: torch.Tensor, stride: int = 1) -> float:
     total = torch.zeros((), dtype=torch.float64, device=eng.device)
     for g, B in enumerate(sizes):
         sim = eng.simulate(gt[g], B)
-        meas = eng.patterns[rows[g * G:g * G + B]].to(torch.float32)
+        meas = _as_f32(eng.patterns, rows[g * G:g * G + B])
         total += torch.sum((torch.sqrt(sim) - torch.sqrt(torch.clamp(meas, min=0))) ** 2, dtype=torch.float64)
     eng.object.copy_(saved)
     return float(total)
@@ -367,7 +381,7 @@ def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.nd
     idx = numpy.arange(0, flat_scan.shape[0], max(1, int(position_stride)))
     sub = pats.reshape(-1, *pats.shape[-2:])
     if len(idx) != flat_scan.shape[0]:
-        sub = sub[torch.from_numpy(idx).to(pats.device)]
+        sub = _as_f32(sub, torch.from_numpy(idx).to(pats.device))
     feats = pattern_features(sub, net.features)
     proj = stitch(net, feats, flat_scan[idx], eng.obj_sampling, (H, W), eng.N, window_sigma)
     r_flat = pattern_residual(eng, eng.object, residual_stride)

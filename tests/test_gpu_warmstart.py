@@ -112,3 +112,18 @@ def test_a_rejected_warm_start_keeps_the_flat_object(trained, held_out):
     obj, info = WS.warm_start_object(net, eng, pats, ds.scan, scales=(60.0,))
     assert not info['used'] and info['residual_warm'] > info['residual_flat']
     assert torch.equal(obj, flat)
+
+
+def test_uint16_patterns_give_the_same_warm_start(trained, held_out):
+    """Counts held as uint16 (the resident format for large scans) give the warm start
+    of the same counts in float32."""
+    net, _ = trained
+    ds, pats = held_out
+    assert float(pats.max()) < 65536 and torch.equal(pats, torch.round(pats))
+    e32 = lsqml_factory(ds, pats)().eng
+    o32, i32 = WS.warm_start_object(net, e32, pats, ds.scan)
+    p16 = pats.to(torch.int32).to(torch.int16).view(torch.uint16)    # same bits as a uint16 cast
+    e16 = lsqml_factory(ds, p16)().eng
+    o16, i16 = WS.warm_start_object(net, e16, p16, ds.scan)
+    assert i16['used'] == i32['used'] and i16['scale'] == i32['scale']
+    assert torch.allclose(o16, o32, rtol=1e-6, atol=1e-6)
