@@ -72,3 +72,30 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     assert lib.phb_fft2_c64(None, None, 1, 128, 0, None) == _lib.PHB_ERR_INVALID_ARG
     assert lib.phb_cutout_get_c64(None, 1, 1, 1, None, 1, 1, 1, 1.0, 0.0, None, None) == _lib.PHB_ERR_INVALID_ARG
     assert lib.phb_solver_group(None, None, None, 0, None) == _lib.PHB_ERR_INVALID_ARG
+
+
+def test_argument_checks_return_status_without_touching_a_gpu():
+    """Entry points reject null pointers and impossible sizes with a status code, before
+    any CUDA call (so this runs without a GPU).  Pointer arguments here are never
+    dereferenced: every call fails its argument check first."""
+    lib = _lib.load()
+    bad = _lib.PHB_ERR_INVALID_ARG
+    fake = ctypes.c_void_p(0x1000)   # non-null but never used: the size checks fail first
+    # resampling: null input, empty shapes
+    assert lib.phb_resample_c64(None, 1, 8, 8, fake, 8, 8, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0, None) == bad
+    assert lib.phb_resample_f32(fake, 0, 8, 8, fake, 8, 8, 1.0, 1.0, 0.0, 0.0, 0.0, 0, None) == bad
+    assert lib.phb_resample_f32(fake, 1, 8, 8, fake, 0, 8, 1.0, 1.0, 0.0, 0.0, 0.0, 0, None) == bad
+    # reslicing: too many slices, bad padding mode, null tables
+    i32 = (ctypes.c_int32 * 1)(1)
+    f32 = (ctypes.c_float * 1)(1.0)
+    assert lib.phb_resample_slices_c64(fake, 200, 16, f32, fake, 1, f32, i32, i32, f32, f32, 0, None) == bad
+    assert lib.phb_resample_slices_c64(fake, 1, 16, f32, fake, 1, f32, i32, i32, f32, f32, 3, None) == bad
+    assert lib.phb_resample_slices_c64(fake, 1, 16, None, fake, 1, f32, i32, i32, f32, f32, 0, None) == bad
+    # warm-start helpers: windows that do not divide, empty batches
+    assert lib.phb_pattern_features(fake, None, 1, 64, 63, 1, 0, fake, None) == bad
+    assert lib.phb_pattern_features(fake, None, 1, 64, 128, 1, 0, fake, None) == bad
+    assert lib.phb_pattern_features(fake, None, 0, 64, 64, 1, 0, fake, None) == bad
+    assert lib.phb_stitch_patches(None, fake, None, 1, 0.0, 0.0, 1.0, 1.0, 64, 32, None, fake, fake, 8, 8, None) == bad
+    assert lib.phb_stitch_patches(fake, fake, None, 1, 0.0, 0.0, 1.0, 1.0, 64, 65, None, fake, fake, 8, 8, None) == bad
+    assert lib.phb_conv3x3_fwd(None, fake, fake, fake, 1, 1, 8, 8, 1, 1, 0, None) == bad
+    assert lib.phb_conv3x3_fwd(fake, fake, fake, fake, 1, 1, 8, 8, 1, 3, 0, None) == _lib.PHB_ERR_UNSUPPORTED
