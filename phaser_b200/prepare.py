@@ -241,8 +241,7 @@ def prepare_for_engine(patterns: Patterns, state: t.Any, engine: t.Any, *,
 
     if isinstance(engine, P.GradientEnginePlan) or hasattr(engine, 'solvers'):
         solvers = P.get(engine, 'solvers', {}) or {}
-        names = set(itertools.chain.from_iterable(
-            (v.strip() for v in k.split(',')) if isinstance(k, str) else tuple(k) for k in solvers))
+        names = set(itertools.chain.from_iterable(P.recons_vars(k) for k in dict(solvers)))
         if 'tilt' in names and state.tilt is None:
             log.info("Creating new, zeroed tilt map...")
             state.tilt = numpy.zeros_like(numpy.asarray(state.scan))
