@@ -157,6 +157,14 @@ def resample_slices(obj: torch.Tensor, old_t, new_t, *, align: str = 'middle',
     return out
 
 
+def solves_for_tilt(engine: t.Any) -> bool:
+    """Whether a gradient plan has a solver for the tilt variable (execute.py:396-400)."""
+    if not (isinstance(engine, P.GradientEnginePlan) or hasattr(engine, 'solvers')):
+        return False
+    solvers = P.get(engine, 'solvers', {}) or {}
+    return 'tilt' in set(itertools.chain.from_iterable(P.recons_vars(k) for k in dict(solvers)))
+
+
 def _as_sampling(s) -> Sampling:
     if isinstance(s, Sampling):
         return s
@@ -239,12 +247,9 @@ def prepare_for_engine(patterns: Patterns, state: t.Any, engine: t.Any, *,
         obj = resample_slices(obj, thick, new_t)
         thick = numpy.array(new_t, dtype=thick.dtype if thick.size else numpy.float32)
 
-    if isinstance(engine, P.GradientEnginePlan) or hasattr(engine, 'solvers'):
-        solvers = P.get(engine, 'solvers', {}) or {}
-        names = set(itertools.chain.from_iterable(P.recons_vars(k) for k in dict(solvers)))
-        if 'tilt' in names and state.tilt is None:
-            log.info("Creating new, zeroed tilt map...")
-            state.tilt = numpy.zeros_like(numpy.asarray(state.scan))
+    if solves_for_tilt(engine) and state.tilt is None:
+        log.info("Creating new, zeroed tilt map...")
+        state.tilt = numpy.zeros_like(numpy.asarray(state.scan))
 
     state.probe.data = probe
     state.probe.sampling = psamp

@@ -99,3 +99,14 @@ def test_product_grid_arithmetic_matches_reference():
     assert PL.slice_thicknesses(PL.SliceList(thicknesses=[])) == [] and PL.slice_thicknesses(None) is None
     with pytest.raises(ValueError):
         PL.slice_thicknesses({'n': 3})
+
+
+def test_tilt_map_rule():
+    """A gradient plan whose solvers name 'tilt' gets a zero tilt map (execute.py:396-400)."""
+    from phaser_b200 import plan as PL
+    from phaser_b200.prepare import solves_for_tilt
+    assert solves_for_tilt(PL.GradientEnginePlan(solvers={'object': {'type': 'adam'}, 'tilt': {'type': 'sgd'}}))
+    assert solves_for_tilt(PL.GradientEnginePlan(solvers={'positions,tilt': {'type': 'sgd'}}))
+    assert solves_for_tilt(PL.GradientEnginePlan(solvers={frozenset({'tilt'}): {'type': 'sgd'}}))
+    assert not solves_for_tilt(PL.GradientEnginePlan(solvers={'object': {'type': 'adam'}}))
+    assert not solves_for_tilt(PL.ConventionalEnginePlan())
