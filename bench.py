@@ -22,12 +22,17 @@ Workload (one "step" = one full LSQ-ML iteration over the scan):
   --impl reference : times the reference's CPU algorithm (the numpy port in
           oracle/) on this host with all its threads, same metric and config.
 
-Multi-GPU (torchrun): every rank runs an independent reconstruction
-(replicas); value = total pos*slice/s over ranks / max rank time.
+Multi-GPU (torchrun): ONE reconstruction split over the ranks (data-parallel:
+each mini-batch's positions are divided into contiguous row ranges, the partial
+update accumulators are summed with NCCL all-reduces, every rank applies the
+same update); value = the reconstruction's pos*slice/s / max rank time
+(strong scaling).  --replicas runs independent reconstructions instead (weak
+scaling, no collective).
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -43,10 +48,14 @@ sys.path.insert(0, ROOT)
 METRIC = "multislice pos*slice/s (LSQ-ML iteration, 1 B200)"
 METRIC_GRAD = "multislice pos*slice/s (gradient-engine iteration, 1 B200)"
 UNIT = "pos*slice/s"
-CONFIG = {"workload": "multislice LSQ-ML: 8 x 517^2 slices (2 nm), probe 128^2 x 4 modes, "
+CONFIG = {"workload": "multislice LSQ-ML: 8 x 518^2 slices (2 nm), probe 128^2 x 4 modes, "
                       "scan 64x64=4096 @ 6 px, batch 256, position correction on",
-          "N": 128, "modes": 4, "slices": 8, "object": [517, 517], "positions": 4096, "batch": 256,
+          "N": 128, "modes": 4, "slices": 8, "object": [518, 518], "positions": 4096, "batch": 256,
           "solver": "lsqml", "noise_model": "amplitude", "l2": "working set > L2 (1.07 GB psi scratch per batch)"}
+
+
+def parallelism(world: int, replicas: bool) -> str:
+    return f"replicas x{world}" if replicas else ("single GPU" if world == 1 else f"data-parallel x{world}")
 
 
 def algorithmic_bytes_per_pos_slice(N: int, M: int, S: int, pattern_bytes: int = 4, engine: str = 'lsqml') -> int:
@@ -203,7 +212,7 @@ def run_reference(args, world, rank):
                 cache[i] = im
         return numpy.stack([cache[int(i)] for i in idx])
 
-    batch = 16
+    batch = args.batch   # the mini-batch size of the GPU arm's line
     S = ds.true_object.shape[0]
     for _ in range(args.warmup):
         cpu_sample(ds, pats, 1, batch, threads, seed=_)
@@ -214,11 +223,14 @@ def run_reference(args, world, rank):
     t = float(numpy.mean(times))
     value = batch * S / t
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference", "config": CONFIG,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak" if (args.replicas or world == 1) else "strong",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference",
+            "config": dict(CONFIG, parallelism=parallelism(world, args.replicas)),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"each step: one LSQ-ML mini-batch of {batch} positions at the full shapes "
-                                       f"(numpy oracle, scipy.fft with {threads} threads)"},
+                             "sample": f"each step: one LSQ-ML mini-batch of {batch} positions (the line's batch) "
+                                       f"at the full shapes (numpy oracle, scipy.fft with {threads} threads; "
+                                       f"patterns simulated by the oracle, untimed)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -242,14 +254,15 @@ def run_b200(args, world, rank, local):
                                 device_id=dev)
     lib = _lib.load()
 
-    # CPU baseline first (rank 0, N == 1), before the device is busy
-    ds = lsqml_multislice_config(seed=rank, scan=args.scan)
-    pats = simulate_patterns(ds, seed=rank, device=dev)
-    config = dict(CONFIG)
+    # CPU baseline first (rank 0, N == 1), before the device is busy.  Data-parallel ranks
+    # share one dataset (same seed); replicas each get their own.
+    dp = world > 1 and not args.replicas
+    ds = lsqml_multislice_config(seed=0 if dp else rank, scan=args.scan)
+    pats = simulate_patterns(ds, seed=0 if dp else rank, device=dev)
+    config = dict(CONFIG, object=[int(v) for v in ds.obj_sampling.shape])
     if args.scan != 64 or args.batch != 256:   # reduced case (profiling); not the benchmark line
         config.update(workload=f"reduced multislice LSQ-ML (scan {args.scan}x{args.scan}, batch {args.batch})",
-                      positions=args.scan * args.scan, batch=args.batch,
-                      object=[int(v) for v in ds.obj_sampling.shape])
+                      positions=args.scan * args.scan, batch=args.batch)
     if args.engine == 'gradient':
         config.update(workload=config["workload"].replace("LSQ-ML", "gradient engine (hand-written adjoint, Adam)")
                       .replace(", position correction on", ""), solver="gradient (adam: object 1e-2, probe 1e-3)")
@@ -258,14 +271,14 @@ def run_b200(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         host_np = pats_host.numpy()
-        rate, secs, desc = cpu_sample(ds, lambda idx: host_np[idx], 2, 16, threads)
+        rate, secs, desc = cpu_sample(ds, lambda idx: host_np[idx], 1, args.batch, threads)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": desc + f" (numpy oracle, scipy.fft with {threads} threads), {secs:.1f} s"}
 
     N, M, S = ds.probe.shape[-1], ds.probe.shape[0], ds.true_object.shape[0]
     n_pos = int(numpy.prod(ds.scan.shape[:-1]))
 
-    def new_engine():
+    def new_engine(split: bool = False):
         state = ReconsState(iter=IterState(), wavelength=ds.wavelength,
                             probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
                             object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
@@ -274,8 +287,11 @@ def run_b200(args, world, rank, local):
             noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
             position_solver={'type': 'momentum', 'step_size': 1e-3, 'max_step_size': 0.2, 'momentum': 0.9},
             niter=10 ** 6, grouping=args.batch, update_positions=True)
-        e = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
-                                'seed': 'bench', 'recons_name': 'bench'}, props, patterns_on_device=pats)
+        cls = ConventionalEngine
+        if split:
+            from phaser_b200.distributed import DistributedConventionalEngine as cls
+        e = cls({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
+                 'seed': 'bench', 'recons_name': 'bench'}, props, patterns_on_device=pats)
         e.presolve()
         return e
 
@@ -287,13 +303,22 @@ def run_b200(args, world, rank, local):
         props = PL.GradientEnginePlan(
             solvers={'object': {'type': 'adam', 'learning_rate': 1e-2}, 'probe': {'type': 'adam', 'learning_rate': 1e-3}},
             noise_model={'type': 'amplitude'}, niter=10 ** 6, grouping=args.batch)
-        e = GradientEngine({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
-                            'seed': 'bench', 'recons_name': 'bench-grad'}, props, patterns_on_device=pats)
+        cls = GradientEngine
+        if dp:
+            from phaser_b200.distributed import DistributedGradientEngine as cls
+        e = cls({'data': Patterns(None, ds.mask), 'state': state, 'dtype': numpy.float32,
+                 'seed': 'bench', 'recons_name': 'bench-grad'}, props, patterns_on_device=pats)
         e.presolve()
         return e
 
-    eng = new_gradient_engine() if args.engine == 'gradient' else new_engine()
+    eng = new_gradient_engine() if args.engine == 'gradient' else new_engine(split=dp)
     stream = torch.cuda.current_stream()
+    # FP32 CUDA-core peak of this GPU (FMA probe), the denominator of fp32_pipe.frac
+    fp32_measured = None
+    if rank == 0:
+        tf = ctypes.c_double()
+        _lib.call('phb_fp32_peak', 4096, ctypes.byref(tf), None, stream.cuda_stream)
+        fp32_measured = tf.value
     it = 0
     for _ in range(args.warmup):
         it += 1
@@ -321,7 +346,6 @@ def run_b200(args, world, rank, local):
     barrier()
     t_ms = ev0.elapsed_time(ev1)
     fused = []
-    import ctypes
     for a, b in eng.fused_events:
         ms = ctypes.c_float()
         _lib.call('phb_event_elapsed_ms', a, b, ctypes.byref(ms))
@@ -333,8 +357,9 @@ def run_b200(args, world, rank, local):
         tt = torch.tensor([t_ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_ms = float(tt.item())
-    units_per_step = n_pos * S
-    value = world * units_per_step * args.steps / (t_ms / 1e3)
+    units_per_step = n_pos * S            # one reconstruction's iteration
+    replicas_here = world if not dp else 1   # replicas each run their own reconstruction
+    value = replicas_here * units_per_step * args.steps / (t_ms / 1e3)
 
     # ---------------- end-to-end: host patterns -> device each step, status back each step.
     # Double-buffered: step k+1's patterns are copied from pinned host memory on a copy
@@ -381,7 +406,7 @@ def run_b200(args, world, rank, local):
         tt = torch.tensor([e2e_t], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_t = float(tt.item())
-    e2e_value = world * units_per_step / (e2e_t / 1e3)
+    e2e_value = replicas_here * units_per_step / (e2e_t / 1e3)
     del bufs
 
     # ---------------- reconstruction quality: plain LSQ-ML from the flat start, NRMSE vs the true object
@@ -396,7 +421,7 @@ def run_b200(args, world, rank, local):
     # ---------------- roofline of the fused kernel
     peak, peak_kind = measured_peaks()
     B = args.batch
-    bytes_launch = algorithmic_bytes_per_pos_slice(N, M, S, engine=args.engine) * B * S
+    bytes_launch = algorithmic_bytes_per_pos_slice(N, M, S, engine=args.engine) * (B if not dp else -(-B // world)) * S
     avg_ms = float(numpy.mean(fused)) if fused else float('nan')
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     traffic = ncu_traffic_per_launch(args.engine)
@@ -410,16 +435,20 @@ def run_b200(args, world, rank, local):
     # (148 SMs x 128 FMA lanes x 2 FLOP x max SM clock, an estimate: not in MEASURED_PEAKS.json)
     flop_ps = 5 * N * N * numpy.log2(N * N) * M * (4 + 4 / S) + 60 * M * N * N
     fp32_peak = 148 * 128 * 2 * (measured_sm_max_mhz() or 1965.0) * 1e6
-    flops = flop_ps * B * S / (avg_ms / 1e3)
+    rows_launch = B if not dp else -(-B // world)   # a data-parallel rank runs its share of the rows
+    flops = flop_ps * rows_launch * S / (avg_ms / 1e3)
     roof["fp32_pipe"] = {"achieved_tflops": flops / 1e12, "peak_tflops_estimate": fp32_peak / 1e12,
-                         "frac": flops / fp32_peak, "flop_per_pos_slice": flop_ps}
+                         "frac_of_estimate": flops / fp32_peak, "flop_per_pos_slice": flop_ps}
+    if fp32_measured:
+        roof["fp32_pipe"].update(peak_tflops_measured=fp32_measured, frac=flops / 1e12 / fp32_measured,
+                                 peak_source="FMA probe (phb_fp32_peak), measured in this run")
 
     if rank == 0:
         line = {"metric": METRIC if args.engine == 'lsqml' else METRIC_GRAD, "value": value, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-                "config": dict(config, parallelism=f"replicas x{world}"),
+                "scaling": "strong" if dp else "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "config": dict(config, parallelism=parallelism(world, args.replicas)),
                 "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(pats_host.numel() * 4),
                         "d2h_bytes_per_step": 32},
@@ -808,6 +837,8 @@ def main():
     ap.add_argument('--steps', type=int, default=10)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--replicas', action='store_true',
+                    help='N > 1: independent reconstructions per rank (weak scaling) instead of one data-parallel one')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-nrmse', action='store_true')

@@ -245,7 +245,11 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
  * on the GPU (other streams, other threads) race and corrupt each other -- order
  * them on one stream.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call waits once for its stream (propagator check). */
+ * capture.  Besides that, EVERY call copies the propagator check's result to
+ * the host and waits for its stream to finish before it launches the step.
+ * PHB_FLAG_PARTIAL is refused with PHB_ERR_UNSUPPORTED: a partial share left in
+ * the library's array could not be summed over ranks by the caller, and the
+ * next call clears it. */
 int phb_solver_group_static(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
                             void *stream);
 
@@ -436,6 +440,13 @@ int phb_iteration_report(const int32_t *status, const int32_t *n_outside, const 
 
 /* Kernel launches issued by this library since it was loaded (all streams). */
 int64_t phb_kernel_launches(void);
+
+/* FP32 CUDA-core throughput of the current device, measured (no counterpart in the
+ * reference: the denominator of the FP32-pipe roofline fraction).  Eight independent
+ * FMA chains per thread, 64 warps per SM, `iters` FMAs per chain; one untimed launch,
+ * then one launch timed with CUDA events on `stream`.  Synchronises on `stream`.
+ * *tflops = FLOP / time (2 FLOP per FMA), *ms the timed launch (may be NULL). */
+int phb_fp32_peak(int32_t iters, double *tflops, float *ms, void *stream);
 
 /* cudaEvent_t helpers for callers without a CUDA runtime binding. */
 int phb_event_create(void **event);

@@ -184,6 +184,7 @@ _SIGNATURES = {
     'phb_iteration_reset': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
     'phb_iteration_report': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p, c_void_p]),
     'phb_kernel_launches': (c_i64, []),
+    'phb_fp32_peak': (c_i32, [c_i32, ctypes.POINTER(c_f64), ctypes.POINTER(c_f32), c_void_p]),
     'phb_event_create': (c_i32, [ctypes.POINTER(c_void_p)]),
     'phb_event_destroy': (c_i32, [c_void_p]),
     'phb_event_record': (c_i32, [c_void_p, c_void_p]),

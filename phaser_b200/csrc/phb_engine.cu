@@ -1753,6 +1753,9 @@ extern "C" int phb_solver_group_static(const phb_engine *e, const phb_step *st, 
                                        void *stream) {
     using namespace phb;
     if (!e || !st || !group || B < 1) return PHB_ERR_INVALID_ARG;
+    // a partial launch leaves its share in the accumulators for a later finish call, but
+    // the next call here clears them (and the caller cannot reach this array): refuse it
+    if (st->flags & PHB_FLAG_PARTIAL) return PHB_ERR_UNSUPPORTED;
     int dev = 0;
     int rc = record_cuda(cudaGetDevice(&dev));
     if (rc) return rc;

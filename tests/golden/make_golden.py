@@ -1,9 +1,10 @@
 """Generate the golden fixtures in this folder by running the REFERENCE phaser
 numpy code (not the oracle) on small seeded inputs.
 
-Run in a container that has the reference sources:
+Run where the reference sources are available, with PHASER_REF naming the
+root of the phaser source tree (required):
 
-    PHASER_REF=/root/reference python tests/golden/make_golden.py
+    PHASER_REF=<phaser source root> python tests/golden/make_golden.py
 
 `pane` (py-pane 0.11.3) is not installed there, so `pane_shim/` supplies the
 few names the reference imports.  The fixtures store inputs and outputs, so the
@@ -19,7 +20,9 @@ from pathlib import Path
 import numpy
 
 HERE = Path(__file__).resolve().parent
-REF = os.environ.get('PHASER_REF', '/root/reference')
+REF = os.environ.get('PHASER_REF')
+if not REF:
+    sys.exit("set PHASER_REF to the root of the phaser source tree")
 sys.path.insert(0, str(HERE / 'pane_shim'))
 sys.path.insert(0, REF)
 

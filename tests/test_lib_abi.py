@@ -72,6 +72,11 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     assert lib.phb_fft2_c64(None, None, 1, 128, 0, None) == _lib.PHB_ERR_INVALID_ARG
     assert lib.phb_cutout_get_c64(None, 1, 1, 1, None, 1, 1, 1, 1.0, 0.0, None, None) == _lib.PHB_ERR_INVALID_ARG
     assert lib.phb_solver_group(None, None, None, 0, None) == _lib.PHB_ERR_INVALID_ARG
+    # the allocation-free step refuses a partial (data-parallel) launch before any CUDA call
+    desc, st = _lib.PhbEngine(), _lib.PhbStep()
+    st.flags = _lib.PHB_FLAG_PARTIAL
+    grp = (ctypes.c_int64 * 1)(0)
+    assert lib.phb_solver_group_static(ctypes.byref(desc), ctypes.byref(st), grp, 1, None) == _lib.PHB_ERR_UNSUPPORTED
 
 
 def test_argument_checks_return_status_without_touching_a_gpu():

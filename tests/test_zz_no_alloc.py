@@ -82,3 +82,10 @@ def test_static_scratch_rejects_problems_beyond_its_limit():
     rc = _lib.load().phb_solver_group_static(ctypes.byref(desc), ctypes.byref(st), gt[0].data_ptr(), 4,
                                              torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.PHB_ERR_SCRATCH_LIMIT
+    # a partial (data-parallel) share would be left where the caller cannot sum it: refused
+    desc = _lib.PhbEngine.from_buffer_copy(eng.desc)
+    st.flags = _lib.PHB_FLAG_PARTIAL | _lib.PHB_FLAG_UPDATE_OBJECT
+    st.b_begin, st.b_end = 0, 2
+    rc = _lib.load().phb_solver_group_static(ctypes.byref(desc), ctypes.byref(st), gt[0].data_ptr(), 4,
+                                             torch.cuda.current_stream().cuda_stream)
+    assert rc == _lib.PHB_ERR_UNSUPPORTED
