@@ -26,7 +26,7 @@ extern "C" {
 /* ------------------------------------------------------------------ status */
 #define PHB_OK                 0
 #define PHB_ERR_INVALID_ARG    1   /* null pointer, bad size, misaligned workspace */
-#define PHB_ERR_UNSUPPORTED    2   /* shape the kernels do not implement (e.g. N not 64/128) */
+#define PHB_ERR_UNSUPPORTED    2   /* shape the kernels do not implement (e.g. N not 64/128/256) */
 #define PHB_ERR_CUDA           3   /* a CUDA launch or runtime call failed */
 #define PHB_ERR_NONFINITE      4   /* NaN/inf found in the object or probe */
 #define PHB_ERR_OUTSIDE        5   /* probe positions completely outside the object */
@@ -81,7 +81,7 @@ int phb_cutout_set_c64(void *obj, int64_t S, int64_t H, int64_t W,
  * Batched 2D FFT with phaser's convention: centred real space, orthonormal.
  * inverse == 0: out = fft2(in)  = fft2(ifftshift(in)) / N   (phaser/utils/num.py:460-468)
  * inverse == 1: out = ifft2(in) = fftshift(ifft2(in)) / N   (phaser/utils/num.py:434-442)
- * N in {64, 128}; `in` and `out` may alias. */
+ * N in {64, 128, 256}; `in` and `out` may alias. */
 int phb_fft2_c64(const void *in, void *out, int64_t batch, int64_t N, int inverse, void *stream);
 
 /* ------------------------------------------------------------- constraints (a17)
@@ -120,7 +120,7 @@ int phb_fourier_mask_c64(void *arr, int64_t batch, int64_t N, const float *mask,
 
 typedef struct phb_engine {
     /* sizes */
-    int32_t N;            /* probe / detector side: 64 or 128 */
+    int32_t N;            /* probe / detector side: 64, 128 or 256 (256: no ePIE) */
     int32_t M;            /* incoherent probe modes, 1..8 */
     int32_t S;            /* object slices */
     int32_t B_max;        /* largest group the workspace was sized for */

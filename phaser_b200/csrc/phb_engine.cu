@@ -20,7 +20,14 @@
 //    (the reference applies them slice by slice, but its cutouts are copies
 //    taken before the backward pass, so deferring is exact);
 //  * step-size numerators / denominators and the position-gradient sums are
-//    accumulated in float64 (block reduce, then one float64 atomic per CTA).
+//    accumulated in float64 (block reduce, then one float64 atomic per CTA);
+//  * N = 256: a tile needs four SMs (512 KB of complex64), so a cluster of 4 CTAs
+//    holds one (position, mode), one quadrant / polyphase component each (the
+//    4-CTA transform of phb_fft.cuh).  The modes of a position are then in
+//    different clusters, so the far field is split over two launches: the forward
+//    launch stores Psi_m = fft2(exit wave) and adds |Psi_m|^2 into a per-position
+//    intensity buffer; the second launch resumes at the detector with the summed
+//    intensity and runs the constraint and the adjoint.
 #include <cooperative_groups.h>
 
 #include "phb_fft.cuh"
@@ -70,11 +77,13 @@ struct Workspace {
     int32_t *info;      // [0] pattern mask is all ones, [1] propagators separable, [2] max deviation (float bits)
     double *sums;       // float64 accumulators, see SumIdx
     double *coef;       // S + M step coefficients
+    float2 *far;        // N = 256 only: B_max * M * N*N far-field waves Psi_m / N (register order)
+    float *far_int;     // N = 256 only: B_max * N*N far-field intensity sum_m |Psi_m / N|^2 (register order)
     size_t bytes;
 };
 
 struct SumIdx {
-    int64_t numO, denO, numP, denP, pnum, pden, pnorm, loss, tilt, total;
+    int64_t numO, denO, numP, denP, pnum, pden, pnorm, loss, tilt, err, total;
     __host__ __device__ SumIdx(int B, int S, int M) {
         numO = 0;
         denO = numO + (int64_t)B * S;
@@ -85,7 +94,8 @@ struct SumIdx {
         pnorm = pden + 2 * (int64_t)B;
         loss = pnorm + B;
         tilt = loss + B;
-        total = tilt + 2 * (int64_t)B;
+        err = tilt + 2 * (int64_t)B;      // N = 256: per-position squared detector error
+        total = err + B;
     }
 };
 
@@ -113,6 +123,10 @@ static Workspace carve(void *base, int N, int M, int S, int B, int64_t H, int64_
     w.info = (int32_t *)take(4 * sizeof(int32_t));
     w.sums = (double *)take((size_t)SumIdx(B, S, M).total * sizeof(double));
     w.coef = (double *)take((size_t)(S + M + 4) * sizeof(double));
+    if (N == 256) {
+        w.far = (float2 *)take((size_t)B * M * NN * sizeof(float2));
+        w.far_int = (float *)take((size_t)B * NN * sizeof(float));
+    }
     w.bytes = off;
     return w;
 }
@@ -134,7 +148,7 @@ struct GroupArgs {
     int32_t *status;       // optional sticky status of the step (see phb_step.status)
     int32_t group_index;
     // float64 accumulator offsets (SumIdx for B_max), precomputed on the host
-    int64_t o_numO, o_denO, o_numP, o_denP, o_pnum, o_pden, o_pnorm, o_loss, o_tilt;
+    int64_t o_numO, o_denO, o_numP, o_denP, o_pnum, o_pden, o_pnorm, o_loss, o_tilt, o_err;
     const float *fy, *fx;
     float2 *psi, *acc_obj, *acc_probe;
     float *illum;
@@ -144,6 +158,9 @@ struct GroupArgs {
     float *sim_out;
     const float *group_patterns;
     const uint16_t *patterns16;   // resident uint16 counts (patterns == nullptr then)
+    float2 *far;                  // N = 256: far-field waves (see Workspace)
+    float *far_int;               // N = 256: far-field intensity
+    int resume;                   // N = 256: 0 = forward launch, 1 = launch resumed at the detector
 };
 
 // One position's measured pattern: host-streamed float32 rows (group_patterns),
@@ -232,17 +249,20 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     constexpr int MR = MC > 0 ? MC : 8;   // capacity of the remote-pointer arrays
     constexpr bool presolve = mode >= MODE_PRE_LSQML;
     constexpr bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
+    constexpr bool QUAD = N == 256;   // 4 CTAs per (position, mode); far field over two launches
+    static_assert(!QUAD || (mode != MODE_EPIE && mode != MODE_PRE_EPIE), "ePIE needs the modes in one cluster");
     cg::cluster_group cl = cg::this_cluster();
     const int M = MC > 0 ? MC : a.M;
     const int S = a.S;
-    const int m = (int)cl.block_rank();
-    const int b = blockIdx.x / M;
+    const int m = QUAD ? (int)((blockIdx.x >> 2) % M) : (int)cl.block_rank();
+    const int b = QUAD ? (int)((blockIdx.x >> 2) / M) : (int)(blockIdx.x / M);
     const int tid = threadIdx.x;
+    const bool resume = QUAD && a.resume;
 
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
     float2 *twid = xb + Lay<N>::BUF;
-    float2 *hy = twid + N, *hx = hy + N;           // sub-pixel shift filter factors
+    float2 *hy = twid + TileCfg<N>::TW, *hx = hy + N;   // sub-pixel shift filter factors
     float2 *py = hx + N, *px = py + N;             // propagator factors of the current slice gap
     double *dred = reinterpret_cast<double *>(px + N);
     float *fred = reinterpret_cast<float *>(dred + 64);              // [0..31] block scratch, [32] cluster slot
@@ -344,9 +364,19 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             }
     };
 
-    load_probe_spectrum(-1);
     int phase = PH_START, s = 0, dir = 0;
     bool fwd = false;
+    if (resume) {
+        // second launch at N = 256: the far-field wave stored by the forward launch
+        const float2 *src = a.far + (size_t)(b * M + m) * NN;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[u][e] = src[I::flat(u, e)];
+        phase = PH_FAR;
+    } else {
+        load_probe_spectrum(-1);
+    }
 
     // The program is 4 S + 2 transforms at most (forward, adjoint, probe, two
     // position directions); the bound turns a logic error into a recorded error
@@ -361,8 +391,10 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             }
             return;
         }
-        if (fwd) fft2_r2k<N>(v, xb, twid);
-        else ifft2_k2r<N>(v, xb, twid);
+        if (!(resume && step == 0)) {
+            if (fwd) fft2_r2k<N>(v, xb, twid);
+            else ifft2_k2r<N>(v, xb, twid);
+        }
         PHB_T_MARK(fwd ? 0 : 1);
         const int timed_phase = phase;
 
@@ -425,7 +457,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
                     if (m == 0) {
                         const PatRow pat(a, pos, b, NN);
-                        for (int f = tid; f < NN; f += FFT_THREADS) {
+                        const int f0 = QUAD ? (cluster_rank() << 14) : 0, f1 = QUAD ? f0 + NN / 4 : NN;
+                        for (int f = f0 + tid; f < f1; f += FFT_THREADS) {
                             int ky, kx;
                             flat_to_k<N>(f, ky, kx);
                             t[1] += (double)(pat.at(ky * N + kx) * __ldg(a.mask_k + f));
@@ -452,7 +485,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         for (int q = 0; q < E; ++q) t[0] += (double)cabs2(v[u][q]);
                     if (m == 0) {
                         const PatRow pat(a, pos, b, NN);
-                        for (int f = tid; f < NN; f += FFT_THREADS) t[1] += (double)pat.at(f);
+                        const int f0 = QUAD ? (cluster_rank() << 14) : 0, f1 = QUAD ? f0 + NN / 4 : NN;
+                        for (int f = f0 + tid; f < f1; f += FFT_THREADS) t[1] += (double)pat.at(f);
                     }
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
                     if (tid == 0) {
@@ -483,19 +517,41 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
         } else if (phase == PH_FAR) {
             // ------------------------------------------- detector: Psi = fft2(exit), constraint
             float *xf = reinterpret_cast<float *>(xb);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    v[u][e] = cscale(v[u][e], inv_n);
-                    xf[I::flat(u, e)] = cabs2(v[u][e]);
-                }
-            cl.sync();
-            // the exchange buffer of every CTA of the cluster (distributed shared memory)
             const float *rxf[MR];
+            if constexpr (QUAD) {
+                if (!resume) {
+                    // the forward launch ends at the detector: store Psi_m / N and add |Psi_m / N|^2
+                    // into the position's intensity (or, simulating, into the output pattern)
+                    float2 *dst = a.far + (size_t)(b * M + m) * NN;
+                    float *itn = a.far_int + (size_t)b * NN;
 #pragma unroll
-            for (int r = 0; r < MR; ++r) rxf[r] = r < M ? cl.map_shared_rank(xf, r) : xf;
-            if constexpr (mode == MODE_SIM) {
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int e = 0; e < E; ++e) {
+                            const float2 w = cscale(v[u][e], inv_n);
+                            if constexpr (mode == MODE_SIM) {
+                                atomicAdd(a.sim_out + (size_t)b * NN + I::ky(u, e) * N + I::kx(u, e), cabs2(w));
+                            } else {
+                                dst[I::flat(u, e)] = w;
+                                atomicAdd(itn + I::flat(u, e), cabs2(w));
+                            }
+                        }
+                    return;
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        v[u][e] = cscale(v[u][e], inv_n);
+                        xf[I::flat(u, e)] = cabs2(v[u][e]);
+                    }
+                cl.sync();
+                // the exchange buffer of every CTA of the cluster (distributed shared memory)
+#pragma unroll
+                for (int r = 0; r < MR; ++r) rxf[r] = r < M ? cl.map_shared_rank(xf, r) : xf;
+            }
+            if constexpr (mode == MODE_SIM && !QUAD) {
                 if (m == 0) {
 #pragma unroll
                     for (int u = 0; u < U; ++u)
@@ -519,8 +575,12 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     for (int e = 0; e < E; ++e) {
                         const int f = I::flat(u, e);
                         float inten = 0.f;
-                        for (int r = 0; r < MR; ++r)
+                        if constexpr (QUAD) {
+                            inten = __ldg(a.far_int + (size_t)b * NN + f);
+                        } else {
+                            for (int r = 0; r < MR; ++r)
                                 if (r < M) inten += rxf[r][f];
+                        }
                         const float pv = pat.at(I::ky(u, e) * N + I::kx(u, e));
                         const float mk = mask_ones ? 1.0f : __ldg(a.mask_k + f);
                         if (calc_err && m == 0) {
@@ -549,13 +609,18 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         }
                         v[u][e] = cscale(v[u][e], fac);
                     }
-                cl.sync();
+                if constexpr (!QUAD) cl.sync();
                 if (m == 0 && (calc_err || grad)) {
                     double t[2] = {e2, loss};
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
                     if (tid == 0) {
-                        if (calc_err) a.errors[pos] = (float)sqrt(t[0]);
-                        if (grad) sums[a.o_loss + b] = t[1];
+                        if constexpr (QUAD) {   // four quadrant CTAs: the finish kernel takes the root
+                            if (calc_err) atomicAdd(sums + a.o_err + b, t[0]);
+                            if (grad) atomicAdd(sums + a.o_loss + b, t[1]);
+                        } else {
+                            if (calc_err) a.errors[pos] = (float)sqrt(t[0]);
+                            if (grad) sums[a.o_loss + b] = t[1];
+                        }
                     }
                 }
                 fwd = false;
@@ -695,7 +760,13 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             if (s > 0) {
                 // the adjoint of slice s-1 reads its stored incident wave after the next
                 // transform pair: start moving it from HBM into L2 now
-                if (upd_obj && tid == 0) prefetch_l2(psi_b + (size_t)(s - 1) * NN, NN * sizeof(float2));
+                if (upd_obj && tid == 0) {
+                    if constexpr (QUAD)
+                        prefetch_l2(psi_b + (size_t)(s - 1) * NN + ((size_t)cluster_rank() << 14),
+                                    (NN / 4) * sizeof(float2));
+                    else
+                        prefetch_l2(psi_b + (size_t)(s - 1) * NN, NN * sizeof(float2));
+                }
                 load_prop(s - 1);
                 fwd = true;
                 phase = PH_BPROP;
@@ -853,6 +924,7 @@ struct FinArgs {
     double *group_loss;
     float *grad_tilt;
     float grad_tilt_scale;
+    float *errors;   // N = 256: per-position errors, the root of the summed squares in `sums`
 };
 
 __global__ void k_finalize(const FinArgs f) {
@@ -923,6 +995,8 @@ __global__ void k_finalize(const FinArgs f) {
             if ((tid & 31) == 0) atomicAdd(f.group_loss, lsum);
         }
     }
+    if (f.errors && (f.flags & PHB_FLAG_CALC_ERROR) && f.mode != MODE_GRAD)
+        for (int b = tid; b < f.B; b += blockDim.x) f.errors[f.group[b]] = (float)sqrt(sums[SI.err + b]);
     __syncthreads();
     for (int64_t i = tid; i < SI.total; i += blockDim.x) sums[i] = 0.0;
 }
@@ -990,14 +1064,14 @@ struct ProbeApplyArgs {
 template <int N>
 __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApplyArgs a) {
     using I = Idx<N>;
-    constexpr int U = I::U, E = I::E, NN = N * N;
+    constexpr int U = I::U, E = I::E, NN = N * N, CTAS = TileCfg<N>::CTAS;
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
     float2 *twid = xb + Lay<N>::BUF;
-    float *fred = reinterpret_cast<float *>(twid + N);
+    float *fred = reinterpret_cast<float *>(twid + TileCfg<N>::TW);
     fft_init_twiddles<N>(twid);
     __syncthreads();
-    const int m = blockIdx.x;
+    const int m = blockIdx.x / CTAS;   // one CTA (N = 256: one 4-CTA cluster) per mode
     float2 *P = a.probe + (size_t)m * NN;
     float2 v[U][E];
     bool bad = false;
@@ -1035,7 +1109,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
             }
         __syncthreads();
     }
-    if (m == 0 && a.new_obj_mag && a.gom)
+    if (m == 0 && a.new_obj_mag && a.gom && (CTAS == 1 || cluster_rank() == 0))
         for (int i = threadIdx.x; i < NN; i += blockDim.x) a.new_obj_mag[i] += a.gom[i];
     if (a.mode == MODE_GRAD) return;
     // refresh spectrum
@@ -1108,21 +1182,12 @@ __global__ void __launch_bounds__(1024) k_prop_init(const float2 *props, int G, 
 
 // ---------------------------------------------------------------- K-order packing
 template <int N>
-__global__ void k_pack_c64(const float2 *src, float2 *dst) {
-    using I = Idx<N>;
-    const size_t base = (size_t)blockIdx.x * N * N;
-#pragma unroll
-    for (int u = 0; u < I::U; ++u)
-#pragma unroll
-        for (int e = 0; e < I::E; ++e) dst[base + I::flat(u, e)] = src[base + I::ky(u, e) * N + I::kx(u, e)];
-}
-template <int N>
 __global__ void k_pack_f32(const float *src, float *dst) {
-    using I = Idx<N>;
-#pragma unroll
-    for (int u = 0; u < I::U; ++u)
-#pragma unroll
-        for (int e = 0; e < I::E; ++e) dst[I::flat(u, e)] = src[I::ky(u, e) * N + I::kx(u, e)];
+    for (int f = threadIdx.x; f < N * N; f += blockDim.x) {
+        int ky, kx;
+        flat_to_k<N>(f, ky, kx);
+        dst[f] = src[ky * N + kx];
+    }
 }
 
 // ---------------------------------------------------------------- per-iteration helpers
@@ -1251,13 +1316,20 @@ __global__ void k_check_finite(const float2 *v, int64_t n, int32_t *status, int3
 // ---------------------------------------------------------------- host glue
 template <int N>
 static size_t group_smem_bytes() {
-    return (size_t)Lay<N>::BUF * sizeof(float2) + 5 * N * sizeof(float2) + 64 * sizeof(double) + 64 * sizeof(float) +
+    return (size_t)Lay<N>::BUF * sizeof(float2) + (TileCfg<N>::TW + 4 * N) * sizeof(float2) + 64 * sizeof(double) +
+           64 * sizeof(float) +
            (size_t)N * N / 32 * sizeof(uint32_t) + 2 * FFT_THREADS * sizeof(uint64_t) +
            (size_t)FFTCfg<N>::U * FFT_THREADS * sizeof(int32_t);
 }
 template <int N>
 static size_t fft_smem_bytes() {
-    return (size_t)Lay<N>::BUF * sizeof(float2) + N * sizeof(float2) + 64 * sizeof(float);
+    return (size_t)Lay<N>::BUF * sizeof(float2) + TileCfg<N>::TW * sizeof(float2) + 64 * sizeof(float);
+}
+
+template <int N>
+static int launch_probe_apply(const ProbeApplyArgs &p, cudaStream_t st) {
+    constexpr unsigned C = TileCfg<N>::CTAS;
+    return launch_clustered(k_probe_apply<N>, (unsigned)p.M * C, FFT_THREADS, C, fft_smem_bytes<N>(), st, p);
 }
 
 template <int N>
@@ -1274,7 +1346,7 @@ static int configure_kernels() {
 
 static int validate(const phb_engine *e) {
     if (!e) return PHB_ERR_INVALID_ARG;
-    if (e->N != 64 && e->N != 128) return PHB_ERR_UNSUPPORTED;
+    if (e->N != 64 && e->N != 128 && e->N != 256) return PHB_ERR_UNSUPPORTED;
     if (e->M < 1 || e->M > 8) return PHB_ERR_UNSUPPORTED;
     if (e->S < 1 || e->B_max < 1 || e->H < 1 || e->W < 1 || e->n_pos < 1) return PHB_ERR_INVALID_ARG;
     if (!e->object || !e->probe || !e->scan || !e->patterns || !e->pattern_mask || !e->ky || !e->kx)
@@ -1331,6 +1403,9 @@ static GroupArgs make_args(const phb_engine *e, const Workspace &w, int mode, in
     a.o_pnorm = SI.pnorm;
     a.o_loss = SI.loss;
     a.o_tilt = SI.tilt;
+    a.o_err = SI.err;
+    a.far = w.far;
+    a.far_int = w.far_int;
     a.probe_k = w.probe_k;
     a.fy = e->ky;
     a.fx = e->kx;
@@ -1351,21 +1426,12 @@ static int launch_group_mode(const GroupArgs &a, cudaStream_t st) {
             return record_cuda(cudaGetLastError());
         configured = true;
     }
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)(a.B * a.M), 1, 1);
-    cfg.blockDim = dim3(FFT_THREADS, 1, 1);
-    cfg.dynamicSmemBytes = group_smem_bytes<N>();
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)a.M;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const int rc = record_cuda(cudaLaunchKernelEx(&cfg, k_group<N, MODE, MC>, a));
-    if (rc == PHB_OK) count_launch();
-    return rc;
+    // N <= 128: one cluster of M CTAs (the modes) per position; N = 256: one cluster of
+    // 4 CTAs (the quadrants) per (position, mode)
+    constexpr unsigned C = TileCfg<N>::CTAS;
+    const unsigned cluster = C > 1 ? C : (unsigned)a.M;
+    return launch_clustered(k_group<N, MODE, MC>, (unsigned)(a.B * a.M) * C, FFT_THREADS, cluster, group_smem_bytes<N>(),
+                            st, a);
 }
 
 template <int N, int MODE>
@@ -1381,15 +1447,49 @@ static int launch_group_m(const GroupArgs &a, cudaStream_t st) {
 
 template <int N>
 static int launch_group(const GroupArgs &a, cudaStream_t st) {
-    switch (a.mode) {
-        case MODE_LSQML: return launch_group_m<N, MODE_LSQML>(a, st);
-        case MODE_EPIE: return launch_group_m<N, MODE_EPIE>(a, st);
-        case MODE_GRAD: return launch_group_m<N, MODE_GRAD>(a, st);
-        case MODE_PRE_LSQML: return launch_group_mode<N, MODE_PRE_LSQML, 0>(a, st);
-        case MODE_PRE_EPIE: return launch_group_mode<N, MODE_PRE_EPIE, 0>(a, st);
-        case MODE_PRE_GRAD: return launch_group_mode<N, MODE_PRE_GRAD, 0>(a, st);
-        case MODE_SIM: return launch_group_m<N, MODE_SIM>(a, st);
-        default: return PHB_ERR_INVALID_ARG;
+    if constexpr (N == 256) {   // modes run in separate clusters: no per-mode template, no ePIE
+        switch (a.mode) {
+            case MODE_LSQML: return launch_group_mode<N, MODE_LSQML, 0>(a, st);
+            case MODE_GRAD: return launch_group_mode<N, MODE_GRAD, 0>(a, st);
+            case MODE_PRE_LSQML: return launch_group_mode<N, MODE_PRE_LSQML, 0>(a, st);
+            case MODE_PRE_GRAD: return launch_group_mode<N, MODE_PRE_GRAD, 0>(a, st);
+            case MODE_SIM: return launch_group_mode<N, MODE_SIM, 0>(a, st);
+            case MODE_EPIE:
+            case MODE_PRE_EPIE: return PHB_ERR_UNSUPPORTED;
+            default: return PHB_ERR_INVALID_ARG;
+        }
+    } else {
+        switch (a.mode) {
+            case MODE_LSQML: return launch_group_m<N, MODE_LSQML>(a, st);
+            case MODE_EPIE: return launch_group_m<N, MODE_EPIE>(a, st);
+            case MODE_GRAD: return launch_group_m<N, MODE_GRAD>(a, st);
+            case MODE_PRE_LSQML: return launch_group_mode<N, MODE_PRE_LSQML, 0>(a, st);
+            case MODE_PRE_EPIE: return launch_group_mode<N, MODE_PRE_EPIE, 0>(a, st);
+            case MODE_PRE_GRAD: return launch_group_mode<N, MODE_PRE_GRAD, 0>(a, st);
+            case MODE_SIM: return launch_group_m<N, MODE_SIM>(a, st);
+            default: return PHB_ERR_INVALID_ARG;
+        }
+    }
+}
+
+// the fused step of one group: one launch, or at N = 256 the forward launch, which
+// leaves the far-field waves and the summed intensity in the workspace, and the
+// launch resumed at the detector
+template <int N>
+static int launch_step(GroupArgs a, const Workspace &w, cudaStream_t st) {
+    if constexpr (N == 256) {
+        const bool split = a.mode == MODE_LSQML || a.mode == MODE_GRAD;
+        if (split) {
+            const int rc = record_cuda(cudaMemsetAsync(w.far_int, 0, (size_t)a.B * N * N * sizeof(float), st));
+            if (rc) return rc;
+        }
+        a.resume = 0;
+        int rc = launch_group<N>(a, st);
+        if (rc || !split) return rc;
+        a.resume = 1;
+        return launch_group<N>(a, st);
+    } else {
+        return launch_group<N>(a, st);
     }
 }
 
@@ -1401,8 +1501,7 @@ static int probe_spectrum(const phb_engine *e, const Workspace &w, cudaStream_t 
     p.probe = (float2 *)e->probe;
     p.probe_k = w.probe_k;
     p.update = 0;
-    k_probe_apply<N><<<e->M, FFT_THREADS, fft_smem_bytes<N>(), st>>>(p);
-    return check_launch();
+    return launch_probe_apply<N>(p, st);
 }
 
 template <int N>
@@ -1421,7 +1520,7 @@ static int engine_init(const phb_engine *e, cudaStream_t st) {
     k_prop_init<N><<<1, 1024, 0, st>>>((const float2 *)e->propagators, e->S - 1, e->pattern_mask, w.prop1d, w.band,
                                         w.info);
     if ((rc = check_launch())) return rc;
-    k_pack_f32<N><<<1, FFT_THREADS, 0, st>>>(e->pattern_mask, w.mask_k);
+    k_pack_f32<N><<<1, 1024, 0, st>>>(e->pattern_mask, w.mask_k);
     if ((rc = check_launch())) return rc;
     if ((rc = probe_spectrum<N>(e, w, st))) return rc;
     // the propagator check is the only result the host needs from init
@@ -1458,6 +1557,9 @@ static int simulate(const phb_engine *e, const int64_t *group, int B, float *out
     GroupArgs a = make_args(e, w, MODE_SIM, 0, group, B);
     a.illum = nullptr;
     a.sim_out = out;
+    if (N == 256) {   // the quadrant clusters add their modes' intensities into the output
+        if ((rc = record_cuda(cudaMemsetAsync(out, 0, (size_t)B * N * N * sizeof(float), st)))) return rc;
+    }
     return launch_group<N>(a, st);
 }
 
@@ -1485,6 +1587,7 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
         a.o_pnorm += b0;
         a.o_loss += b0;
         a.o_tilt += 2 * (int64_t)b0;
+        a.o_err += b0;
     }
     a.errors = sp->errors;
     a.beta_object = sp->beta_object;
@@ -1503,7 +1606,7 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
     a.status = sp->status;
     a.group_index = sp->group_index;
     if (sp->event_begin && (rc = record_cuda(cudaEventRecord((cudaEvent_t)sp->event_begin, st)))) return rc;
-    if ((rc = launch_group<N>(a, st))) return rc;
+    if ((rc = launch_step<N>(a, w, st))) return rc;
     if (sp->event_end && (rc = record_cuda(cudaEventRecord((cudaEvent_t)sp->event_end, st)))) return rc;
     if (partial) return PHB_OK;
     return solver_finish<N>(e, sp, group, B, st);
@@ -1541,6 +1644,7 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
     f.group_loss = sp->group_loss;
     f.grad_tilt = sp->grad_tilt;
     f.grad_tilt_scale = sp->grad_tilt_scale;
+    f.errors = N == 256 ? sp->errors : nullptr;   // quadrant launches leave squared sums
     k_finalize<<<1, 256, 0, st>>>(f);
     if ((rc = check_launch())) return rc;
 
@@ -1585,8 +1689,7 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
         p.group_index = sp->group_index;
         p.update = upd_probe;
         if (mode == MODE_GRAD && !sp->grad_probe) p.update = 0;
-        k_probe_apply<N><<<e->M, FFT_THREADS, fft_smem_bytes<N>(), st>>>(p);
-        if ((rc = check_launch())) return rc;
+        if ((rc = launch_probe_apply<N>(p, st))) return rc;
     }
     return PHB_OK;
 }
@@ -1613,22 +1716,23 @@ size_t phb_engine_workspace_bytes(int32_t N, int32_t M, int32_t S, int32_t B_max
     return carve(nullptr, N, M, S, B_max, H, W).bytes;
 }
 
+// call F<N>(args...) for the engine's probe size
+#define PHB_DISPATCH_N(n, F, ...) \
+    ((n) == 256 ? F<256>(__VA_ARGS__) : (n) == 128 ? F<128>(__VA_ARGS__) : F<64>(__VA_ARGS__))
+
 int phb_engine_init(const phb_engine *e, void *stream) {
     int rc = validate(e);
     if (rc) return rc;
-    return e->N == 128 ? engine_init<128>(e, (cudaStream_t)stream) : engine_init<64>(e, (cudaStream_t)stream);
+    return PHB_DISPATCH_N(e->N, engine_init, e, (cudaStream_t)stream);
 }
 
 int phb_engine_probe_changed(const phb_engine *e, void *stream) {
     int rc = validate(e);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    if (e->N == 128) {
-        if ((rc = configure_kernels<128>())) return rc;
-        return probe_spectrum<128>(e, carve(e->workspace, 128, e->M, e->S, e->B_max, e->H, e->W), st);
-    }
-    if ((rc = configure_kernels<64>())) return rc;
-    return probe_spectrum<64>(e, carve(e->workspace, 64, e->M, e->S, e->B_max, e->H, e->W), st);
+    if ((rc = PHB_DISPATCH_N(e->N, configure_kernels))) return rc;
+    const Workspace w = carve(e->workspace, e->N, e->M, e->S, e->B_max, e->H, e->W);
+    return PHB_DISPATCH_N(e->N, probe_spectrum, e, w, st);
 }
 
 int phb_presolve_group(const phb_engine *e, const int64_t *group, int32_t B, int32_t solver, int32_t gradient_form,
@@ -1636,9 +1740,9 @@ int phb_presolve_group(const phb_engine *e, const int64_t *group, int32_t B, int
     int rc = validate(e);
     if (rc) return rc;
     if (!group || !rescale_num || !rescale_den || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
+    if (e->N == 256 && solver == PHB_SOLVER_EPIE && !gradient_form) return PHB_ERR_UNSUPPORTED;
     cudaStream_t st = (cudaStream_t)stream;
-    return e->N == 128 ? presolve<128>(e, group, B, solver, gradient_form, rescale_num, rescale_den, st)
-                       : presolve<64>(e, group, B, solver, gradient_form, rescale_num, rescale_den, st);
+    return PHB_DISPATCH_N(e->N, presolve, e, group, B, solver, gradient_form, rescale_num, rescale_den, st);
 }
 
 int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, float *intensity, void *stream) {
@@ -1646,7 +1750,7 @@ int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, flo
     if (rc) return rc;
     if (!group || !intensity || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    return e->N == 128 ? simulate<128>(e, group, B, intensity, st) : simulate<64>(e, group, B, intensity, st);
+    return PHB_DISPATCH_N(e->N, simulate, e, group, B, intensity, st);
 }
 
 int phb_solver_group_finish(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B, void *stream) {
@@ -1655,7 +1759,7 @@ int phb_solver_group_finish(const phb_engine *e, const phb_step *st, const int64
     if (!st || !group || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
     if (st->solver < PHB_SOLVER_LSQML || st->solver > PHB_SOLVER_GRAD) return PHB_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    return e->N == 128 ? solver_finish<128>(e, st, group, B, s) : solver_finish<64>(e, st, group, B, s);
+    return PHB_DISPATCH_N(e->N, solver_finish, e, st, group, B, s);
 }
 
 int phb_engine_reduce_layout(int32_t N, int32_t M, int32_t S, int32_t B_max, int64_t H, int64_t W, int64_t *out4) {
@@ -1688,8 +1792,9 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
         return PHB_ERR_INVALID_ARG;
     if ((st->flags & PHB_FLAG_PARTIAL) && (st->b_begin < 0 || st->b_end > B || st->b_begin >= st->b_end))
         return PHB_ERR_INVALID_ARG;
+    if (e->N == 256 && st->solver == PHB_SOLVER_EPIE) return PHB_ERR_UNSUPPORTED;
     cudaStream_t s = (cudaStream_t)stream;
-    return e->N == 128 ? solver_group<128>(e, st, group, B, s) : solver_group<64>(e, st, group, B, s);
+    return PHB_DISPATCH_N(e->N, solver_group, e, st, group, B, s);
 }
 
 int phb_position_update(float *scan, float *pos_update, float *momentum_state, int64_t n_pos, int32_t use_momentum,
@@ -1777,7 +1882,7 @@ extern "C" int phb_solver_group_static(const phb_engine *e, const phb_step *st, 
     cudaStream_t s = (cudaStream_t)stream;
     // the array keeps the previous call's contents: engine_init clears every accumulator and
     // rebuilds the tables (propagator factors, mask, probe spectrum) from this call's inputs
-    rc = ws.N == 128 ? engine_init<128>(&ws, s) : engine_init<64>(&ws, s);
+    rc = PHB_DISPATCH_N(ws.N, engine_init, &ws, s);
     if (rc) return rc;
     return phb_solver_group(&ws, st, group, B, stream);
 }

@@ -23,6 +23,16 @@
 //   (two wavefronts per warp-wide 8-byte access) and every address is a
 //   per-thread base plus a compile-time offset.
 //
+// N = 256 (a cluster of 4 CTAs per tile, each holding one 128 x 128 part):
+//   real space: CTA rank q = 2 a + b holds the quadrant x[128 a + y', 128 b + x'] in the
+//   N = 128 R layout of (y', x');  Fourier space: it holds the polyphase component
+//   X[2 ky' + a, 2 kx' + b] in the N = 128 K layout of (ky', kx').  The forward transform
+//   is one radix-2 x 2 decimation-in-frequency stage across the cluster -- each CTA
+//   publishes its quadrant in shared memory, combines the four quadrants at its own
+//   register slots through distributed shared memory (signs (-1)^(ac + bd)) and applies
+//   the twiddle W256^(c y' + d x') -- followed by the CTA's own 128 x 128 transform; the
+//   inverse runs the same steps in reverse order with conjugate twiddles.
+//
 // N = 64 (8 values per thread, three exchanges): a line FFT of length
 // N = E * NT runs as a radix-E DFT in registers (elements strided by NT) ->
 // twiddle -> exchange among the NT threads of the line -> radix-NT DFTs:
@@ -30,9 +40,18 @@
 //   K layout: v[u][p NT + k2] = X[ky = (t%8) P + p + E k2][kx = t/8 + RPP u]
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "phb_common.cuh"
 
 namespace phb {
+
+// rank of this CTA in its thread-block cluster
+__device__ __forceinline__ int cluster_rank() {
+    unsigned r;
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return (int)r;
+}
 
 #ifndef PHB_FFT_THREADS
 #define PHB_FFT_THREADS 512
@@ -41,7 +60,12 @@ constexpr int FFT_THREADS = PHB_FFT_THREADS;  // threads per tile (256: 4 lines 
 constexpr int RPP = FFT_THREADS / 8;          // rows (lines) handled per pass: 8 threads per line
 
 template <int N> struct FFTCfg;
+template <> struct FFTCfg<256> { static constexpr int E = 32, U = 1; };   // per CTA of the 4-CTA cluster
 template <> struct FFTCfg<128> { static constexpr int E = 32, U = 1; };
+
+// CTAs per tile (thread-block cluster of the transform) and twiddle-table entries
+template <int N> struct TileCfg { static constexpr int CTAS = 1, TW = N; };
+template <> struct TileCfg<256> { static constexpr int CTAS = 4, TW = 128 + 256; };
 template <> struct FFTCfg<64>  { static constexpr int E = 8,  NT = 8, P = 1, U = 64 / RPP; };
 
 // ----------------------------------------------------------------- small DFTs
@@ -188,6 +212,11 @@ struct Lay<128> {
     static constexpr int S1 = 33, S2 = 17;   // row strides of exchanges 1 and 2
     static constexpr int BUF = 1024 * S2;    // complex elements of the exchange buffer (>= 512 * S1)
 };
+template <>
+struct Lay<256> {
+    static constexpr int BUF = Lay<128>::BUF;   // the 128 x 128 part's exchanges; also holds the
+                                                // 16384 values a CTA publishes to its cluster
+};
 
 template <int N>
 struct Lay {
@@ -201,16 +230,25 @@ struct Lay {
     }
 };
 
-// twiddle table, N entries: N = 128: twid[j] = exp(-2 pi i j / 128);
-// N = 64: twid[k1 * NT + jj] = exp(-2 pi i jj k1 / 64)
+// twiddle table, TileCfg<N>::TW entries: N = 128: twid[j] = exp(-2 pi i j / 128);
+// N = 64: twid[k1 * NT + jj] = exp(-2 pi i jj k1 / 64);
+// N = 256: the N = 128 table, then twid[128 + j] = exp(-2 pi i j / 256)
 template <int N>
 __device__ __forceinline__ void fft_init_twiddles(float2 *twid) {
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        int e;
-        if constexpr (N == 128) e = i;
-        else e = (i % FFTCfg<N>::NT) * (i / FFTCfg<N>::NT);
+    for (int i = threadIdx.x; i < TileCfg<N>::TW; i += blockDim.x) {
+        int e, n;
+        if constexpr (N == 256) {
+            e = i < 128 ? i : i - 128;
+            n = i < 128 ? 128 : 256;
+        } else if constexpr (N == 128) {
+            e = i;
+            n = 128;
+        } else {
+            e = (i % FFTCfg<N>::NT) * (i / FFTCfg<N>::NT);
+            n = N;
+        }
         float s, c;
-        sincospif(-2.0f * (float)e / (float)N, &s, &c);
+        sincospif(-2.0f * (float)e / (float)n, &s, &c);
         twid[i] = make_float2(c, s);
     }
 }
@@ -327,6 +365,73 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
 #pragma unroll
         for (int m = 0; m < 8; ++m) dft4<true>(x[m], x[8 + m], x[16 + m], x[24 + m]);    // k1 -> j
     }
+}
+
+// ------------------------------------------------- N = 256: 4-CTA cluster form
+// Radix-2 x 2 stage across the cluster at every register slot: this CTA (rank
+// 2 c + d) gets sum over ranks 2 a + b of (-1)^(a c + b d) x_ab.  Both sides of
+// both cluster barriers: the first publishes every CTA's values, the second keeps
+// each CTA's buffer intact until all remote reads of it are done.
+__device__ __forceinline__ void quad_butterfly(float2 (&v)[1][32], float2 *xb) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int t = threadIdx.x;
+    float2 *x = v[0];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) xb[i * 512 + t] = x[i];
+    cl.sync();
+    const int q = cluster_rank() & 3;
+    const float sy = (q & 2) ? -1.f : 1.f, sx = (q & 1) ? -1.f : 1.f;
+    const float2 *r0 = cl.map_shared_rank(xb, 0) + t, *r1 = cl.map_shared_rank(xb, 1) + t;
+    const float2 *r2 = cl.map_shared_rank(xb, 2) + t, *r3 = cl.map_shared_rank(xb, 3) + t;
+#pragma unroll
+    for (int i0 = 0; i0 < 32; i0 += 4) {
+        float2 a[4], b[4], c[4], d[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            a[j] = r0[(i0 + j) * 512];
+            b[j] = r1[(i0 + j) * 512];
+            c[j] = r2[(i0 + j) * 512];
+            d[j] = r3[(i0 + j) * 512];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float2 top = make_float2(fmaf(sx, b[j].x, a[j].x), fmaf(sx, b[j].y, a[j].y));
+            const float2 bot = make_float2(fmaf(sx, d[j].x, c[j].x), fmaf(sx, d[j].y, c[j].y));
+            x[i0 + j] = make_float2(fmaf(sy, bot.x, top.x), fmaf(sy, bot.y, top.y));
+        }
+    }
+    cl.sync();
+}
+
+// multiply slot i (real-space position (y', x') of the N = 128 R layout) by
+// W256^(c y' + d x') (CONJ: its conjugate); c, d = the CTA's rank bits
+template <bool CONJ>
+__device__ __forceinline__ void quad_twiddle(float2 (&v)[1][32], const float2 *tw256) {
+    const int q = cluster_rank() & 3;
+    if (q == 0) return;   // uniform over the CTA
+    const int c = q >> 1, d = q & 1, t = threadIdx.x;
+    const int base = c * (t >> 5) + d * (t & 31);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        const int e = (base + c * 16 * (i & 7) + d * 32 * (i >> 3)) & 255;
+        const float2 w = tw256[e];
+        v[0][i] = CONJ ? cmulc(v[0][i], w) : cmul(v[0][i], w);
+    }
+}
+
+// Forward 256 x 256 (cluster of 4): quadrant in R layout -> polyphase component in K layout.
+__device__ __forceinline__ void fft256_r2k(float2 (&v)[1][32], float2 *xb, const float2 *twid) {
+    quad_butterfly(v, xb);
+    quad_twiddle<false>(v, twid + 128);
+    fft128_r2k(v, xb, twid);
+}
+
+// Inverse (unnormalised): polyphase component in K layout -> quadrant in R layout.
+__device__ __forceinline__ void ifft256_k2r(float2 (&v)[1][32], float2 *xb, const float2 *twid) {
+    fft128_k2r(v, xb, twid);
+    quad_twiddle<true>(v, twid + 128);
+    quad_butterfly(v, xb);
 }
 
 // ----------------------------------------------------------------- line passes
@@ -466,7 +571,9 @@ __device__ __forceinline__ void transpose_kr(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>
 template <int N>
 __device__ __forceinline__ void fft2_r2k(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
                                          const float2 *twid) {
-    if constexpr (N == 128) {
+    if constexpr (N == 256) {
+        fft256_r2k(v, xb, twid);
+    } else if constexpr (N == 128) {
         fft128_r2k(v, xb, twid);
     } else {
         line_pass_fwd<N>(v, xb, twid);
@@ -479,7 +586,9 @@ __device__ __forceinline__ void fft2_r2k(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E]
 template <int N>
 __device__ __forceinline__ void ifft2_k2r(float2 (&v)[FFTCfg<N>::U][FFTCfg<N>::E], float2 *xb,
                                           const float2 *twid) {
-    if constexpr (N == 128) {
+    if constexpr (N == 256) {
+        ifft256_k2r(v, xb, twid);
+    } else if constexpr (N == 128) {
         fft128_k2r(v, xb, twid);
     } else {
         line_pass_inv<N>(v, xb, twid);
@@ -540,17 +649,48 @@ struct Idx<64> {
     }
 };
 
+// N = 256: the CTA of cluster rank q = 2 a + b holds the quadrant (a, b) in real space
+// and the polyphase component (a, b) in Fourier space, each in the N = 128 layouts;
+// register-order flat indices are CTA-major (q * 16384 + the N = 128 flat index).
+template <>
+struct Idx<256> {
+    using B = Idx<128>;
+    static constexpr int U = 1, E = 32;
+    static __device__ __forceinline__ int quad() { return cluster_rank() & 3; }
+    static __device__ __forceinline__ int row(int u, int q) { return B::row(u, q) + ((quad() >> 1) << 7); }
+    static __device__ __forceinline__ int col(int u, int q) { return B::col(u, q) + ((quad() & 1) << 7); }
+    static __host__ __device__ __forceinline__ constexpr int drow(int q) { return B::drow(q); }
+    static __host__ __device__ __forceinline__ constexpr int dcol(int q) { return B::dcol(q); }
+    static __device__ __forceinline__ int kx(int u, int e) { return 2 * B::kx(u, e) + (quad() & 1); }
+    static __device__ __forceinline__ int ky(int u, int e) { return 2 * B::ky(u, e) + (quad() >> 1); }
+    static __device__ __forceinline__ int flat(int u, int e) { return (quad() << 14) + B::flat(u, e); }
+};
+
 // decode a register-order flat index (from any thread) to (row, col) in R layout
 template <int N>
 __device__ __forceinline__ void flat_to_rc(int f, int &r, int &c) {
-    const int t = f % FFT_THREADS, s = f / FFT_THREADS;   // s = u*E + q
-    Idx<N>::rc_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, r, c);
+    if constexpr (N == 256) {
+        const int q = f >> 14;
+        flat_to_rc<128>(f & 16383, r, c);
+        r += (q >> 1) << 7;
+        c += (q & 1) << 7;
+    } else {
+        const int t = f % FFT_THREADS, s = f / FFT_THREADS;   // s = u*E + q
+        Idx<N>::rc_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, r, c);
+    }
 }
 // ... and to (ky, kx) in K layout
 template <int N>
 __device__ __forceinline__ void flat_to_k(int f, int &ky, int &kx) {
-    const int t = f % FFT_THREADS, s = f / FFT_THREADS;
-    Idx<N>::k_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, ky, kx);
+    if constexpr (N == 256) {
+        const int q = f >> 14;
+        flat_to_k<128>(f & 16383, ky, kx);
+        ky = 2 * ky + (q >> 1);
+        kx = 2 * kx + (q & 1);
+    } else {
+        const int t = f % FFT_THREADS, s = f / FFT_THREADS;
+        Idx<N>::k_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, ky, kx);
+    }
 }
 
 }  // namespace phb

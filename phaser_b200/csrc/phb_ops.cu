@@ -77,8 +77,9 @@ __global__ void k_cutout_add_f32(float *obj, int64_t S, int64_t H, int64_t W, co
 }
 
 // --------------------------------------------------------------- batched FFT
-// One CTA per N x N tile.  fft2: out = (-1)^(ky+kx) DFT(in) / N  (== the
-// ifftshift-then-FFT convention for even N); ifft2: out = IDFT((-1)^(ky+kx) in) / N.
+// One CTA per N x N tile (N = 256: one cluster of 4 CTAs).  fft2: out = (-1)^(ky+kx)
+// DFT(in) / N  (== the ifftshift-then-FFT convention for even N); ifft2: out =
+// IDFT((-1)^(ky+kx) in) / N.
 template <int N>
 __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *in, float2 *out, int inverse) {
     using I = Idx<N>;
@@ -87,8 +88,9 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
     float2 *twid = xb + Lay<N>::BUF;
     fft_init_twiddles<N>(twid);
-    const float2 *src = in + (size_t)blockIdx.x * N * N;
-    float2 *dst = out + (size_t)blockIdx.x * N * N;
+    const size_t tile = blockIdx.x / TileCfg<N>::CTAS;
+    const float2 *src = in + tile * N * N;
+    float2 *dst = out + tile * N * N;
     float2 v[U][E];
     const float scale = 1.0f / (float)N;
     if (!inverse) {
@@ -126,16 +128,17 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fft2_centred(const float2 *i
 
 template <int N>
 static int launch_fft2(const float2 *in, float2 *out, int64_t batch, int inverse, cudaStream_t st) {
-    const size_t smem = (size_t)Lay<N>::BUF * sizeof(float2) + N * sizeof(float2);
+    const size_t smem = (size_t)Lay<N>::BUF * sizeof(float2) + TileCfg<N>::TW * sizeof(float2);
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(k_fft2_centred<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return PHB_ERR_CUDA;
         configured = true;
     }
-    // in-place is safe: each CTA reads its whole tile into registers before writing
-    k_fft2_centred<N><<<(unsigned)batch, FFT_THREADS, smem, st>>>(in, out, inverse);
-    return check_launch();
+    // in-place is safe: each CTA reads its part of the tile into registers before the
+    // first exchange, and writes after the last one
+    constexpr unsigned C = TileCfg<N>::CTAS;
+    return launch_clustered(k_fft2_centred<N>, (unsigned)batch * C, FFT_THREADS, C, smem, st, in, out, inverse);
 }
 
 // ------------------------------------------------------------- constraints
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
     float2 *twid = xb + Lay<N>::BUF;
     fft_init_twiddles<N>(twid);
-    float2 *t = a + (size_t)blockIdx.x * N * N;
+    float2 *t = a + (size_t)(blockIdx.x / TileCfg<N>::CTAS) * N * N;
     float2 v[U][E];
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -181,15 +184,15 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_fourier_mask(float2 *a, cons
 
 template <int N>
 static int launch_fourier_mask(float2 *a, const float *mask, int64_t batch, cudaStream_t st) {
-    const size_t smem = (size_t)Lay<N>::BUF * sizeof(float2) + N * sizeof(float2);
+    const size_t smem = (size_t)Lay<N>::BUF * sizeof(float2) + TileCfg<N>::TW * sizeof(float2);
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(k_fourier_mask<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return record_cuda(cudaGetLastError());
         configured = true;
     }
-    k_fourier_mask<N><<<(unsigned)batch, FFT_THREADS, smem, st>>>(a, mask);
-    return check_launch();
+    constexpr unsigned C = TileCfg<N>::CTAS;
+    return launch_clustered(k_fourier_mask<N>, (unsigned)batch * C, FFT_THREADS, C, smem, st, a, mask);
 }
 
 }  // namespace phb
@@ -274,6 +277,8 @@ int phb_fft2_c64(const void *in, void *out, int64_t batch, int64_t N, int invers
     if (batch == 0) return PHB_OK;
     if (batch > 0x7fffffff) return PHB_ERR_INVALID_ARG;
     cudaStream_t st = (cudaStream_t)stream;
+    if (batch > 0x7fffffff / 4) return PHB_ERR_INVALID_ARG;
+    if (N == 256) return launch_fft2<256>((const float2 *)in, (float2 *)out, batch, inverse, st);
     if (N == 128) return launch_fft2<128>((const float2 *)in, (float2 *)out, batch, inverse, st);
     if (N == 64) return launch_fft2<64>((const float2 *)in, (float2 *)out, batch, inverse, st);
     return PHB_ERR_UNSUPPORTED;
@@ -290,6 +295,7 @@ int phb_fourier_mask_c64(void *arr, int64_t batch, int64_t N, const float *mask,
     if (!arr || !mask || batch < 0) return PHB_ERR_INVALID_ARG;
     if (batch == 0) return PHB_OK;
     cudaStream_t st = (cudaStream_t)stream;
+    if (N == 256) return launch_fourier_mask<256>((float2 *)arr, mask, batch, st);
     if (N == 128) return launch_fourier_mask<128>((float2 *)arr, mask, batch, st);
     if (N == 64) return launch_fourier_mask<64>((float2 *)arr, mask, batch, st);
     return PHB_ERR_UNSUPPORTED;

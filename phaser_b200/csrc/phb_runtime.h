@@ -12,4 +12,26 @@ int record_cuda(cudaError_t err);
 // count a kernel launch issued without check_launch() (e.g. cudaLaunchKernelEx)
 void count_launch();
 
+// launch `kernel` over `blocks` CTAs of `threads` threads in thread-block clusters
+// of `cluster` CTAs (1 = no cluster attribute)
+template <typename... P, typename... A>
+inline int launch_clustered(void (*kernel)(P...), unsigned blocks, unsigned threads, unsigned cluster, size_t smem,
+                            cudaStream_t st, A &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(blocks, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = cluster > 1 ? 1 : 0;
+    const int rc = record_cuda(cudaLaunchKernelEx(&cfg, kernel, static_cast<A &&>(args)...));
+    if (rc == PHB_OK) count_launch();
+    return rc;
+}
+
 }  // namespace phb

@@ -69,8 +69,8 @@ class DeviceEngine:
         if not (_is_complex64(probe) and _is_complex64(obj)):
             raise TypeError("the B200 backend computes in complex64 (plan dtype float32)")
         M, N, N2 = probe.shape
-        if N != N2 or N not in (64, 128):
-            raise NotImplementedError(f"probe size {N}x{N2}: the B200 kernels support N in (64, 128)")
+        if N != N2 or N not in (64, 128, 256):
+            raise NotImplementedError(f"probe size {N}x{N2}: the B200 kernels support N in (64, 128, 256)")
         S, H, W = obj.shape
         self.N, self.M, self.S, self.H, self.W = N, M, S, H, W
         self.scan_shape = scan.shape[:-1]
@@ -198,6 +198,8 @@ class DeviceEngine:
     def presolve(self, groups: torch.Tensor, sizes: t.Sequence[int], solver: str = 'lsqml',
                  gradient_form: bool = False) -> float:
         """Mean measured/model intensity ratio over all positions (solvers.py:36-63)."""
+        if solver == 'epie' and self.N == 256 and not gradient_form:
+            raise NotImplementedError("ePIE at a 256 x 256 probe (use LSQ-ML or the gradient engine)")
         G = len(sizes)
         num = torch.zeros((G, self.group_max), dtype=torch.float64, device=self.device)
         den = torch.zeros((G, self.group_max), dtype=torch.float64, device=self.device)
@@ -219,6 +221,9 @@ class DeviceEngine:
         """One mini-batch step (phb_solver_group).  With `rows` = (b0, b1) only those
         rows of the group run (PHB_FLAG_PARTIAL): sum reduce_views() over ranks, then
         call finish()."""
+        if solver == 'epie' and self.N == 256:
+            raise NotImplementedError("ePIE at a 256 x 256 probe: its per-slice maximum over the modes needs all "
+                                      "modes in one cluster (use LSQ-ML or the gradient engine)")
         st = self._step_struct(solver, flags, beta_object, beta_probe, illum_reg_object, illum_reg_probe, gamma,
                                group_index, grad_object, grad_probe, grad_pos, loss, group_patterns, events,
                                grad_pos_scale, group_loss, rows)

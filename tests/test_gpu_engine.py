@@ -41,6 +41,8 @@ CONFIGS = [
     dict(seed=3, N=128, M=4, S=2),
     dict(seed=4, N=64, M=3, S=2, tilt=True),
     dict(seed=5, N=128, M=1, S=3, scan_shape=(3, 3)),
+    dict(seed=6, N=256, M=8, S=4, scan_shape=(2, 2)),
+    dict(seed=7, N=256, M=2, S=3, scan_shape=(2, 2), tilt=True),
 ]
 
 
@@ -102,6 +104,8 @@ GROUP_CONFIGS = [
     ('epie', dict(seed=27, N=128, M=1, S=2), {}),
     ('lsqml', dict(seed=28, N=64, M=2, S=8, scan_shape=(3, 3)), {}),
     ('epie', dict(seed=29, N=64, M=1, S=6, scan_shape=(3, 3)), {}),
+    ('lsqml', dict(seed=30, N=256, M=8, S=4, scan_shape=(3, 3)), {}),
+    ('lsqml', dict(seed=32, N=256, M=2, S=2, scan_shape=(2, 2), tilt=True), {}),
 ]
 
 
@@ -121,8 +125,9 @@ def test_group_step_matches_oracle(solver, cfg, flags):
     assert rel_l2(got['pos'], ref['pos_update']) < 2e-3
 
 
-def test_presolve_rescale_matches_oracle():
-    c = make_case(seed=31, N=64, M=2, S=3)
+@pytest.mark.parametrize('N', [64, 256])
+def test_presolve_rescale_matches_oracle(N):
+    c = make_case(seed=31, N=N, M=2, S=3, scan_shape=(4, 4) if N == 64 else (3, 3))
     n = c.scan.shape[0] * c.scan.shape[1]
     eng = engine_for(c, 8)
     flat = numpy.arange(n, dtype=numpy.int64)
@@ -133,7 +138,7 @@ def test_presolve_rescale_matches_oracle():
     ref = []
     for ch in chunks:
         ref.append(P.epie_dry_run(g, c.probe, c.obj, c.scan.reshape(-1, 2)[ch],
-                                  c.patterns.reshape(-1, 64, 64)[ch], c.mask, c.props(), None))
+                                  c.patterns.reshape(-1, N, N)[ch], c.mask, c.props(), None))
     assert r == pytest.approx(float(numpy.mean(numpy.concatenate(ref))), rel=1e-5)
 
 
@@ -189,6 +194,12 @@ def test_unsupported_shapes_fail_loudly():
     eng = engine_for(c, 2)
     with pytest.raises(ValueError):
         eng.group_tensor([numpy.arange(4)])
+    # ePIE needs every mode of a position in one cluster: not at a 256 x 256 probe
+    c2 = make_case(seed=53, N=256, M=2, S=2, scan_shape=(2, 2))
+    eng = engine_for(c2, 4)
+    gt, sizes = eng.group_tensor([numpy.arange(4)])
+    with pytest.raises(NotImplementedError):
+        eng.step('epie', gt[0], sizes[0], flags=_lib.PHB_FLAG_UPDATE_OBJECT)
 
 
 @pytest.mark.parametrize('solver', ['lsqml', 'epie', 'grad'])

@@ -40,6 +40,8 @@ GRAD_CONFIGS = [
     ('anscombe', dict(seed=83, N=128, M=4, S=2)),
     ('amplitude', dict(seed=84, N=64, M=2, S=2, tilt=True)),
     ('poisson', dict(seed=85, N=128, M=2, S=5, scan_shape=(3, 3))),
+    ('poisson', dict(seed=86, N=256, M=2, S=3, scan_shape=(2, 2))),
+    ('amplitude', dict(seed=87, N=256, M=2, S=2, scan_shape=(2, 2), tilt=True)),
 ]
 
 
@@ -209,8 +211,9 @@ def test_autograd_function_matches_oracle_adjoint():
     assert rel_l2(g.cpu().numpy(), r_obj) < 1e-4
 
 
-@pytest.mark.parametrize('cfg', [dict(seed=87, N=64, M=2, S=3), dict(seed=88, N=128, M=2, S=4, scan_shape=(3, 3))],
-                         ids=['N64M2S3', 'N128M2S4'])
+@pytest.mark.parametrize('cfg', [dict(seed=87, N=64, M=2, S=3), dict(seed=88, N=128, M=2, S=4, scan_shape=(3, 3)),
+                                 dict(seed=89, N=256, M=2, S=3, scan_shape=(2, 2))],
+                         ids=['N64M2S3', 'N128M2S4', 'N256M2S3'])
 def test_tilt_gradient_matches_oracle_adjoint(cfg):
     c = make_case(tilt=True, **cfg)
     n = c.scan.shape[0] * c.scan.shape[1]

@@ -27,7 +27,7 @@ def dev():
     return torch.device('cuda')
 
 
-@pytest.mark.parametrize('N', [64, 128])
+@pytest.mark.parametrize('N', [64, 128, 256])
 def test_fft2_ifft2_match_oracle(dev, N):
     rng = numpy.random.default_rng(N)
     a = (rng.normal(size=(5, N, N)) + 1j * rng.normal(size=(5, N, N))).astype(numpy.complex64)
@@ -40,7 +40,7 @@ def test_fft2_ifft2_match_oracle(dev, N):
     assert rel_l2(back, a) < 2e-6
 
 
-@pytest.mark.parametrize('N', [64, 128])
+@pytest.mark.parametrize('N', [64, 128, 256])
 def test_fft2_known_answers(dev, N):
     # centred delta -> constant; constant -> corner delta (reference tests/test_num.py:102-155)
     a = numpy.zeros((1, N, N), numpy.complex64)
