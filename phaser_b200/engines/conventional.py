@@ -10,6 +10,7 @@ groupings and reads back one status block per iteration.
 """
 from __future__ import annotations
 
+import dataclasses
 import logging
 import typing as t
 
@@ -86,6 +87,72 @@ class EPIESolver(_SolverBase):
 SOLVERS = {'lsqml': LSQMLSolver, 'epie': EPIESolver}
 
 
+@dataclasses.dataclass
+class HostInputs:
+    """What the conventional engine reads from EngineArgs and the plan before any
+    device work: the parsed plan fields and the exact arguments of the upload."""
+    state: t.Any
+    observer: t.Any
+    noise: NoiseSpec
+    solver_kind: str
+    solver_props: t.Any
+    pos_solver: t.Optional[t.Tuple[str, t.Any]]
+    niter: int
+    grouping: int
+    compact: bool
+    update_probe: t.Callable
+    update_object: t.Callable
+    update_positions: t.Callable
+    calc_error: t.Callable
+    shuffle_groups: t.Callable
+    device_kwargs: t.Dict[str, t.Any]
+
+
+def host_inputs(args: t.Mapping[str, t.Any], props: t.Any, *,
+                patterns_on_device: t.Optional[torch.Tensor] = None) -> HostInputs:
+    """Parse EngineArgs (phaser/hooks/__init__.py:174-181) and a conventional engine plan
+    (the reference's ConventionalEnginePlan, a dict of the same shape, or
+    phaser_b200.plan.ConventionalEnginePlan) on the host, with the reference's checks
+    (conventional/run.py:15-45).  No device work happens here."""
+    state = args['state']
+    data = args['data']
+    dtype = numpy.dtype(args.get('dtype', numpy.float32))
+    if dtype != numpy.float32:
+        raise NotImplementedError("the B200 backend computes in float32/complex64 (plan dtype 'float32')")
+    noise = _noise(props)
+    if noise.kind == 'poisson':
+        # the reference's Poisson model has no wave update (noise_models.py:104-112)
+        raise NotImplementedError("the Poisson noise model has no wave update; use 'amplitude' or 'anscombe'")
+    solver_kind, solver_props = P.solver(P.get(props, 'solver'))
+    compact = bool(P.get(props, 'compact', False))
+    probe0 = _array(state.probe.data)
+    obj0 = _array(state.object.data)
+    scan0 = numpy.asarray(state.scan)
+    if not (_is_complex64(probe0) and _is_complex64(obj0)):
+        raise TypeError("object and probe must be complex64")
+    if patterns_on_device is None and torch.is_tensor(data.patterns):
+        patterns_on_device = data.patterns   # device-resident patterns (e.g. from prepare_for_engine)
+    grouping = int(P.get(props, 'grouping', None) or 64)
+    device_kwargs = dict(
+        probe=probe0, obj=obj0, scan=scan0,
+        patterns=None if patterns_on_device is not None else numpy.asarray(data.patterns),
+        mask=_host(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
+        obj_sampling=_object_sampling(state.object.sampling), thicknesses=numpy.asarray(state.object.thicknesses),
+        wavelength=float(state.wavelength), tilt=None if state.tilt is None else numpy.asarray(state.tilt),
+        noise=noise, bwlim_frac=P.get(props, 'bwlim_frac', 2 / 3), group_max=grouping,
+        patterns_on_device=patterns_on_device)
+    return HostInputs(
+        state=state, observer=args.get('observer', None), noise=noise, solver_kind=solver_kind,
+        solver_props=solver_props, pos_solver=P.position_solver(P.get(props, 'position_solver')),
+        niter=int(P.get(props, 'niter', 10)), grouping=grouping, compact=compact,
+        update_probe=P.process_flag(P.get(props, 'update_probe', True)),
+        update_object=P.process_flag(P.get(props, 'update_object', True)),
+        update_positions=P.process_flag(P.get(props, 'update_positions', False)),
+        calc_error=P.process_flag(P.get(props, 'calc_error', P.Flag(every=1))),
+        shuffle_groups=P.process_flag(P.get(props, 'shuffle_groups', None) or not compact),
+        device_kwargs=device_kwargs)
+
+
 class ConventionalEngine:
     """One conventional-engine run on the device: construction uploads the
     state, `presolve()` rescales the probe, `iteration(i)` runs one full
@@ -94,46 +161,21 @@ class ConventionalEngine:
 
     def __init__(self, args: t.Mapping[str, t.Any], props: t.Any, *,
                  patterns_on_device: t.Optional[torch.Tensor] = None):
-        state = args['state']
-        data = args['data']
-        self.state = state
-        self.observer = args.get('observer', None)
-        dtype = numpy.dtype(args.get('dtype', numpy.float32))
-        if dtype != numpy.float32:
-            raise NotImplementedError("the B200 backend computes in float32/complex64 (plan dtype 'float32')")
-        self.noise = _noise(props)
-        if self.noise.kind == 'poisson':
-            # the reference's Poisson model has no wave update (noise_models.py:104-112)
-            raise NotImplementedError("the Poisson noise model has no wave update; use 'amplitude' or 'anscombe'")
-        self.solver_kind, solver_props = P.solver(P.get(props, 'solver'))
-        self.solver = SOLVERS[self.solver_kind](props, solver_props)
-        self.pos_solver = P.position_solver(P.get(props, 'position_solver'))
-        self.niter = int(P.get(props, 'niter', 10))
-        grouping = int(P.get(props, 'grouping', None) or 64)
-        self.compact = bool(P.get(props, 'compact', False))
-        self.update_probe = P.process_flag(P.get(props, 'update_probe', True))
-        self.update_object = P.process_flag(P.get(props, 'update_object', True))
-        self.update_positions = P.process_flag(P.get(props, 'update_positions', False))
-        self.calc_error = P.process_flag(P.get(props, 'calc_error', P.Flag(every=1)))
-        self.shuffle_groups = P.process_flag(P.get(props, 'shuffle_groups', None) or not self.compact)
-
-        probe0 = _array(state.probe.data)
-        obj0 = _array(state.object.data)
-        self.scan0 = numpy.asarray(state.scan)
-        if not (_is_complex64(probe0) and _is_complex64(obj0)):
-            raise TypeError("object and probe must be complex64")
-        if patterns_on_device is None and torch.is_tensor(data.patterns):
-            patterns_on_device = data.patterns   # device-resident patterns (e.g. from prepare_for_engine)
-        osamp = _object_sampling(state.object.sampling)
-        thick = numpy.asarray(state.object.thicknesses)
-        self.eng = eng = DeviceEngine(
-            probe=probe0, obj=obj0, scan=self.scan0,
-            patterns=None if patterns_on_device is not None else numpy.asarray(data.patterns),
-            mask=_host(data.pattern_mask), probe_sampling=state.probe.sampling.sampling,
-            obj_sampling=osamp, thicknesses=thick, wavelength=float(state.wavelength),
-            tilt=None if state.tilt is None else numpy.asarray(state.tilt), noise=self.noise,
-            bwlim_frac=P.get(props, 'bwlim_frac', 2 / 3), group_max=grouping,
-            patterns_on_device=patterns_on_device)
+        h = host_inputs(args, props, patterns_on_device=patterns_on_device)
+        state = self.state = h.state
+        self.observer = h.observer
+        self.noise = h.noise
+        self.solver_kind = h.solver_kind
+        self.solver = SOLVERS[self.solver_kind](props, h.solver_props)
+        self.pos_solver = h.pos_solver
+        self.niter = h.niter
+        grouping = h.grouping
+        self.compact = h.compact
+        self.update_probe, self.update_object = h.update_probe, h.update_object
+        self.update_positions, self.calc_error = h.update_positions, h.calc_error
+        self.shuffle_groups = h.shuffle_groups
+        self.scan0 = h.device_kwargs['scan']
+        self.eng = eng = DeviceEngine(**h.device_kwargs)   # the upload: raises without a CUDA device
         self.group_cons = build_constraints(P.get(props, 'group_constraints', []) or [], eng, state, per_group=True)
         self.iter_cons = build_constraints(P.get(props, 'iter_constraints', []) or [], eng, state, per_group=False)
         self.groups = GroupManager(self.scan0.shape[:-1], grouping, self.compact, seed=args.get('seed', None))
