@@ -40,10 +40,11 @@ pytestmark = pytest.mark.skipif(REF is None, reason="phaser reference sources no
 
 @pytest.fixture(scope='module')
 def ref():
+    # appended, not prepended: the reference tree has its own `tests` package, which must
+    # not shadow this repository's (child processes inherit sys.path)
     shim = os.path.join(ROOT, 'tests', 'golden', 'pane_shim')
-    for p in (shim, REF):
-        if p not in sys.path:
-            sys.path.insert(0, p)
+    added = [p for p in (shim, REF) if p not in sys.path]
+    sys.path.extend(added)
     import phaser
     import phaser.execute
     import phaser.plan
@@ -54,9 +55,11 @@ def ref():
     from phaser.hooks.solver import (NoiseModelHook, ConventionalSolverHook, PositionSolverHook,
                                      MomentumPositionSolverProps)
     from phaser.utils.object import ObjectSampling
-    return dict(phaser=phaser, EngineHook=EngineHook, NoiseModelHook=NoiseModelHook,
-                ConventionalSolverHook=ConventionalSolverHook, PositionSolverHook=PositionSolverHook,
-                MomentumPositionSolverProps=MomentumPositionSolverProps, ObjectSampling=ObjectSampling)
+    yield dict(phaser=phaser, EngineHook=EngineHook, NoiseModelHook=NoiseModelHook,
+               ConventionalSolverHook=ConventionalSolverHook, PositionSolverHook=PositionSolverHook,
+               MomentumPositionSolverProps=MomentumPositionSolverProps, ObjectSampling=ObjectSampling)
+    for p in added:
+        sys.path.remove(p)
 
 
 def reference_inputs(ref, N=64, M=2, S=3):
