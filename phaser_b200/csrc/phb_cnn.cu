@@ -209,6 +209,251 @@ __global__ void __launch_bounds__(256) k_conv_bwd_w(const float *in, const float
     }
 }
 
+// ------------------------------------------- tensor-core implicit GEMM (tcgen05)
+// The 3x3 convolution as a GEMM D[m][c] = sum_k A[m][k] B[c][k] on the 5th-generation
+// tensor cores: m = 128 output pixels per CTA (UMMA M = 128), c = the output channels
+// (UMMA N = 32 or 64, the accumulator a 128 x N float32 tile in tensor memory), k = the
+// reduction (channel, tap) pairs in chunks of 16 channels x 9 taps = 144 (9 MMAs of
+// K = 16 each).  Forward: A = im2col(in), B = the weights.  Data gradient: A = the
+// transposed-convolution gather of dout, B = the weights with channels exchanged.
+//
+// Operands are bf16 in shared memory in the K-major canonical layout without swizzle
+// (8 rows x 16 bytes per core matrix; the two core matrices of one K = 16 step 128 bytes
+// apart, 8-row groups 2304 bytes apart).  The weights are bf16 already; each float32
+// activation is split into bf16 hi + bf16 lo parts and both are multiplied (two MMAs per
+// step into the same accumulator), so the products keep ~16 mantissa bits of the
+// activation: the results match the float32-activation / bf16-weight / float32-accumulate
+// definition of the FP32 kernels above to ~1e-5.  Chunks are double buffered: the CTA
+// stages chunk c + 1 while the tensor cores run chunk c (tcgen05.commit -> mbarrier).
+namespace tc {
+constexpr int BM = 128;                 // output pixels per CTA
+constexpr int CC = 16;                  // reduction channels per chunk
+constexpr int KC = CC * 9;              // 144 reduction elements per chunk
+constexpr int KSTEPS = KC / 16;         // 9 MMAs (x2: hi and lo) per chunk
+constexpr uint32_t SBO = (KC / 8) * 128;   // 2304 bytes between 8-row groups
+constexpr uint32_t LBO = 128;              // bytes between the two K halves of a step
+constexpr int A_BYTES = BM * KC * 2;       // 36864 per stage and part
+constexpr int THREADS = 256;
+template <int NT> struct Smem {
+    static constexpr int B_BYTES = NT * KC * 2;
+    static constexpr int TOTAL = 2 * 2 * A_BYTES + 2 * B_BYTES + 64;
+};
+constexpr long long WAIT_LIMIT = 1ll << 22;   // try_wait attempts before a wait is abandoned
+}  // namespace tc
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: K-major, no swizzle, sm_100 descriptor version 1
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((tc::LBO >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((tc::SBO >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+// instruction descriptor of kind::f16: D float32, A and B bf16, both K-major, M x N
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                 :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(mbar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+    const uint32_t addr = smem_u32(mbar);
+    for (long long i = 0; i < tc::WAIT_LIMIT; ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
+    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// MODE 0: forward (out = conv(in, w) + bias, optional ReLU; src = in, Cr = Ci, N = Co,
+//         output Ho x Wo, source Hs x Ws = Hi x Wi);
+// MODE 1: data gradient (din = conv^T(dout, w); src = dout, Cr = Co, N = Ci, output
+//         Hi x Wi, source Hs x Ws = Ho x Wo).
+template <int NT, int S, int MODE>
+__global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, const __nv_bfloat16 *w, const float *bias,
+                                                            float *out, int Mtot, int Cr, int Ncol, int Hs, int Ws,
+                                                            int Ho, int Wo, int Ci_w, int relu) {
+    using namespace tc;
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    unsigned char *Ahi = tsm, *Alo = tsm + 2 * A_BYTES, *Bs = tsm + 4 * A_BYTES;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * Smem<NT>::B_BYTES);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * BM;
+    const int HWo = Ho * Wo;
+
+    if (warp == 0) {   // tensor-memory accumulator: NT columns x 128 lanes of float32
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"((uint32_t)NT) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    constexpr uint32_t IDESC = umma_idesc_bf16(BM, NT);
+    const int nchunks = (Cr + CC - 1) / CC;
+    bool ok = true;
+
+    for (int c = 0; c < nchunks; ++c) {
+        const int sb = c & 1;
+        if (c >= 2) {   // chunk c - 2 has left this buffer (the decision is uniform over the CTA)
+            const bool done = mbar_wait(&mbar[sb], (uint32_t)(((c >> 1) - 1) & 1));
+            if (!__syncthreads_and(done)) {
+                ok = false;
+                break;
+            }
+        }
+        const int ch0 = c * CC;
+        // A: 2304 16-byte units (8 reduction elements of one pixel row each), hi and lo parts
+        for (int L = tid; L < BM * (KC / 8); L += THREADS) {
+            const int g = L / (KC / 8 * 8), rem = L % (KC / 8 * 8), c8 = rem >> 3, r = rem & 7;
+            const int mg = m0 + 8 * g + r;
+            float vals[8];
+            if (mg < Mtot) {
+                const int n = mg / HWo, p = mg - n * HWo, y = p / Wo, x = p - y * Wo;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int k = 8 * c8 + j, ch = ch0 + k / 9, tap = k % 9, ky = tap / 3, kx = tap % 3;
+                    float v = 0.f;
+                    if (ch < Cr) {
+                        int sy, sx;
+                        bool in;
+                        if constexpr (MODE == 0) {
+                            sy = S * y + ky - 1;
+                            sx = S * x + kx - 1;
+                            in = sy >= 0 && sy < Hs && sx >= 0 && sx < Ws;
+                        } else {
+                            const int ty = y + 1 - ky, tx = x + 1 - kx;
+                            sy = ty / S;
+                            sx = tx / S;
+                            in = ty >= 0 && tx >= 0 && ty % S == 0 && tx % S == 0 && sy < Hs && sx < Ws;
+                        }
+                        if (in) v = __ldg(src + (((size_t)n * Cr + ch) * Hs + sy) * Ws + sx);
+                    }
+                    vals[j] = v;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) vals[j] = 0.f;
+            }
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat16 h0 = __float2bfloat16_rn(vals[2 * j]), h1 = __float2bfloat16_rn(vals[2 * j + 1]);
+                const __nv_bfloat16 l0 = __float2bfloat16_rn(vals[2 * j] - __bfloat162float(h0));
+                const __nv_bfloat16 l1 = __float2bfloat16_rn(vals[2 * j + 1] - __bfloat162float(h1));
+                hi[j] = pack_bf16(h0, h1);
+                lo[j] = pack_bf16(l0, l1);
+            }
+            *reinterpret_cast<uint4 *>(Ahi + sb * A_BYTES + L * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4 *>(Alo + sb * A_BYTES + L * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
+        // B: NT rows of the weights for this chunk
+        for (int L = tid; L < NT * (KC / 8); L += THREADS) {
+            const int g = L / (KC / 8 * 8), rem = L % (KC / 8 * 8), c8 = rem >> 3, r = rem & 7;
+            const int col = 8 * g + r;
+            uint32_t wv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                __nv_bfloat16 e[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = 8 * c8 + 2 * j + h, ch = ch0 + k / 9, tap = k % 9;
+                    e[h] = __float2bfloat16_rn(0.f);
+                    if (ch < Cr && col < Ncol) {
+                        // forward: w[co = col][ci = ch]; data gradient: w[co = ch][ci = col]
+                        const size_t idx = MODE == 0 ? ((size_t)col * Ci_w + ch) * 9 + tap : ((size_t)ch * Ci_w + col) * 9 + tap;
+                        e[h] = w[idx];
+                    }
+                }
+                wv[j] = pack_bf16(e[0], e[1]);
+            }
+            *reinterpret_cast<uint4 *>(Bs + sb * Smem<NT>::B_BYTES + L * 16) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+        }
+        // generic-proxy writes -> visible to the tensor cores (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a_hi = smem_u32(Ahi + sb * A_BYTES), a_lo = smem_u32(Alo + sb * A_BYTES);
+            const uint32_t b0 = smem_u32(Bs + sb * Smem<NT>::B_BYTES);
+#pragma unroll 1
+            for (int j = 0; j < KSTEPS; ++j) {
+                const uint64_t db = umma_desc(b0 + 256 * j);
+                umma_bf16(tmem, umma_desc(a_hi + 256 * j), db, IDESC, (c > 0 || j > 0) ? 1u : 0u);
+                umma_bf16(tmem, umma_desc(a_lo + 256 * j), db, IDESC, 1u);
+            }
+            umma_commit(&mbar[sb]);
+        }
+    }
+    if (ok) ok = mbar_wait(&mbar[(nchunks - 1) & 1], (uint32_t)(((nchunks - 1) >> 1) & 1));   // all MMAs done
+    ok = __syncthreads_and(ok);
+    if (!ok) {   // a wait gave up: let the issued MMAs drain (bounded) before the memory is released
+        mbar_wait(&mbar[0], 0);
+        mbar_wait(&mbar[1], 0);
+        __syncthreads();
+    }
+    tc_fence_after();
+    // accumulator -> registers: warp w reads lanes 32 (w % 4) .. +31, columns of half w / 4
+    {
+        const int q = warp & 3, half = warp >> 2;
+        const int m = 32 * q + lane, mg = m0 + m;
+        constexpr int COLS = NT / 2;
+        uint32_t r[COLS];
+#pragma unroll
+        for (int c16 = 0; c16 < COLS / 16; ++c16) {
+            const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(half * COLS + 16 * c16);
+            uint32_t *d = r + 16 * c16;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                         "%12, %13, %14, %15}, [%16];"
+                         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
+                           "=r"(d[7]), "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]),
+                           "=r"(d[14]), "=r"(d[15])
+                         : "r"(taddr));
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (mg < Mtot) {
+            const int n = mg / HWo, p = mg - n * HWo;
+#pragma unroll
+            for (int j = 0; j < COLS; ++j) {
+                const int col = half * COLS + j;
+                if (col >= Ncol) break;
+                float v = ok ? __uint_as_float(r[j]) : __int_as_float(0x7fc00000);
+                if constexpr (MODE == 0) {
+                    v += bias[col];
+                    if (relu) v = fmaxf(v, 0.f);
+                }
+                out[((size_t)n * Ncol + col) * HWo + p] = v;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"((uint32_t)NT) : "memory");
+    }
+}
+
 // ----------------------------------------------------------- elementwise
 __global__ void k_relu_bwd(float *g, const float *y, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -359,6 +604,35 @@ static void launch_bwd_data(const float *dout, const __nv_bfloat16 *w, float *di
     k_conv_bwd_data<CIO, S><<<grid, 256, 0, st>>>(dout, w, din, Ci, Hi, Wi, Co, Ho, Wo);
 }
 
+// the tensor-core form serves GEMM widths (output channels) of 32 and 64
+template <int S, int MODE>
+static int launch_conv_tc(const float *src, const __nv_bfloat16 *w, const float *bias, float *out, int Mtot, int Cr,
+                          int Ncol, int Hs, int Ws, int Ho, int Wo, int Ci_w, int relu, cudaStream_t st) {
+    const unsigned grid = (unsigned)((Mtot + tc::BM - 1) / tc::BM);
+    if (Ncol <= 32) {
+        auto k = k_conv_tc<32, S, MODE>;
+        static bool cfg = false;
+        if (!cfg) {
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::Smem<32>::TOTAL) != cudaSuccess)
+                return record_cuda(cudaGetLastError());
+            cfg = true;
+        }
+        k<<<grid, tc::THREADS, tc::Smem<32>::TOTAL, st>>>(src, w, bias, out, Mtot, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu);
+    } else {
+        auto k = k_conv_tc<64, S, MODE>;
+        static bool cfg = false;
+        if (!cfg) {
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::Smem<64>::TOTAL) != cudaSuccess)
+                return record_cuda(cudaGetLastError());
+            cfg = true;
+        }
+        k<<<grid, tc::THREADS, tc::Smem<64>::TOTAL, st>>>(src, w, bias, out, Mtot, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu);
+    }
+    return check_launch();
+}
+
+static bool tc_width(int n) { return n == 32 || n == 64; }
+
 extern "C" {
 
 int phb_conv3x3_fwd(const float *in, const void *w_bf16, const float *bias, float *out, int32_t Nb, int32_t Ci,
@@ -369,6 +643,11 @@ int phb_conv3x3_fwd(const float *in, const void *w_bf16, const float *bias, floa
     const int Ho = Hi / stride, Wo = Wi / stride;
     const __nv_bfloat16 *w = (const __nv_bfloat16 *)w_bf16;
     cudaStream_t st = (cudaStream_t)stream;
+    const int64_t Mtot = (int64_t)Nb * Ho * Wo;
+    if (tc_width(Co) && Mtot < (1ll << 31)) {   // tensor cores (tcgen05): 32 or 64 output channels
+        return stride == 1 ? launch_conv_tc<1, 0>(in, w, bias, out, (int)Mtot, Ci, Co, Hi, Wi, Ho, Wo, Ci, relu, st)
+                           : launch_conv_tc<2, 0>(in, w, bias, out, (int)Mtot, Ci, Co, Hi, Wi, Ho, Wo, Ci, relu, st);
+    }
     if (Co <= 2) {
         if (stride == 1) launch_fwd<2, 1>(in, w, bias, out, Nb, Ci, Hi, Wi, Co, Ho, Wo, relu, st);
         else launch_fwd<2, 2>(in, w, bias, out, Nb, Ci, Hi, Wi, Co, Ho, Wo, relu, st);
@@ -387,6 +666,11 @@ int phb_conv3x3_bwd_data(const float *dout, const void *w_bf16, float *din, int3
     const int Ho = Hi / stride, Wo = Wi / stride;
     const __nv_bfloat16 *w = (const __nv_bfloat16 *)w_bf16;
     cudaStream_t st = (cudaStream_t)stream;
+    const int64_t Mtot = (int64_t)Nb * Hi * Wi;
+    if (tc_width(Ci) && Mtot < (1ll << 31)) {   // tensor cores: the GEMM width is the input-channel count
+        return stride == 1 ? launch_conv_tc<1, 1>(dout, w, nullptr, din, (int)Mtot, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st)
+                           : launch_conv_tc<2, 1>(dout, w, nullptr, din, (int)Mtot, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st);
+    }
     if (stride == 1) launch_bwd_data<16, 1>(dout, w, din, Nb, Ci, Hi, Wi, Co, Ho, Wo, st);
     else launch_bwd_data<16, 2>(dout, w, din, Nb, Ci, Hi, Wi, Co, Ho, Wo, st);
     return check_launch();

@@ -28,9 +28,14 @@ def bf16_tensor(w):
     return q
 
 
+# 32 / 64 output (forward) or input (data gradient) channels run on the tensor cores
+# (tcgen05 implicit GEMM, 128-pixel tiles, 16-channel reduction chunks); the others on the
+# FP32 pipe.  Partial pixel tiles (B H^2 not a multiple of 128) and partial / several
+# reduction chunks are included.
 @pytest.mark.parametrize('ci,co,stride,H', [(1, 32, 2, 64), (32, 64, 2, 32), (64, 64, 1, 16), (64, 32, 1, 32),
                                             (32, 2, 1, 32), (3, 5, 1, 20), (5, 17, 2, 18), (6, 20, 1, 40),
-                                            (7, 33, 1, 34)])
+                                            (7, 33, 1, 34), (7, 32, 1, 10), (40, 64, 2, 14), (32, 48, 1, 12),
+                                            (64, 40, 2, 16)])
 def test_conv_layer_matches_oracle(ci, co, stride, H):
     rng = numpy.random.default_rng(ci * 100 + co)
     B = 3
