@@ -627,9 +627,10 @@ def chained(out, net, ds, pats, ref, iters, stream, target, new_engine, gradient
 
 
 def run_large_race(args):
-    """Time to the plain LSQ-ML's final NRMSE on the large configuration (detector binned
-    2x2 to 128^2, see large_multislice_config): plain LSQ-ML against warm start ->
-    3 gradient-engine iterations -> LSQ-ML polish, `--nrmse-iters` iterations each."""
+    """Time to the plain LSQ-ML's final NRMSE on the large configuration: plain LSQ-ML
+    against warm start -> 3 gradient-engine iterations -> LSQ-ML polish, `--nrmse-iters`
+    iterations each.  --spec runs it at the stated size (256^2 probe and detector), else
+    with the detector binned 2x2 to 128^2 (see large_multislice_config)."""
     import torch
     from phaser_b200.synthetic import large_multislice_config, simulate_patterns
     from phaser_b200.engines.conventional import ConventionalEngine
@@ -638,10 +639,8 @@ def run_large_race(args):
     from phaser_b200 import plan as PL
     dev = torch.device('cuda', 0)
     torch.cuda.set_device(dev)
-    ds = large_multislice_config(seed=3)
-    pats = simulate_patterns(ds, seed=3, device=dev, group=256)
-    pats16 = pats.to(torch.uint16)
-    del pats
+    ds = large_multislice_config(seed=3, binned=not args.spec)
+    pats16 = simulate_patterns(ds, seed=3, device=dev, group=256, counts_u16=True)
     torch.cuda.empty_cache()
     N = ds.probe.shape[-1]
 
@@ -661,12 +660,77 @@ def run_large_race(args):
 
     res = time_to_target(ds, pats16, new_engine, args.nrmse_iters, torch.cuda.current_stream(),
                          arms=("warm_gradient_lsqml",))
-    print(json.dumps({"metric": "time to the plain LSQ-ML's final NRMSE (s), large configuration, detector binned "
-                                "2x2 to 128^2", "config": {"slices": ds.true_object.shape[0],
-                                                           "object": list(ds.true_object.shape[-2:]), "modes": 8,
-                                                           "positions": int(numpy.prod(ds.scan.shape[:-1])),
-                                                           "batch": 256, "patterns": "uint16 counts, 5e5 e-"},
+    size = "256^2 probe and detector (as specified)" if args.spec else "detector binned 2x2 to 128^2"
+    print(json.dumps({"metric": f"time to the plain LSQ-ML's final NRMSE (s), large configuration, {size}",
+                      "config": {"slices": ds.true_object.shape[0], "object": list(ds.true_object.shape[-2:]),
+                                 "N": N, "modes": 8, "positions": int(numpy.prod(ds.scan.shape[:-1])),
+                                 "batch": 256, "patterns": "uint16 counts, 5e5 e-, resident"},
                       "nrmse": res}), flush=True)
+
+
+def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3):
+    """The large configuration as specified (32 x 1033^2 slices, 256^2 probe and detector
+    x 8 modes, 65536 positions at 3 px, uint16 counts resident): LSQ-ML and gradient-engine
+    throughput over `steps` of the first iteration's mini-batches of 256 (after `warmup`),
+    device time of the group steps (fused launches + update kernels)."""
+    import torch
+    from phaser_b200.synthetic import large_multislice_config, simulate_patterns
+    from phaser_b200.engines.conventional import ConventionalEngine
+    from phaser_b200.engines.gradient import GradientEngine
+    from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
+    from phaser_b200.sampling import Sampling
+    from phaser_b200 import plan as PL
+    t0 = time.perf_counter()
+    ds = large_multislice_config(seed=seed, binned=False)
+    t_obj = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pats16 = simulate_patterns(ds, seed=seed, device=dev, group=256, counts_u16=True)
+    e1.record(stream)
+    e1.synchronize()
+    t_sim = e0.elapsed_time(e1) / 1e3
+    N, S = ds.probe.shape[-1], ds.true_object.shape[0]
+    n_pos = int(numpy.prod(ds.scan.shape[:-1]))
+    out = {"workload": f"large multislice as specified: {S} x {ds.obj_sampling.shape[0]}^2 slices, probe and "
+                       f"detector {N}^2 x 8 modes, 256x256 scan @ 3 px, 5e5 e-/pattern as uint16 counts resident "
+                       f"({pats16.numel() * 2 / 1e9:.1f} GB), batch 256",
+           "unit": UNIT, "positions": n_pos, "object_setup_seconds": t_obj, "simulation_seconds": t_sim,
+           "sample": f"{steps} of the {-(-n_pos // 256)} mini-batches of one iteration, after {warmup}"}
+
+    def state_of():
+        return ReconsState(iter=IterState(), wavelength=ds.wavelength,
+                           probe=ProbeState(Sampling((N, N), sampling=ds.probe_sampling), ds.probe.copy()),
+                           object=ObjectState(ds.obj_sampling, ds.init_object.copy(), ds.thicknesses.copy()),
+                           scan=ds.scan.copy())
+
+    for kind in ('lsqml', 'gradient'):
+        if kind == 'lsqml':
+            props = PL.ConventionalEnginePlan(
+                noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
+                position_solver={'type': 'momentum', 'step_size': 1e-3, 'max_step_size': 0.2, 'momentum': 0.9},
+                niter=10 ** 6, grouping=256, update_positions=True)
+            eng = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state_of(), 'dtype': numpy.float32,
+                                      'seed': 'bench-c5', 'recons_name': 'c5'}, props, patterns_on_device=pats16)
+        else:
+            props = PL.GradientEnginePlan(
+                solvers={'object': {'type': 'adam', 'learning_rate': 1e-2},
+                         'probe': {'type': 'adam', 'learning_rate': 1e-3}},
+                noise_model={'type': 'amplitude'}, niter=10 ** 6, grouping=256)
+            eng = GradientEngine({'data': Patterns(None, ds.mask), 'state': state_of(), 'dtype': numpy.float32,
+                                  'seed': 'bench-c5', 'recons_name': 'c5-grad'}, props, patterns_on_device=pats16)
+        e0.record(stream)
+        eng.presolve()
+        e1.record(stream)
+        e1.synchronize()
+        t_pre = e0.elapsed_time(e1) / 1e3
+        secs = eng.time_group_steps(1, warmup, steps, stream)
+        out[kind] = {"value": steps * 256 * S / secs, "ms_per_mini_batch": secs / steps * 1e3,
+                     "presolve_seconds": t_pre}
+        del eng
+        torch.cuda.empty_cache()
+    del pats16
+    torch.cuda.empty_cache()
+    return out
 
 
 def extra_configs(dev, stream):
@@ -851,6 +915,10 @@ def main():
     ap.add_argument('--batch', type=int, default=256, help='mini-batch size (256 = the benchmark configuration)')
     ap.add_argument('--large-race', action='store_true',
                     help='only the time-to-NRMSE race on the large configuration (several minutes)')
+    ap.add_argument('--spec', action='store_true',
+                    help='--large-race at the stated size (256^2 probe and detector) instead of the binned one')
+    ap.add_argument('--large-rate', action='store_true',
+                    help='only the large configuration at the stated size: LSQ-ML / gradient-engine throughput')
     ap.add_argument('--cnn', type=int, default=0, metavar='PATTERNS',
                     help='only time the warm-start network on this many patterns (training step and inference)')
     args = ap.parse_args()
@@ -860,6 +928,14 @@ def main():
         return
     if args.large_race:
         run_large_race(args)
+        return
+    if args.large_rate:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"metric": "large configuration as specified, pos*slice/s",
+                          "large_multislice_spec": large_spec_rate(dev, torch.cuda.current_stream(), args.steps,
+                                                                   args.warmup)}), flush=True)
         return
     if args.impl == 'reference':
         run_reference(args, world, rank)

@@ -202,9 +202,18 @@ class ConventionalEngine:
         _call(self.observer, 'start_engine', self.state)
         return rescale
 
-    def iteration(self, i: int, *, sync: bool = True) -> t.Optional[float]:
+    def time_group_steps(self, i: int, warmup: int, steps: int, stream) -> float:
+        """Seconds of device time (CUDA events on `stream`) of mini-batches warmup ..
+        warmup + steps - 1 of iteration i, run as the iteration runs them (the iteration's
+        tail -- position update, report -- is not part of the sample)."""
+        return _time_groups(self, i, warmup, steps, stream)
+
+    def iteration(self, i: int, *, sync: bool = True, groups_only: t.Optional[int] = None,
+                  on_group: t.Optional[t.Callable[[int], None]] = None) -> t.Optional[float]:
         """Run iteration i (1-based).  With sync=True, wait for the device, raise
-        on NaN / positions outside the object, record and return the error."""
+        on NaN / positions outside the object, record and return the error.
+        groups_only=k runs only the first k mini-batches (no iteration tail); on_group(gi)
+        is called before mini-batch gi is enqueued (timing samples)."""
         eng, state = self.eng, self.state
         state.iter.engine_iter = i
         state.iter.total_iter = self.start_i + i
@@ -220,6 +229,10 @@ class ConventionalEngine:
         gt, sizes = eng.group_tensor([self.groups.flat(g) for g in glist])
         eng.iteration_reset()
         for gi, B in enumerate(sizes):
+            if groups_only is not None and gi >= groups_only:
+                return None
+            if on_group is not None:
+                on_group(gi)
             f = flags | (_lib.PHB_FLAG_CALC_ERROR if (it_err and self.calc_error_mask[gi]) else 0)
             ev = None
             if self.fused_events is not None:
@@ -279,6 +292,19 @@ class ConventionalEngine:
         self.state.scan = scan.astype(self.scan0.dtype)
         _call(self.observer, 'finish_engine', self.state)
         return self.state
+
+
+def _time_groups(engine, i: int, warmup: int, steps: int, stream) -> float:
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def mark(gi: int) -> None:
+        if gi == warmup:
+            e0.record(stream)
+
+    engine.iteration(i, sync=False, groups_only=warmup + steps, on_group=mark)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3
 
 
 def _new_event_pair() -> t.Tuple[int, int]:

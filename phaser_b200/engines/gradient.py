@@ -333,9 +333,18 @@ class GradientEngine:
         _call(self.observer, 'start_engine', self.state)
         return rescale
 
-    def iteration(self, i: int, *, sync: bool = True) -> t.Optional[float]:
+    def time_group_steps(self, i: int, warmup: int, steps: int, stream) -> float:
+        """Seconds of device time of mini-batches warmup .. warmup + steps - 1 of iteration
+        i (loss, adjoint and optimizer steps; not the iteration's tail)."""
+        from .conventional import _time_groups
+        return _time_groups(self, i, warmup, steps, stream)
+
+    def iteration(self, i: int, *, sync: bool = True, groups_only: t.Optional[int] = None,
+                  on_group: t.Optional[t.Callable[[int], None]] = None) -> t.Optional[float]:
         """Run iteration i (1-based).  With sync=True, wait for the device, raise on
-        NaN / positions outside the object and return the mean loss."""
+        NaN / positions outside the object and return the mean loss.  groups_only=k runs
+        only the first k mini-batches (no iteration tail); on_group(gi) is called before
+        mini-batch gi is enqueued (timing samples)."""
         eng, state = self.eng, self.state
         state.iter.engine_iter = i
         state.iter.total_iter = self.start_i + i
@@ -357,6 +366,10 @@ class GradientEngine:
         eng.status.fill_(-1)
         probe_int = self.probe_int
         for gi, B in enumerate(sizes):
+            if groups_only is not None and gi >= groups_only:
+                return None
+            if on_group is not None:
+                on_group(gi)
             if 'object' in iter_vars:
                 self.grad_object.zero_()
             if 'probe' in iter_vars:

@@ -110,15 +110,15 @@ def lsqml_multislice_config(seed: int = 0, scan: int = 64) -> Dataset:
                         peak_rad=0.2, counts=1e6, mode_powers=(0.70, 0.15, 0.10, 0.05), seed=seed)
 
 
-# the large multislice configuration (32 slices of 1032^2, 8 modes, 256 x 256 scan at 3 px,
-# 5e5 e-/pattern) with its 256^2 detector binned 2 x 2 to 128^2: the pixel size stays
-# 0.2 A, the probe window halves to 25.6 A (the 25 mrad probe at 200 A defocus is ~10 A
-# across), i.e. prepare_for_engine with sim_shape (128, 128), resize_method 'resample'.
-# The object grid is the one the reference builds for the 256^2 probe.
-def large_multislice_config(seed: int = 0, scan: int = 256) -> Dataset:
-    return make_dataset(N=128, M=8, S=32, scan_shape=(scan, scan), step_px=3.0, sampling=0.2, kv=300e3,
-                        conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
-                        peak_rad=0.2, counts=5e5, seed=seed, grid_probe_px=256)
+# the large multislice configuration: 32 slices of 1032^2-class, probe and detector 256^2
+# with 8 modes, 256 x 256 scan at 3 px, 5e5 e-/pattern.  binned=True keeps the object grid
+# but bins the detector 2 x 2 to 128^2: the pixel size stays 0.2 A, the probe window
+# halves to 25.6 A (the 25 mrad probe at 200 A defocus is ~10 A across), i.e.
+# prepare_for_engine with sim_shape (128, 128), resize_method 'resample'.
+def large_multislice_config(seed: int = 0, scan: int = 256, binned: bool = True) -> Dataset:
+    return make_dataset(N=128 if binned else 256, M=8, S=32, scan_shape=(scan, scan), step_px=3.0, sampling=0.2,
+                        kv=300e3, conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0,
+                        sigma_px=1.5, peak_rad=0.2, counts=5e5, seed=seed, grid_probe_px=256)
 
 
 # the single-slice ePIE configuration (256^2-class object, 64^2 probe, 32^2 scan)
@@ -135,8 +135,12 @@ def gradient_multislice_config(seed: int = 0, scan: int = 128) -> Dataset:
                         peak_rad=0.2, counts=1e6, mode_powers=(0.7, 0.3), seed=seed)
 
 
-def simulate_patterns(ds: Dataset, *, seed: int = 0, group: int = 256, device='cuda'):
-    """Noisy patterns (n_pos, N, N) float32 on the device, from the B200 forward kernel."""
+def simulate_patterns(ds: Dataset, *, seed: int = 0, group: int = 256, device='cuda', counts_u16: bool = False):
+    """Noisy patterns (n_pos, N, N) on the device, from the B200 forward kernel: float32,
+    or (counts_u16) uint16 detector counts, drawn group by group so that no float32 copy
+    of the whole set is held."""
+    if counts_u16:
+        return _simulate_counts_u16(ds, seed=seed, group=group, device=device)
     import torch
     from .device import DeviceEngine
     N = ds.probe.shape[-1]
@@ -158,3 +162,32 @@ def simulate_patterns(ds: Dataset, *, seed: int = 0, group: int = 256, device='c
     pats = torch.poisson(out * (ds.counts / total), generator=gen).to(torch.float32)
     del eng, dummy
     return pats
+
+
+def _simulate_counts_u16(ds: Dataset, *, seed: int, group: int, device) -> 'torch.Tensor':
+    import torch
+    from .device import DeviceEngine
+    N = ds.probe.shape[-1]
+    n = int(numpy.prod(ds.scan.shape[:-1]))
+    out = torch.empty((n, N, N), dtype=torch.uint16, device=device)
+    eng = DeviceEngine(probe=ds.probe, obj=ds.true_object, scan=ds.scan, patterns=None, mask=ds.mask,
+                       probe_sampling=ds.probe_sampling, obj_sampling=ds.obj_sampling,
+                       thicknesses=ds.thicknesses, wavelength=ds.wavelength, group_max=group,
+                       device=device, patterns_on_device=out)
+    idx = numpy.arange(n, dtype=numpy.int64)
+    chunks = [idx[i:i + group] for i in range(0, n, group)]
+    gt, sizes = eng.group_tensor(chunks)
+    buf = torch.empty((group, N, N), dtype=torch.float32, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    peak = torch.zeros((), dtype=torch.float32, device=device)
+    for g, B in enumerate(sizes):
+        inten = eng.simulate(gt[g], B, buf[:B])
+        total = inten.sum(dim=(1, 2), keepdim=True)
+        cnt = torch.poisson(inten * (ds.counts / total), generator=gen)
+        peak = torch.maximum(peak, cnt.max())
+        out[g * group:g * group + B] = cnt.to(torch.uint16)
+    if float(peak) >= 65536:
+        raise RuntimeError(f"{float(peak)} counts do not fit uint16")
+    del eng, buf
+    return out

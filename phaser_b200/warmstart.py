@@ -61,6 +61,20 @@ class FeatureSpec:
 
 
 DEFAULT_FEATURES = FeatureSpec()
+TRAIN_N = 128   # detector side of the training patterns
+
+
+def features_for(spec: FeatureSpec, N: int) -> FeatureSpec:
+    """The feature window for N^2 patterns of the training pixel size in real space: a
+    detector of N > TRAIN_N pixels samples reciprocal space N / TRAIN_N times finer, so
+    the window covers N / TRAIN_N times more pixels, binned by that factor -- the same
+    angular range at the same resolution the network was trained on."""
+    if N == TRAIN_N:
+        return spec
+    if N % TRAIN_N:
+        raise ValueError(f"no feature window for {N}^2 patterns (a multiple of {TRAIN_N} is needed)")
+    f = N // TRAIN_N
+    return dataclasses.replace(spec, crop=spec.crop * f, bin=spec.bin * f)
 
 
 def _stream() -> int:
@@ -382,7 +396,7 @@ def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.nd
     sub = pats.reshape(-1, *pats.shape[-2:])
     if len(idx) != flat_scan.shape[0]:
         sub = _as_f32(sub, torch.from_numpy(idx).to(pats.device))
-    feats = pattern_features(sub, net.features)
+    feats = pattern_features(sub, features_for(net.features, eng.N))
     proj = stitch(net, feats, flat_scan[idx], eng.obj_sampling, (H, W), eng.N, window_sigma)
     r_flat = pattern_residual(eng, eng.object, residual_stride)
     best = None
