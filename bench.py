@@ -250,6 +250,9 @@ def run_b200(args, world, rank, local):
     dev = torch.device('cuda', local)
     if world > 1:
         import datetime
+        # NCCL's initialisation log (stderr) shows the ranks and the NVLink / NVLS paths it set up
+        os.environ.setdefault('NCCL_DEBUG', 'INFO')
+        os.environ.setdefault('NCCL_DEBUG_SUBSYS', 'INIT')
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
     lib = _lib.load()
