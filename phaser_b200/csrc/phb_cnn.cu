@@ -210,43 +210,53 @@ __global__ void __launch_bounds__(256) k_conv_bwd_w(const float *in, const float
 }
 
 // ------------------------------------------- tensor-core implicit GEMM (tcgen05)
-// The 3x3 convolution as a GEMM D[m][c] = sum_k A[m][k] B[c][k] on the 5th-generation
-// tensor cores: m = 128 output pixels per CTA (UMMA M = 128), c = the output channels
-// (UMMA N = 32 or 64, the accumulator a 128 x N float32 tile in tensor memory), k = the
-// reduction (channel, tap) pairs in chunks of 16 channels x 9 taps = 144 (9 MMAs of
-// K = 16 each).  Forward: A = im2col(in), B = the weights.  Data gradient: A = the
-// transposed-convolution gather of dout, B = the weights with channels exchanged.
+// A 3x3 convolution as nine shifted GEMMs on the 5th-generation tensor cores:
+// D[m][c] = sum_tap sum_k A_tap[m][k] B_tap[c][k], m = 128 output pixels of one image per
+// CTA (UMMA M = 128), c = the output channels (UMMA N = 32 or 64; the accumulator is a
+// 128 x N float32 tile in tensor memory), k = 16 reduction channels per MMA.
 //
-// Operands are bf16 in shared memory in the K-major canonical layout without swizzle
-// (8 rows x 16 bytes per core matrix; the two core matrices of one K = 16 step 128 bytes
-// apart, 8-row groups 2304 bytes apart).  The weights are bf16 already; each float32
-// activation is split into bf16 hi + bf16 lo parts and both are multiplied (two MMAs per
-// step into the same accumulator), so the products keep ~16 mantissa bits of the
-// activation: the results match the float32-activation / bf16-weight / float32-accumulate
-// definition of the FP32 kernels above to ~1e-5.  Chunks are double buffered: the CTA
-// stages chunk c + 1 while the tensor cores run chunk c (tcgen05.commit -> mbarrier).
+// Pixels are numbered on a padded grid of pitch Wp: output pixel (y, x) is row
+// q = (y + 1) Wp + (x + 1).  A CTA stages, once per chunk of 16 reduction channels, the
+// rows its 128 outputs read -- for stride 1 the input plane itself (rows q0 - Wp - 1 ..
+// q0 + 128 + Wp), for stride 2 its four polyphase components in[2i + py][2j + px] (rows
+// q0 - Wp - 1 .. q0 + 127 each) -- as bf16 rows of 16 channels.  Every tap then reads
+// the same staged rows shifted by a constant (dy Wp + dx rows), which in the operand
+// layout (K-major, no swizzle: row r at 16 r bytes, the two 8-channel halves of a row
+// R * 16 bytes apart) is only a different start address of the matrix descriptor, so
+// each staged value serves all nine taps.
+//
+// Precision: the weights are bf16 already; each float32 activation is split into bf16
+// hi + bf16 lo and both parts are multiplied (two MMAs per tap into the same
+// accumulator), so the products keep ~16 mantissa bits of the activation and the
+// results match the FP32 kernels' float32-activation / bf16-weight / float32-accumulate
+// definition to ~1e-5.  Chunks are double buffered (the CTA stages chunk c + 1 while the
+// tensor cores run chunk c; tcgen05.commit arrives on an mbarrier per buffer), and every
+// wait is bounded.
+//
+// MODE 0: forward, stride 1 or 2 (out = conv(in, w) + bias, optional ReLU).
+// MODE 1: data gradient at stride 1 (din[ci][Y][X] = sum w[co][ci][ky][kx] dout[co][Y+1-ky][X+1-kx]:
+//         the tap offsets mirrored and the channel roles exchanged).
 namespace tc {
-constexpr int BM = 128;                 // output pixels per CTA
-constexpr int CC = 16;                  // reduction channels per chunk
-constexpr int KC = CC * 9;              // 144 reduction elements per chunk
-constexpr int KSTEPS = KC / 16;         // 9 MMAs (x2: hi and lo) per chunk
-constexpr uint32_t SBO = (KC / 8) * 128;   // 2304 bytes between 8-row groups
-constexpr uint32_t LBO = 128;              // bytes between the two K halves of a step
-constexpr int A_BYTES = BM * KC * 2;       // 36864 per stage and part
+constexpr int BM = 128;                 // output pixels (padded-grid rows) per CTA
+constexpr int CC = 16;                  // reduction channels per chunk (one MMA K)
 constexpr int THREADS = 256;
-template <int NT> struct Smem {
-    static constexpr int B_BYTES = NT * KC * 2;
-    static constexpr int TOTAL = 2 * 2 * A_BYTES + 2 * B_BYTES + 64;
-};
 constexpr long long WAIT_LIMIT = 1ll << 22;   // try_wait attempts before a wait is abandoned
+__host__ __device__ constexpr int pitch(int S, int Wo) { return S == 1 ? Wo + 2 : Wo + 1; }
+// staged rows per phase
+__host__ __device__ constexpr int rows(int S, int Wp) { return S == 1 ? BM + 2 * Wp + 2 : BM + Wp + 1; }
+__host__ __device__ constexpr int phases(int S) { return S == 1 ? 1 : 4; }
+template <int NT> struct B_ { static constexpr int BYTES = 9 * NT * CC * 2; };
+// bytes of one stage: A (phases x rows x 16 channels x bf16, hi and lo) + B (9 taps x NT x 16)
+__host__ __device__ constexpr int a_bytes(int S, int Wp) { return phases(S) * rows(S, Wp) * CC * 2; }
 }  // namespace tc
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// shared-memory matrix descriptor: K-major, no swizzle, sm_100 descriptor version 1
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((tc::LBO >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((tc::SBO >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+// shared-memory matrix descriptor: K-major, no swizzle, sm_100 descriptor version 1;
+// rows 16 bytes apart (SBO 128 bytes per 8-row group), the two K halves `lbo` bytes apart
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(128u >> 4) << 32) | ((uint64_t)1 << 46);
 }
 // instruction descriptor of kind::f16: D float32, A and B bf16, both K-major, M x N
 __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
@@ -279,22 +289,23 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) 
     return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
 
-// MODE 0: forward (out = conv(in, w) + bias, optional ReLU; src = in, Cr = Ci, N = Co,
-//         output Ho x Wo, source Hs x Ws = Hi x Wi);
-// MODE 1: data gradient (din = conv^T(dout, w); src = dout, Cr = Co, N = Ci, output
-//         Hi x Wi, source Hs x Ws = Ho x Wo).
+// src (Nb, Cr, Hs, Ws) -> out (Nb, Ncol, Ho, Wo); tiles of 128 padded-grid rows, T per image
 template <int NT, int S, int MODE>
-__global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, const __nv_bfloat16 *w, const float *bias,
-                                                            float *out, int Mtot, int Cr, int Ncol, int Hs, int Ws,
-                                                            int Ho, int Wo, int Ci_w, int relu) {
+__global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const __nv_bfloat16 *w, const float *bias,
+                                                         float *out, int Cr, int Ncol, int Hs, int Ws, int Ho, int Wo,
+                                                         int Ci_w, int relu) {
     using namespace tc;
+    static_assert(MODE == 0 || S == 1, "the data gradient runs at stride 1 only");
     extern __shared__ __align__(1024) unsigned char tsm[];
-    unsigned char *Ahi = tsm, *Alo = tsm + 2 * A_BYTES, *Bs = tsm + 4 * A_BYTES;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * Smem<NT>::B_BYTES);
+    const int Wp = pitch(S, Wo), Hp = Ho + (S == 1 ? 2 : 1), R = rows(S, Wp);
+    const int ABYTES = a_bytes(S, Wp);                 // per stage, one part (hi or lo)
+    unsigned char *Ahi = tsm, *Alo = tsm + 2 * ABYTES, *Bs = tsm + 4 * ABYTES;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * B_<NT>::BYTES);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * BM;
-    const int HWo = Ho * Wo;
+    const int T = (Hp * Wp + BM - 1) / BM;             // tiles per image
+    const int n = blockIdx.x / T, q0 = (blockIdx.x % T) * BM;
+    const int lo_row = q0 - (Wp + 1);                  // padded-grid row of staged row 0
 
     if (warp == 0) {   // tensor-memory accumulator: NT columns x 128 lanes of float32
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -311,6 +322,7 @@ __global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, co
     const uint32_t tmem = *tmem_slot;
     constexpr uint32_t IDESC = umma_idesc_bf16(BM, NT);
     const int nchunks = (Cr + CC - 1) / CC;
+    const float *srcn = src + (size_t)n * Cr * Hs * Ws;
     bool ok = true;
 
     for (int c = 0; c < nchunks; ++c) {
@@ -323,37 +335,31 @@ __global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, co
             }
         }
         const int ch0 = c * CC;
-        // A: 2304 16-byte units (8 reduction elements of one pixel row each), hi and lo parts
-        for (int L = tid; L < BM * (KC / 8); L += THREADS) {
-            const int g = L / (KC / 8 * 8), rem = L % (KC / 8 * 8), c8 = rem >> 3, r = rem & 7;
-            const int mg = m0 + 8 * g + r;
-            float vals[8];
-            if (mg < Mtot) {
-                const int n = mg / HWo, p = mg - n * HWo, y = p / Wo, x = p - y * Wo;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int k = 8 * c8 + j, ch = ch0 + k / 9, tap = k % 9, ky = tap / 3, kx = tap % 3;
-                    float v = 0.f;
-                    if (ch < Cr) {
-                        int sy, sx;
-                        bool in;
-                        if constexpr (MODE == 0) {
-                            sy = S * y + ky - 1;
-                            sx = S * x + kx - 1;
-                            in = sy >= 0 && sy < Hs && sx >= 0 && sx < Ws;
-                        } else {
-                            const int ty = y + 1 - ky, tx = x + 1 - kx;
-                            sy = ty / S;
-                            sx = tx / S;
-                            in = ty >= 0 && tx >= 0 && ty % S == 0 && tx % S == 0 && sy < Hs && sx < Ws;
-                        }
-                        if (in) v = __ldg(src + (((size_t)n * Cr + ch) * Hs + sy) * Ws + sx);
-                    }
-                    vals[j] = v;
-                }
+        unsigned char *ah = Ahi + sb * ABYTES, *al = Alo + sb * ABYTES;
+        // A: per phase, R rows x two 8-channel halves; unit (phase, half, row) at
+        // ((phase * 2 + half) * R + row) * 16 bytes.  Consecutive threads take consecutive
+        // rows, so every channel plane is read in coalesced runs.
+        const int units = phases(S) * 2 * R;
+        for (int L = tid; L < units; L += THREADS) {
+            const int row = L % R, ph_half = L / R, half = ph_half & 1, ph = ph_half >> 1;
+            const int qg = lo_row + row, qy = qg / Wp, qx = qg - qy * Wp;   // qg may be negative: then outside
+            // source pixel of this staged row
+            int sy, sx;
+            bool in;
+            if constexpr (S == 1) {
+                sy = qy - 1;
+                sx = qx - 1;
+                in = qg >= 0 && qy >= 1 && qy <= Hs && qx >= 1 && qx <= Ws;
             } else {
+                sy = 2 * (qy - 1) + (ph >> 1);
+                sx = 2 * (qx - 1) + (ph & 1);
+                in = qg >= 0 && qy >= 1 && qx >= 1 && sy < Hs && sx < Ws;
+            }
+            float vals[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) vals[j] = 0.f;
+            for (int j = 0; j < 8; ++j) {
+                const int ch = ch0 + 8 * half + j;
+                vals[j] = (in && ch < Cr) ? __ldg(srcn + ((size_t)ch * Hs + sy) * Ws + sx) : 0.f;
             }
             uint32_t hi[4], lo[4];
 #pragma unroll
@@ -364,43 +370,56 @@ __global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, co
                 hi[j] = pack_bf16(h0, h1);
                 lo[j] = pack_bf16(l0, l1);
             }
-            *reinterpret_cast<uint4 *>(Ahi + sb * A_BYTES + L * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4 *>(Alo + sb * A_BYTES + L * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            *reinterpret_cast<uint4 *>(ah + L * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4 *>(al + L * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
         }
-        // B: NT rows of the weights for this chunk
-        for (int L = tid; L < NT * (KC / 8); L += THREADS) {
-            const int g = L / (KC / 8 * 8), rem = L % (KC / 8 * 8), c8 = rem >> 3, r = rem & 7;
-            const int col = 8 * g + r;
+        // B: per tap, NT rows x two 8-channel halves; unit (tap, half, col) at ((tap * 2 + half) * NT + col) * 16
+        unsigned char *bsb = Bs + sb * B_<NT>::BYTES;
+        for (int L = tid; L < 9 * 2 * NT; L += THREADS) {
+            const int col = L % NT, tap_half = L / NT, half = tap_half & 1, tap = tap_half >> 1;
             uint32_t wv[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 __nv_bfloat16 e[2];
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int k = 8 * c8 + 2 * j + h, ch = ch0 + k / 9, tap = k % 9;
+                    const int ch = ch0 + 8 * half + 2 * j + h;
                     e[h] = __float2bfloat16_rn(0.f);
                     if (ch < Cr && col < Ncol) {
-                        // forward: w[co = col][ci = ch]; data gradient: w[co = ch][ci = col]
-                        const size_t idx = MODE == 0 ? ((size_t)col * Ci_w + ch) * 9 + tap : ((size_t)ch * Ci_w + col) * 9 + tap;
-                        e[h] = w[idx];
+                        // forward: w[co = col][ci = ch][tap]; data gradient: w[co = ch][ci = col][tap]
+                        // (its A operand is shifted by the mirrored tap offset)
+                        e[h] = MODE == 0 ? w[((size_t)col * Ci_w + ch) * 9 + tap] : w[((size_t)ch * Ci_w + col) * 9 + tap];
                     }
                 }
                 wv[j] = pack_bf16(e[0], e[1]);
             }
-            *reinterpret_cast<uint4 *>(Bs + sb * Smem<NT>::B_BYTES + L * 16) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            *reinterpret_cast<uint4 *>(bsb + L * 16) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
         }
         // generic-proxy writes -> visible to the tensor cores (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a_hi = smem_u32(Ahi + sb * A_BYTES), a_lo = smem_u32(Alo + sb * A_BYTES);
-            const uint32_t b0 = smem_u32(Bs + sb * Smem<NT>::B_BYTES);
+            const uint32_t a_hi = smem_u32(ah), a_lo = smem_u32(al), b0 = smem_u32(bsb);
+            const uint32_t lbo_a = (uint32_t)R * 16, lbo_b = (uint32_t)NT * 16;
 #pragma unroll 1
-            for (int j = 0; j < KSTEPS; ++j) {
-                const uint64_t db = umma_desc(b0 + 256 * j);
-                umma_bf16(tmem, umma_desc(a_hi + 256 * j), db, IDESC, (c > 0 || j > 0) ? 1u : 0u);
-                umma_bf16(tmem, umma_desc(a_lo + 256 * j), db, IDESC, 1u);
+            for (int tap = 0; tap < 9; ++tap) {
+                const int ky = tap / 3, kx = tap % 3;
+                int ph = 0, start;
+                if constexpr (S == 1) {
+                    // output row m reads padded row q0 + m + (ky - 1) Wp + (kx - 1) (mirrored for the data gradient)
+                    const int dy = MODE == 0 ? ky - 1 : 1 - ky, dx = MODE == 0 ? kx - 1 : 1 - kx;
+                    start = Wp + 1 + dy * Wp + dx;
+                } else {
+                    // input row 2y + ky - 1: phase (ky + 1) & 1 at phase row y - (ky == 0)
+                    const int py = (ky + 1) & 1, px = (kx + 1) & 1, dy = ky == 0 ? -1 : 0, dx = kx == 0 ? -1 : 0;
+                    ph = 2 * py + px;
+                    start = Wp + 1 + dy * Wp + dx;
+                }
+                const uint32_t aoff = (uint32_t)((ph * 2 * R + start) * 16);
+                const uint64_t db = umma_desc(b0 + (uint32_t)(tap * 2 * NT * 16), lbo_b);
+                umma_bf16(tmem, umma_desc(a_hi + aoff, lbo_a), db, IDESC, (c > 0 || tap > 0) ? 1u : 0u);
+                umma_bf16(tmem, umma_desc(a_lo + aoff, lbo_a), db, IDESC, 1u);
             }
             umma_commit(&mbar[sb]);
         }
@@ -415,13 +434,14 @@ __global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, co
     tc_fence_after();
     // accumulator -> registers: warp w reads lanes 32 (w % 4) .. +31, columns of half w / 4
     {
-        const int q = warp & 3, half = warp >> 2;
-        const int m = 32 * q + lane, mg = m0 + m;
+        const int qd = warp & 3, halfc = warp >> 2;
+        const int m = 32 * qd + lane, qg = q0 + m, qy = qg / Wp, qx = qg - qy * Wp;
+        const int y = qy - 1, x = qx - 1;   // the padded grid's first row and column are halo
         constexpr int COLS = NT / 2;
         uint32_t r[COLS];
 #pragma unroll
         for (int c16 = 0; c16 < COLS / 16; ++c16) {
-            const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(half * COLS + 16 * c16);
+            const uint32_t taddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(halfc * COLS + 16 * c16);
             uint32_t *d = r + 16 * c16;
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
                          "%12, %13, %14, %15}, [%16];"
@@ -431,18 +451,17 @@ __global__ void __launch_bounds__(tc::THREADS, 1) k_conv_tc(const float *src, co
                          : "r"(taddr));
         }
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (mg < Mtot) {
-            const int n = mg / HWo, p = mg - n * HWo;
+        if (y >= 0 && y < Ho && x >= 0 && x < Wo) {   // a real output pixel (not a halo row / column)
 #pragma unroll
             for (int j = 0; j < COLS; ++j) {
-                const int col = half * COLS + j;
+                const int col = halfc * COLS + j;
                 if (col >= Ncol) break;
                 float v = ok ? __uint_as_float(r[j]) : __int_as_float(0x7fc00000);
                 if constexpr (MODE == 0) {
                     v += bias[col];
                     if (relu) v = fmaxf(v, 0.f);
                 }
-                out[((size_t)n * Ncol + col) * HWo + p] = v;
+                out[(((size_t)n * Ncol + col) * Ho + y) * Wo + x] = v;
             }
         }
     }
@@ -605,30 +624,26 @@ static void launch_bwd_data(const float *dout, const __nv_bfloat16 *w, float *di
 }
 
 // the tensor-core form serves GEMM widths (output channels) of 32 and 64
-template <int S, int MODE>
-static int launch_conv_tc(const float *src, const __nv_bfloat16 *w, const float *bias, float *out, int Mtot, int Cr,
-                          int Ncol, int Hs, int Ws, int Ho, int Wo, int Ci_w, int relu, cudaStream_t st) {
-    const unsigned grid = (unsigned)((Mtot + tc::BM - 1) / tc::BM);
-    if (Ncol <= 32) {
-        auto k = k_conv_tc<32, S, MODE>;
-        static bool cfg = false;
-        if (!cfg) {
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::Smem<32>::TOTAL) != cudaSuccess)
-                return record_cuda(cudaGetLastError());
-            cfg = true;
-        }
-        k<<<grid, tc::THREADS, tc::Smem<32>::TOTAL, st>>>(src, w, bias, out, Mtot, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu);
-    } else {
-        auto k = k_conv_tc<64, S, MODE>;
-        static bool cfg = false;
-        if (!cfg) {
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::Smem<64>::TOTAL) != cudaSuccess)
-                return record_cuda(cudaGetLastError());
-            cfg = true;
-        }
-        k<<<grid, tc::THREADS, tc::Smem<64>::TOTAL, st>>>(src, w, bias, out, Mtot, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu);
-    }
+template <int NT, int S, int MODE>
+static int launch_conv_tc_n(const float *src, const __nv_bfloat16 *w, const float *bias, float *out, int Nb, int Cr,
+                            int Ncol, int Hs, int Ws, int Ho, int Wo, int Ci_w, int relu, cudaStream_t st) {
+    const int Wp = tc::pitch(S, Wo), Hp = Ho + (S == 1 ? 2 : 1);
+    const int smem = 4 * tc::a_bytes(S, Wp) + 2 * tc::B_<NT>::BYTES + 64;
+    if (smem > 200 * 1024) return PHB_ERR_UNSUPPORTED;   // wider images than this network uses
+    const long long tiles = (long long)Nb * ((Hp * Wp + tc::BM - 1) / tc::BM);
+    if (tiles > 0x7fffffffll) return PHB_ERR_UNSUPPORTED;
+    auto k = k_conv_tc<NT, S, MODE>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return record_cuda(cudaGetLastError());
+    k<<<(unsigned)tiles, tc::THREADS, smem, st>>>(src, w, bias, out, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu);
     return check_launch();
+}
+
+template <int S, int MODE>
+static int launch_conv_tc(const float *src, const __nv_bfloat16 *w, const float *bias, float *out, int Nb, int Cr,
+                          int Ncol, int Hs, int Ws, int Ho, int Wo, int Ci_w, int relu, cudaStream_t st) {
+    return Ncol <= 32 ? launch_conv_tc_n<32, S, MODE>(src, w, bias, out, Nb, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu, st)
+                      : launch_conv_tc_n<64, S, MODE>(src, w, bias, out, Nb, Cr, Ncol, Hs, Ws, Ho, Wo, Ci_w, relu, st);
 }
 
 static bool tc_width(int n) { return n == 32 || n == 64; }
@@ -643,10 +658,9 @@ int phb_conv3x3_fwd(const float *in, const void *w_bf16, const float *bias, floa
     const int Ho = Hi / stride, Wo = Wi / stride;
     const __nv_bfloat16 *w = (const __nv_bfloat16 *)w_bf16;
     cudaStream_t st = (cudaStream_t)stream;
-    const int64_t Mtot = (int64_t)Nb * Ho * Wo;
-    if (tc_width(Co) && Mtot < (1ll << 31)) {   // tensor cores (tcgen05): 32 or 64 output channels
-        return stride == 1 ? launch_conv_tc<1, 0>(in, w, bias, out, (int)Mtot, Ci, Co, Hi, Wi, Ho, Wo, Ci, relu, st)
-                           : launch_conv_tc<2, 0>(in, w, bias, out, (int)Mtot, Ci, Co, Hi, Wi, Ho, Wo, Ci, relu, st);
+    if (tc_width(Co) && Wo <= 64) {   // tensor cores (tcgen05): 32 or 64 output channels
+        return stride == 1 ? launch_conv_tc<1, 0>(in, w, bias, out, Nb, Ci, Co, Hi, Wi, Ho, Wo, Ci, relu, st)
+                           : launch_conv_tc<2, 0>(in, w, bias, out, Nb, Ci, Co, Hi, Wi, Ho, Wo, Ci, relu, st);
     }
     if (Co <= 2) {
         if (stride == 1) launch_fwd<2, 1>(in, w, bias, out, Nb, Ci, Hi, Wi, Co, Ho, Wo, relu, st);
@@ -666,10 +680,8 @@ int phb_conv3x3_bwd_data(const float *dout, const void *w_bf16, float *din, int3
     const int Ho = Hi / stride, Wo = Wi / stride;
     const __nv_bfloat16 *w = (const __nv_bfloat16 *)w_bf16;
     cudaStream_t st = (cudaStream_t)stream;
-    const int64_t Mtot = (int64_t)Nb * Hi * Wi;
-    if (tc_width(Ci) && Mtot < (1ll << 31)) {   // tensor cores: the GEMM width is the input-channel count
-        return stride == 1 ? launch_conv_tc<1, 1>(dout, w, nullptr, din, (int)Mtot, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st)
-                           : launch_conv_tc<2, 1>(dout, w, nullptr, din, (int)Mtot, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st);
+    if (tc_width(Ci) && stride == 1 && Wi <= 64) {   // tensor cores: the GEMM width is the input-channel count
+        return launch_conv_tc<1, 1>(dout, w, nullptr, din, Nb, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st);
     }
     if (stride == 1) launch_bwd_data<16, 1>(dout, w, din, Nb, Ci, Hi, Wi, Co, Ho, Wo, st);
     else launch_bwd_data<16, 2>(dout, w, din, Nb, Ci, Hi, Wi, Co, Ho, Wo, st);
