@@ -316,7 +316,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     const float inv_n = 1.0f / (float)N, inv_nn = 1.0f / (float)NN;
 
     float2 v[U][E];
-    // propagator of slice gap g (and this position's tilt ramp) into py/px
+    // propagator of slice gap g (and this position's tilt ramp) into py/px; px carries the
+    // 1/N^2 of the unnormalised transform pair, so the propagation multiply needs no scaling
     auto load_prop = [&](int g) {
         const float2 *src = a.prop1d + (size_t)g * 2 * N;
         for (int k = tid; k < 2 * N; k += blockDim.x) {
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 sincospif(2.0f * (dz * (t * f)), &sn, &cs);
                 p = cmul(p, make_float2(cs, sn));
             }
-            py[k] = p;   // py[0..N) then px[0..N): contiguous
+            py[k] = k < N ? p : cscale(p, inv_nn);   // py[0..N) then px[0..N): contiguous
         }
         __syncthreads();
     };
@@ -509,7 +510,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int e = 0; e < E; ++e) {
                     const int ky = I::ky(u, e), kx = I::kx(u, e);
                     const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
-                    v[u][e] = cscale(cmul(v[u][e], p), inv_nn);
+                    v[u][e] = cmul(v[u][e], p);
                 }
             fwd = false;
             phase = PH_START;
@@ -827,7 +828,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int e = 0; e < E; ++e) {
                     const int ky = I::ky(u, e), kx = I::kx(u, e);
                     const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
-                    v[u][e] = cscale(cmulc(v[u][e], p), inv_nn);
+                    v[u][e] = cmulc(v[u][e], p);
                 }
             fwd = false;
             phase = PH_BACK;
@@ -841,7 +842,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 for (int e = 0; e < E; ++e) {
                     const int ky = I::ky(u, e), kx = I::kx(u, e);
                     const float2 p = ((kband >> (u * E + e)) & 1ull) ? cmul(py[ky], px[kx]) : make_float2(0.f, 0.f);
-                    v[u][e] = cscale(cmulc(v[u][e], p), inv_nn);
+                    v[u][e] = cmulc(v[u][e], p);
                 }
             fwd = false;
             phase = PH_BACK;

@@ -27,10 +27,9 @@
 //   real space: CTA rank q = 2 a + b holds the quadrant x[128 a + y', 128 b + x'] in the
 //   N = 128 R layout of (y', x');  Fourier space: it holds the polyphase component
 //   X[2 ky' + a, 2 kx' + b] in the N = 128 K layout of (ky', kx').  The forward transform
-//   is one radix-2 x 2 decimation-in-frequency stage across the cluster -- each CTA
-//   publishes its quadrant in shared memory, combines the four quadrants at its own
-//   register slots through distributed shared memory (signs (-1)^(ac + bd)) and applies
-//   the twiddle W256^(c y' + d x') -- followed by the CTA's own 128 x 128 transform; the
+//   is one radix-2 x 2 decimation-in-frequency stage across the cluster -- two pairwise
+//   radix-2 exchanges through distributed shared memory (signs (-1)^(ac + bd)) and the
+//   twiddle W256^(c y' + d x') -- followed by the CTA's own 128 x 128 transform; the
 //   inverse runs the same steps in reverse order with conjugate twiddles.
 //
 // N = 64 (8 values per thread, three exchanges): a line FFT of length
@@ -170,28 +169,6 @@ __device__ __forceinline__ float2 tw32(float2 a, int j) {
     return cmul(a, make_float2(c, INV ? s : -s));
 }
 
-// 32-point DFT in place, natural order: n = n2 + 8 n1, k = k1 + 4 k2
-// (DFT-4 over n1, twiddle W32^{n2 k1}, DFT-8 over n2).
-template <bool INV>
-__device__ __forceinline__ void dft32(float2 *x) {
-#pragma unroll
-    for (int n2 = 0; n2 < 8; ++n2) dft4<INV>(x[n2], x[n2 + 8], x[n2 + 16], x[n2 + 24]);
-#pragma unroll
-    for (int k1 = 1; k1 < 4; ++k1)
-#pragma unroll
-        for (int n2 = 1; n2 < 8; ++n2) x[n2 + 8 * k1] = tw32<INV>(x[n2 + 8 * k1], n2 * k1);
-#pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1) dft8<INV>(&x[8 * k1]);
-    // slot 8 k1 + k2 holds X[k1 + 4 k2]
-    float2 t[32];
-#pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1)
-#pragma unroll
-        for (int k2 = 0; k2 < 8; ++k2) t[k1 + 4 * k2] = x[8 * k1 + k2];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) x[i] = t[i];
-}
-
 // --------------------------------------------------------------- addressing
 // Every shared-memory access below is (per-thread base) + (compile-time
 // offset), so the compiler keeps a handful of base registers instead of one
@@ -264,25 +241,25 @@ __device__ __forceinline__ void fft128_r2k(float2 (&v)[1][32], float2 *xb, const
         const int xt = t & 31, yt = t >> 5;
 #pragma unroll
         for (int m = 0; m < 8; ++m) dft4<false>(x[m], x[8 + m], x[16 + m], x[24 + m]);   // j -> k1
+        float2 wy[8];
 #pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) dft8<false>(&x[8 * k1]);                         // m -> ky2
-#pragma unroll
-        for (int k1 = 1; k1 < 4; ++k1) {
-            const float2 w = twid[xt * k1];
-#pragma unroll
-            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
-        }
-#pragma unroll
-        for (int ky2 = 1; ky2 < 8; ++ky2) {
-            const float2 w = twid[yt * ky2];
-#pragma unroll
-            for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
-        }
+        for (int ky2 = 1; ky2 < 8; ++ky2) wy[ky2] = twid[yt * ky2];
         float2 *wb = xb + yt * S1 + xt;                     // row yt + 16 (ky2 + 8 k1)
+        // each k1 group is finished and stored before the next is transformed, so the
+        // exchange stores of one group overlap the arithmetic of the next
 #pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1)
+        for (int k1 = 0; k1 < 4; ++k1) {
+            dft8<false>(&x[8 * k1]);                                                     // m -> ky2
+            if (k1 > 0) {
+                const float2 w = twid[xt * k1];
+#pragma unroll
+                for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], w);
+            }
+#pragma unroll
+            for (int ky2 = 1; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmul(x[8 * k1 + ky2], wy[ky2]);
 #pragma unroll
             for (int ky2 = 0; ky2 < 8; ++ky2) wb[16 * (ky2 + 8 * k1) * S1] = x[8 * k1 + ky2];
+        }
     }
     __syncthreads();
     {   // pass B: this thread's row t, DFT-32 over xt
@@ -291,12 +268,22 @@ __device__ __forceinline__ void fft128_r2k(float2 (&v)[1][32], float2 *xb, const
         for (int i = 0; i < 32; ++i) x[i] = rb[i];
     }
     __syncthreads();
-    dft32<false>(x);
-    {
+    {   // DFT-32 (n = n2 + 8 n1, k = k1' + 4 k2') with each DFT-8 group's outputs stored as
+        // soon as they are final: row 128 ky2 + kx, kx = k1 + 4 k, k = k1' + 4 k2'
         const int yt = t & 15, ky2 = (t >> 4) & 7, k1 = t >> 7;
-        float2 *wb = xb + (ky2 * 128 + k1) * S2 + yt;       // row 128 ky2 + kx, kx = k1 + 4 k2
+        float2 *wb = xb + (ky2 * 128 + k1) * S2 + yt;
 #pragma unroll
-        for (int k2 = 0; k2 < 32; ++k2) wb[4 * k2 * S2] = x[k2];
+        for (int n2 = 0; n2 < 8; ++n2) dft4<false>(x[n2], x[n2 + 8], x[n2 + 16], x[n2 + 24]);
+#pragma unroll
+        for (int g = 1; g < 4; ++g)
+#pragma unroll
+            for (int n2 = 1; n2 < 8; ++n2) x[n2 + 8 * g] = tw32<false>(x[n2 + 8 * g], n2 * g);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            dft8<false>(&x[8 * g]);                           // slot 8 g + k2' holds X[g + 4 k2']
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2) wb[4 * (g + 4 * k2) * S2] = x[8 * g + k2];
+        }
     }
     __syncthreads();
     {   // pass C: DFT-16 over yt for two columns
@@ -306,9 +293,9 @@ __device__ __forceinline__ void fft128_r2k(float2 (&v)[1][32], float2 *xb, const
 #pragma unroll
             for (int y = 0; y < 16; ++y) x[16 * c + y] = rb[64 * c * S2 + y];
     }
-    __syncthreads();
     dft16<false>(&x[0]);
     dft16<false>(&x[16]);
+    __syncthreads();   // every read of the exchange buffer is done before its next writer
 }
 
 // Inverse (unnormalised): K layout in, R layout out.
@@ -316,14 +303,14 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
     constexpr int S1 = Lay<128>::S1, S2 = Lay<128>::S2;
     const int t = threadIdx.x;
     float2 *x = v[0];
-    dft16<true>(&x[0]);                                     // pass C: ky1 -> yt
-    dft16<true>(&x[16]);
-    {
+    {   // pass C: ky1 -> yt, each column stored once transformed
         float2 *wb = xb + ((t >> 6) * 128 + (t & 63)) * S2;
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
+        for (int c = 0; c < 2; ++c) {
+            dft16<true>(&x[16 * c]);
 #pragma unroll
             for (int y = 0; y < 16; ++y) wb[64 * c * S2 + y] = x[16 * c + y];
+        }
     }
     __syncthreads();
     {   // pass B: k2 -> xt
@@ -333,35 +320,43 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
         for (int k2 = 0; k2 < 32; ++k2) x[k2] = rb[4 * k2 * S2];
     }
     __syncthreads();
-    dft32<true>(x);
-    {
+    {   // inverse DFT-32, each DFT-8 group's outputs stored as soon as they are final
         float2 *wb = xb + t * S1;
 #pragma unroll
-        for (int i = 0; i < 32; ++i) wb[i] = x[i];
+        for (int n2 = 0; n2 < 8; ++n2) dft4<true>(x[n2], x[n2 + 8], x[n2 + 16], x[n2 + 24]);
+#pragma unroll
+        for (int g = 1; g < 4; ++g)
+#pragma unroll
+            for (int n2 = 1; n2 < 8; ++n2) x[n2 + 8 * g] = tw32<true>(x[n2 + 8 * g], n2 * g);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            dft8<true>(&x[8 * g]);                            // slot 8 g + k2' holds X[g + 4 k2']
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2) wb[g + 4 * k2] = x[8 * g + k2];
+        }
     }
     __syncthreads();
     {   // pass A: conj twiddles, ky2 -> m, k1 -> j
         const int xt = t & 31, yt = t >> 5;
         const float2 *rb = xb + yt * S1 + xt;
+        float2 wy[8];
 #pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1)
+        for (int ky2 = 1; ky2 < 8; ++ky2) wy[ky2] = twid[yt * ky2];
+        // group by group: the exchange loads of the next k1 group overlap this group's arithmetic
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
 #pragma unroll
             for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = rb[16 * (ky2 + 8 * k1) * S1];
+#pragma unroll
+            for (int ky2 = 1; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], wy[ky2]);
+            if (k1 > 0) {
+                const float2 w = twid[xt * k1];
+#pragma unroll
+                for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
+            }
+            dft8<true>(&x[8 * k1]);                                                      // ky2 -> m
+        }
         __syncthreads();
-#pragma unroll
-        for (int ky2 = 1; ky2 < 8; ++ky2) {
-            const float2 w = twid[yt * ky2];
-#pragma unroll
-            for (int k1 = 0; k1 < 4; ++k1) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
-        }
-#pragma unroll
-        for (int k1 = 1; k1 < 4; ++k1) {
-            const float2 w = twid[xt * k1];
-#pragma unroll
-            for (int ky2 = 0; ky2 < 8; ++ky2) x[8 * k1 + ky2] = cmulc(x[8 * k1 + ky2], w);
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) dft8<true>(&x[8 * k1]);                          // ky2 -> m
 #pragma unroll
         for (int m = 0; m < 8; ++m) dft4<true>(x[m], x[8 + m], x[16 + m], x[24 + m]);    // k1 -> j
     }
@@ -369,39 +364,43 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
 
 // ------------------------------------------------- N = 256: 4-CTA cluster form
 // Radix-2 x 2 stage across the cluster at every register slot: this CTA (rank
-// 2 c + d) gets sum over ranks 2 a + b of (-1)^(a c + b d) x_ab.  Both sides of
-// both cluster barriers: the first publishes every CTA's values, the second keeps
-// each CTA's buffer intact until all remote reads of it are done.
-__device__ __forceinline__ void quad_butterfly(float2 (&v)[1][32], float2 *xb) {
+// 2 c + d) gets sum over ranks 2 a + b of (-1)^(a c + b d) x_ab.  It runs as two
+// pairwise radix-2 steps (partner rank q ^ 2, then q ^ 1), so a CTA reads 2 x 128 KB of
+// its partners' shared memory instead of 3 x 128 KB, in 16-byte loads.  Each step: every
+// CTA publishes its values (two register slots per float4), a cluster barrier, the
+// partner's values are read at the same slots, and a second barrier keeps each buffer
+// intact until its partner has read it.
+__device__ __forceinline__ void quad_pair_step(float2 (&v)[1][32], float2 *xb, int partner, bool upper) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     const int t = threadIdx.x;
     float2 *x = v[0];
+    float4 *mine = reinterpret_cast<float4 *>(xb);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) xb[i * 512 + t] = x[i];
+    for (int j = 0; j < 16; ++j) mine[j * 512 + t] = make_float4(x[2 * j].x, x[2 * j].y, x[2 * j + 1].x, x[2 * j + 1].y);
     cl.sync();
-    const int q = cluster_rank() & 3;
-    const float sy = (q & 2) ? -1.f : 1.f, sx = (q & 1) ? -1.f : 1.f;
-    const float2 *r0 = cl.map_shared_rank(xb, 0) + t, *r1 = cl.map_shared_rank(xb, 1) + t;
-    const float2 *r2 = cl.map_shared_rank(xb, 2) + t, *r3 = cl.map_shared_rank(xb, 3) + t;
+    const float4 *theirs = cl.map_shared_rank(mine, partner) + t;
+    // lower rank of the pair: x_own + x_partner; upper: x_partner - x_own
+    const float so = upper ? -1.f : 1.f;
 #pragma unroll
-    for (int i0 = 0; i0 < 32; i0 += 4) {
-        float2 a[4], b[4], c[4], d[4];
+    for (int j0 = 0; j0 < 16; j0 += 4) {
+        float4 p[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            a[j] = r0[(i0 + j) * 512];
-            b[j] = r1[(i0 + j) * 512];
-            c[j] = r2[(i0 + j) * 512];
-            d[j] = r3[(i0 + j) * 512];
-        }
+        for (int j = 0; j < 4; ++j) p[j] = theirs[(j0 + j) * 512];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float2 top = make_float2(fmaf(sx, b[j].x, a[j].x), fmaf(sx, b[j].y, a[j].y));
-            const float2 bot = make_float2(fmaf(sx, d[j].x, c[j].x), fmaf(sx, d[j].y, c[j].y));
-            x[i0 + j] = make_float2(fmaf(sy, bot.x, top.x), fmaf(sy, bot.y, top.y));
+            float2 &e0 = x[2 * (j0 + j)], &e1 = x[2 * (j0 + j) + 1];
+            e0 = make_float2(fmaf(so, e0.x, p[j].x), fmaf(so, e0.y, p[j].y));
+            e1 = make_float2(fmaf(so, e1.x, p[j].z), fmaf(so, e1.y, p[j].w));
         }
     }
     cl.sync();
+}
+
+__device__ __forceinline__ void quad_butterfly(float2 (&v)[1][32], float2 *xb) {
+    const int q = cluster_rank() & 3;
+    quad_pair_step(v, xb, q ^ 2, (q & 2) != 0);   // rows: a <-> c
+    quad_pair_step(v, xb, q ^ 1, (q & 1) != 0);   // columns: b <-> d
 }
 
 // multiply slot i (real-space position (y', x') of the N = 128 R layout) by

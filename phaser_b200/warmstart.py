@@ -61,19 +61,19 @@ class FeatureSpec:
 
 
 DEFAULT_FEATURES = FeatureSpec()
-TRAIN_N = 128   # detector side of the training patterns
 
 
-def features_for(spec: FeatureSpec, N: int) -> FeatureSpec:
-    """The feature window for N^2 patterns of the training pixel size in real space: a
-    detector of N > TRAIN_N pixels samples reciprocal space N / TRAIN_N times finer, so
-    the window covers N / TRAIN_N times more pixels, binned by that factor -- the same
-    angular range at the same resolution the network was trained on."""
-    if N == TRAIN_N:
+def features_for(spec: FeatureSpec, N: int, train_n: int = 128) -> FeatureSpec:
+    """The feature window for N^2 patterns of the training pixel size in real space, for a
+    network trained on train_n^2 patterns with window `spec`: a detector of N > train_n
+    pixels samples reciprocal space N / train_n times finer, so the window covers
+    N / train_n times more pixels, binned by that factor -- the same angular range at the
+    same resolution the network was trained on."""
+    if N == train_n:
         return spec
-    if N % TRAIN_N:
-        raise ValueError(f"no feature window for {N}^2 patterns (a multiple of {TRAIN_N} is needed)")
-    f = N // TRAIN_N
+    if N < train_n or N % train_n:
+        raise ValueError(f"no feature window for {N}^2 patterns from a network trained on {train_n}^2")
+    f = N // train_n
     return dataclasses.replace(spec, crop=spec.crop * f, bin=spec.bin * f)
 
 
@@ -86,9 +86,10 @@ class WarmStartNet:
     gradients, Adam state and activation buffers, all on one device."""
 
     def __init__(self, seed: int = 0, device: t.Union[str, torch.device] = 'cuda',
-                 features: FeatureSpec = DEFAULT_FEATURES):
+                 features: FeatureSpec = DEFAULT_FEATURES, train_n: int = 128):
         self.device = torch.device(device)
         self.features = features
+        self.train_n = train_n   # detector side of the patterns the network is trained on
         rng = numpy.random.default_rng(seed)
         self.w, self.b, self.wq, self.gw, self.gb, self.m, self.v = [], [], [], [], [], [], []
         for (ci, co, *_r) in LAYERS:
@@ -235,25 +236,36 @@ def lattice_phase_fast(shape: t.Tuple[int, int], spacing: float, sigma: float, p
     return numpy.bincount((ys * W + xs)[ok], weights=vals[ok], minlength=H * W).reshape(H, W)
 
 
-def lattice_geometry(scan: int = 32, seed: int = 0):
-    """The multislice LSQ-ML configuration's optics and scan geometry (128^2 probe at
-    0.2 A/px, 25 mrad, 300 kV, 200 A defocus, 4 Hermite modes holding 70/15/10/5 %,
-    6 px steps, 1e6 e- per pattern) on a scan x scan raster: a Dataset whose object
-    the training loop replaces."""
+def lattice_geometry(scan: int = 32, seed: int = 0, geometry: str = 'multislice'):
+    """Optics and scan geometry of the training data on a scan x scan raster: a Dataset
+    whose object the training loop replaces.
+      'multislice': the multislice LSQ-ML configuration (128^2 probe at 0.2 A/px, 25 mrad,
+                    300 kV, 200 A defocus, 4 Hermite modes holding 70/15/10/5 %, 6 px steps,
+                    1e6 e- per pattern);
+      'single':     the single-slice configuration's optics (64^2 probe at 0.2 A/px,
+                    20 mrad, 200 kV, 100 A defocus, 1 mode, 4 px steps with +-0.5 px
+                    jitter, 1e5 e- per pattern), used for multislice objects here."""
     from .synthetic import make_dataset
+    if geometry == 'single':
+        return make_dataset(N=64, M=1, S=1, scan_shape=(scan, scan), step_px=4.0, sampling=0.2, kv=200e3,
+                            conv_mrad=20.0, defocus=100.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
+                            peak_rad=0.0, counts=1e5, scan_jitter_px=0.5, seed=seed)
+    if geometry != 'multislice':
+        raise ValueError(f"unknown training geometry '{geometry}'")
     return make_dataset(N=128, M=4, S=1, scan_shape=(scan, scan), step_px=6.0, sampling=0.2, kv=300e3,
                         conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
                         peak_rad=0.0, counts=1e6, mode_powers=(0.70, 0.15, 0.10, 0.05), seed=seed)
 
 
 def random_lattice_objects(n: int, *, seed: int = 0, scan: int = 32, slices: t.Tuple[int, int] = (4, 12),
-                           peak: t.Tuple[float, float] = (0.1, 0.5), spacing: t.Tuple[float, float] = (6., 14.)):
-    """Yield n training datasets on lattice_geometry(scan): each with 4-12 slices of 2 nm,
-    every slice an independently shifted Gaussian-atom lattice (sigma 1.5 px) of one
-    random spacing (6-14 px) and peak phase (0.1-0.5 rad).  The same Dataset object is
+                           peak: t.Tuple[float, float] = (0.1, 0.5), spacing: t.Tuple[float, float] = (6., 14.),
+                           geometry: str = 'multislice'):
+    """Yield n training datasets on lattice_geometry(scan, geometry): each with 4-12 slices
+    of 2 nm, every slice an independently shifted Gaussian-atom lattice (sigma 1.5 px) of
+    one random spacing (6-14 px) and peak phase (0.1-0.5 rad).  The same Dataset object is
     reused: consume each before drawing the next."""
     rng = numpy.random.default_rng(seed)
-    ds = lattice_geometry(scan, seed)
+    ds = lattice_geometry(scan, seed, geometry)
     H, W = ds.true_object.shape[-2:]
     for _ in range(n):
         S = int(rng.integers(slices[0], slices[1] + 1))
@@ -311,7 +323,8 @@ def patch_targets(ds, pats: torch.Tensor) -> torch.Tensor:
 def training_set(n_objects: int, *, seed: int = 0, scan: int = 32, slices: t.Tuple[int, int] = (4, 12),
                  spec: FeatureSpec = DEFAULT_FEATURES, device='cuda', **objects):
     """(features, targets) of n_objects random-lattice objects x scan^2 positions, the
-    patterns simulated by the fused forward kernel with Poisson noise."""
+    patterns simulated by the fused forward kernel with Poisson noise; `objects` passes
+    spacing / peak / geometry to random_lattice_objects."""
     from .synthetic import simulate_patterns
     fs, ts = [], []
     for k, ds in enumerate(random_lattice_objects(n_objects, seed=seed, scan=scan, slices=slices, **objects)):
@@ -396,7 +409,7 @@ def warm_start_object(net: WarmStartNet, eng, pats: torch.Tensor, scan: numpy.nd
     sub = pats.reshape(-1, *pats.shape[-2:])
     if len(idx) != flat_scan.shape[0]:
         sub = _as_f32(sub, torch.from_numpy(idx).to(pats.device))
-    feats = pattern_features(sub, features_for(net.features, eng.N))
+    feats = pattern_features(sub, features_for(net.features, eng.N, getattr(net, 'train_n', 128)))
     proj = stitch(net, feats, flat_scan[idx], eng.obj_sampling, (H, W), eng.N, window_sigma)
     r_flat = pattern_residual(eng, eng.object, residual_stride)
     best = None
