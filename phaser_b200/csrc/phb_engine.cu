@@ -6,15 +6,21 @@
 // phaser/engines/common/simulation.py:160-306 and phaser/utils/object.py.
 //
 // Design (sm_100a):
-//  * one CTA of 512 threads per (position b, probe mode m); the M CTAs of a
-//    position form a thread-block cluster and exchange per-pixel mode sums
-//    (illumination, far-field intensity, object-update numerators) through
-//    distributed shared memory, so every global atomic is issued once per
-//    position rather than once per mode;
-//  * each CTA keeps its N x N wavefield in registers for the whole forward
-//    and adjoint pass (phb_fft.cuh), multiplying cutouts and propagators in
-//    as it goes; only the per-slice incident waves travel to HBM (for the
-//    adjoint) -- the minimum traffic of the algorithm;
+//  * one CTA of 512 threads per (position b, probe mode m); each CTA keeps its
+//    N x N wavefield in registers for the whole forward and adjoint pass
+//    (phb_fft.cuh), multiplying cutouts and propagators in as it goes; only the
+//    per-slice incident waves travel to HBM (for the adjoint) -- the minimum
+//    traffic of the algorithm;
+//  * the modes of a position meet only at the detector (the intensity is their
+//    sum).  LSQ-ML and the gradient engine split the step there into two launches:
+//    the forward launch stores Psi_m = fft2(exit wave) / N and adds |Psi_m / N|^2
+//    into a per-position intensity buffer with float32 atomics; the second launch
+//    resumes at the detector with the summed intensity and runs the constraint and
+//    the adjoint.  The CTAs of a launch are independent, so they run without
+//    clusters on every SM (a 4-CTA cluster fits only 4 of a GPC's SMs per 4: 132
+//    of 148 SMs).  ePIE keeps the M CTAs of a position in one cluster: its far
+//    field and its per-slice maximum over the modes go through distributed shared
+//    memory;
 //  * object / probe updates are accumulated during the pass and applied by
 //    small follow-up kernels once the group-global step sizes are known
 //    (the reference applies them slice by slice, but its cutouts are copies
@@ -23,11 +29,7 @@
 //    accumulated in float64 (block reduce, then one float64 atomic per CTA);
 //  * N = 256: a tile needs four SMs (512 KB of complex64), so a cluster of 4 CTAs
 //    holds one (position, mode), one quadrant / polyphase component each (the
-//    4-CTA transform of phb_fft.cuh).  The modes of a position are then in
-//    different clusters, so the far field is split over two launches: the forward
-//    launch stores Psi_m = fft2(exit wave) and adds |Psi_m|^2 into a per-position
-//    intensity buffer; the second launch resumes at the detector with the summed
-//    intensity and runs the constraint and the adjoint.
+//    4-CTA transform of phb_fft.cuh), with the same two-launch far field.
 #include <cooperative_groups.h>
 
 #include "phb_fft.cuh"
@@ -77,8 +79,8 @@ struct Workspace {
     int32_t *info;      // [0] pattern mask is all ones, [1] propagators separable, [2] max deviation (float bits)
     double *sums;       // float64 accumulators, see SumIdx
     double *coef;       // S + M step coefficients
-    float2 *far;        // N = 256 only: B_max * M * N*N far-field waves Psi_m / N (register order)
-    float *far_int;     // N = 256 only: B_max * N*N far-field intensity sum_m |Psi_m / N|^2 (register order)
+    float2 *far;        // B_max * M * N*N far-field waves Psi_m / N (register order)
+    float *far_int;     // B_max * N*N far-field intensity sum_m |Psi_m / N|^2 (register order)
     size_t bytes;
 };
 
@@ -123,10 +125,8 @@ static Workspace carve(void *base, int N, int M, int S, int B, int64_t H, int64_
     w.info = (int32_t *)take(4 * sizeof(int32_t));
     w.sums = (double *)take((size_t)SumIdx(B, S, M).total * sizeof(double));
     w.coef = (double *)take((size_t)(S + M + 4) * sizeof(double));
-    if (N == 256) {
-        w.far = (float2 *)take((size_t)B * M * NN * sizeof(float2));
-        w.far_int = (float *)take((size_t)B * NN * sizeof(float));
-    }
+    w.far = (float2 *)take((size_t)B * M * NN * sizeof(float2));
+    w.far_int = (float *)take((size_t)B * NN * sizeof(float));
     w.bytes = off;
     return w;
 }
@@ -158,9 +158,9 @@ struct GroupArgs {
     float *sim_out;
     const float *group_patterns;
     const uint16_t *patterns16;   // resident uint16 counts (patterns == nullptr then)
-    float2 *far;                  // N = 256: far-field waves (see Workspace)
-    float *far_int;               // N = 256: far-field intensity
-    int resume;                   // N = 256: 0 = forward launch, 1 = launch resumed at the detector
+    float2 *far;                  // far-field waves (see Workspace)
+    float *far_int;               // far-field intensity
+    int resume;                   // 0 = forward launch, 1 = launch resumed at the detector
 };
 
 // One position's measured pattern: host-streamed float32 rows (group_patterns),
@@ -249,15 +249,20 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     constexpr int MR = MC > 0 ? MC : 8;   // capacity of the remote-pointer arrays
     constexpr bool presolve = mode >= MODE_PRE_LSQML;
     constexpr bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
-    constexpr bool QUAD = N == 256;   // 4 CTAs per (position, mode); far field over two launches
+    constexpr bool QUAD = N == 256;   // 4 CTAs per (position, mode)
+    // Far field through global memory (two launches): the modes of a position are then
+    // independent CTAs, launched without clusters, and every SM takes work (a cluster of 4
+    // fits only 4 of a GPC's SMs per 4).  ePIE keeps its modes in one cluster: its
+    // per-slice maximum over the modes goes through distributed shared memory.
+    constexpr bool SPLIT = mode != MODE_EPIE;
     static_assert(!QUAD || (mode != MODE_EPIE && mode != MODE_PRE_EPIE), "ePIE needs the modes in one cluster");
     cg::cluster_group cl = cg::this_cluster();
     const int M = MC > 0 ? MC : a.M;
     const int S = a.S;
-    const int m = QUAD ? (int)((blockIdx.x >> 2) % M) : (int)cl.block_rank();
+    const int m = QUAD ? (int)((blockIdx.x >> 2) % M) : SPLIT ? (int)(blockIdx.x % M) : (int)cl.block_rank();
     const int b = QUAD ? (int)((blockIdx.x >> 2) / M) : (int)(blockIdx.x / M);
     const int tid = threadIdx.x;
-    const bool resume = QUAD && a.resume;
+    const bool resume = SPLIT && a.resume;
 
     extern __shared__ float4 smem_raw[];
     float2 *xb = reinterpret_cast<float2 *>(smem_raw);
@@ -519,7 +524,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             // ------------------------------------------- detector: Psi = fft2(exit), constraint
             float *xf = reinterpret_cast<float *>(xb);
             const float *rxf[MR];
-            if constexpr (QUAD) {
+            if constexpr (SPLIT) {
                 if (!resume) {
                     // the forward launch ends at the detector: store Psi_m / N and add |Psi_m / N|^2
                     // into the position's intensity (or, simulating, into the output pattern)
@@ -552,7 +557,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 #pragma unroll
                 for (int r = 0; r < MR; ++r) rxf[r] = r < M ? cl.map_shared_rank(xf, r) : xf;
             }
-            if constexpr (mode == MODE_SIM && !QUAD) {
+            if constexpr (mode == MODE_SIM && !SPLIT) {
                 if (m == 0) {
 #pragma unroll
                     for (int u = 0; u < U; ++u)
@@ -576,7 +581,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                     for (int e = 0; e < E; ++e) {
                         const int f = I::flat(u, e);
                         float inten = 0.f;
-                        if constexpr (QUAD) {
+                        if constexpr (SPLIT) {
                             inten = __ldg(a.far_int + (size_t)b * NN + f);
                         } else {
                             for (int r = 0; r < MR; ++r)
@@ -610,12 +615,12 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                         }
                         v[u][e] = cscale(v[u][e], fac);
                     }
-                if constexpr (!QUAD) cl.sync();
+                if constexpr (!SPLIT) cl.sync();
                 if (m == 0 && (calc_err || grad)) {
                     double t[2] = {e2, loss};
                     block_sum_doubles<FFT_THREADS>(t, 2, dred);
                     if (tid == 0) {
-                        if constexpr (QUAD) {   // four quadrant CTAs: the finish kernel takes the root
+                        if constexpr (SPLIT) {   // per-CTA partial sums: the finish kernel takes the root
                             if (calc_err) atomicAdd(sums + a.o_err + b, t[0]);
                             if (grad) atomicAdd(sums + a.o_loss + b, t[1]);
                         } else {
@@ -1427,10 +1432,10 @@ static int launch_group_mode(const GroupArgs &a, cudaStream_t st) {
             return record_cuda(cudaGetLastError());
         configured = true;
     }
-    // N <= 128: one cluster of M CTAs (the modes) per position; N = 256: one cluster of
-    // 4 CTAs (the quadrants) per (position, mode)
+    // N = 256: one cluster of 4 CTAs (the quadrants) per (position, mode); ePIE at N <= 128:
+    // one cluster of M CTAs (the modes) per position; otherwise independent CTAs
     constexpr unsigned C = TileCfg<N>::CTAS;
-    const unsigned cluster = C > 1 ? C : (unsigned)a.M;
+    const unsigned cluster = C > 1 ? C : (MODE == MODE_EPIE ? (unsigned)a.M : 1u);
     return launch_clustered(k_group<N, MODE, MC>, (unsigned)(a.B * a.M) * C, FFT_THREADS, cluster, group_smem_bytes<N>(),
                             st, a);
 }
@@ -1473,25 +1478,21 @@ static int launch_group(const GroupArgs &a, cudaStream_t st) {
     }
 }
 
-// the fused step of one group: one launch, or at N = 256 the forward launch, which
-// leaves the far-field waves and the summed intensity in the workspace, and the
-// launch resumed at the detector
+// the fused step of one group: for LSQ-ML and the gradient engine the forward launch,
+// which leaves the far-field waves and the summed intensity in the workspace, and the
+// launch resumed at the detector; ePIE in one launch
 template <int N>
 static int launch_step(GroupArgs a, const Workspace &w, cudaStream_t st) {
-    if constexpr (N == 256) {
-        const bool split = a.mode == MODE_LSQML || a.mode == MODE_GRAD;
-        if (split) {
-            const int rc = record_cuda(cudaMemsetAsync(w.far_int, 0, (size_t)a.B * N * N * sizeof(float), st));
-            if (rc) return rc;
-        }
-        a.resume = 0;
-        int rc = launch_group<N>(a, st);
-        if (rc || !split) return rc;
-        a.resume = 1;
-        return launch_group<N>(a, st);
-    } else {
-        return launch_group<N>(a, st);
+    const bool split = a.mode == MODE_LSQML || a.mode == MODE_GRAD;
+    if (split) {
+        const int rc = record_cuda(cudaMemsetAsync(w.far_int, 0, (size_t)a.B * N * N * sizeof(float), st));
+        if (rc) return rc;
     }
+    a.resume = 0;
+    int rc = launch_group<N>(a, st);
+    if (rc || !split) return rc;
+    a.resume = 1;
+    return launch_group<N>(a, st);
 }
 
 template <int N>
@@ -1558,9 +1559,8 @@ static int simulate(const phb_engine *e, const int64_t *group, int B, float *out
     GroupArgs a = make_args(e, w, MODE_SIM, 0, group, B);
     a.illum = nullptr;
     a.sim_out = out;
-    if (N == 256) {   // the quadrant clusters add their modes' intensities into the output
-        if ((rc = record_cuda(cudaMemsetAsync(out, 0, (size_t)B * N * N * sizeof(float), st)))) return rc;
-    }
+    // the CTAs (clusters) of the modes add their intensities into the output
+    if ((rc = record_cuda(cudaMemsetAsync(out, 0, (size_t)B * N * N * sizeof(float), st)))) return rc;
     return launch_group<N>(a, st);
 }
 
@@ -1645,7 +1645,7 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
     f.group_loss = sp->group_loss;
     f.grad_tilt = sp->grad_tilt;
     f.grad_tilt_scale = sp->grad_tilt_scale;
-    f.errors = N == 256 ? sp->errors : nullptr;   // quadrant launches leave squared sums
+    f.errors = mode == MODE_LSQML ? sp->errors : nullptr;   // the split far field leaves squared sums
     k_finalize<<<1, 256, 0, st>>>(f);
     if ((rc = check_launch())) return rc;
 
