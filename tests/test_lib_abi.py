@@ -33,8 +33,9 @@ def test_host_only_entry_points():
     assert lib.phb_status_string(_lib.PHB_ERR_UNSUPPORTED).startswith(b'unsupported')
     # workspace sizing is host arithmetic
     n = lib.phb_engine_workspace_bytes(128, 4, 8, 256, 517, 517)
-    psi = 256 * 4 * 8 * 128 * 128 * 8
-    assert psi < n < psi + 64 * 2 ** 20
+    psi = 256 * 4 * 8 * 128 * 128 * 8                     # per-slice incident waves
+    far = 256 * 4 * 128 * 128 * 8 + 256 * 128 * 128 * 4   # far-field waves and intensities
+    assert psi + far < n < psi + far + 64 * 2 ** 20
     assert lib.phb_engine_workspace_bytes(0, 4, 8, 256, 517, 517) == 0
 
 
