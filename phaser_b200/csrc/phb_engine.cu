@@ -37,6 +37,16 @@
 
 namespace cg = cooperative_groups;
 
+// Elements of a thread's 32 whose global loads (object cutout, stored wavefield) are
+// issued together in the incident-wave and adjoint loops of the fused kernel (a build-time
+// tuning constant: more loads in flight, more registers).
+#ifndef PHB_START_CHUNK
+#define PHB_START_CHUNK 8
+#endif
+#ifndef PHB_BACK_CHUNK
+#define PHB_BACK_CHUNK 8
+#endif
+
 namespace phb {
 
 // Optional per-phase cycle accounting of the fused kernel (off unless the
@@ -423,7 +433,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 const bool store = upd_obj || upd_tilt;
                 float2 *dst = psi_b + (size_t)s * NN;
                 float *ill = do_illum ? a.illum + (size_t)s * a.H * a.W : nullptr;
-                constexpr int CH = 8;
+                constexpr int CH = PHB_START_CHUNK < E ? PHB_START_CHUNK : E;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
@@ -651,7 +661,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 float2 *__restrict__ dst = a.acc_obj + (size_t)s * a.H * a.W;
                 // chunks of 8 elements: issue all object / wavefield loads of a chunk before
                 // its atomics, so they are in flight together
-                constexpr int CH = 8;
+                constexpr int CH = PHB_BACK_CHUNK < E ? PHB_BACK_CHUNK : E;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
 #pragma unroll
