@@ -504,7 +504,7 @@ def train_network(geometry: str = 'multislice', slices=(4, 12), seed: int = 7):
     import torch
     from phaser_b200 import warmstart as WS
     spec = WS.DEFAULT_FEATURES
-    train_n = 128 if geometry == 'multislice' else 64
+    train_n = 64 if geometry == 'single' else 128
     t0 = time.perf_counter()
     feats, targets = WS.training_set(196, seed=seed, slices=slices, spec=spec, geometry=geometry)
     torch.cuda.synchronize()
@@ -719,8 +719,10 @@ def run_large_race(args):
         e.presolve()
         return e
 
+    # the network is trained with this configuration's optics and slice count (28-36 slices)
+    net = train_network('large', slices=(28, 36), seed=13)
     res = time_to_target(ds, pats16, new_engine, args.nrmse_iters, torch.cuda.current_stream(),
-                         arms=("warm_gradient_lsqml",))
+                         arms=("warm_gradient_lsqml",), net=net)
     size = "256^2 probe and detector (as specified)" if args.spec else "detector binned 2x2 to 128^2"
     print(json.dumps({"metric": f"time to the plain LSQ-ML's final NRMSE (s), large configuration, {size}",
                       "config": {"slices": ds.true_object.shape[0], "object": list(ds.true_object.shape[-2:]),

@@ -244,8 +244,16 @@ def lattice_geometry(scan: int = 32, seed: int = 0, geometry: str = 'multislice'
                     1e6 e- per pattern);
       'single':     the single-slice configuration's optics (64^2 probe at 0.2 A/px,
                     20 mrad, 200 kV, 100 A defocus, 1 mode, 4 px steps with +-0.5 px
-                    jitter, 1e5 e- per pattern), used for multislice objects here."""
+                    jitter, 1e5 e- per pattern), used for multislice objects here;
+      'large':      the large configuration's optics (300 kV, 25 mrad, 200 A defocus,
+                    8 modes, 3 px steps, 5e5 e- per pattern) on a 128^2 detector at
+                    0.2 A/px: the reciprocal sampling of its 256^2 detector binned 2 x 2,
+                    which is what the network sees of those patterns (features_for)."""
     from .synthetic import make_dataset
+    if geometry == 'large':
+        return make_dataset(N=128, M=8, S=1, scan_shape=(scan, scan), step_px=3.0, sampling=0.2, kv=300e3,
+                            conv_mrad=25.0, defocus=200.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
+                            peak_rad=0.0, counts=5e5, seed=seed)
     if geometry == 'single':
         return make_dataset(N=64, M=1, S=1, scan_shape=(scan, scan), step_px=4.0, sampling=0.2, kv=200e3,
                             conv_mrad=20.0, defocus=100.0, slice_thickness=20.0, spacing_px=10.0, sigma_px=1.5,
