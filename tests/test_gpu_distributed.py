@@ -55,7 +55,12 @@ def test_partial_steps_summed_match_one_step(solver):
     assert rel_l2(p_0, p_f) < 1e-5
     assert rel_l2(r0.pos_update.cpu().numpy()[idx], full.pos_update.cpu().numpy()[idx]) < 1e-4
     err_f = full.errors.cpu().numpy()[idx]
-    err_s = numpy.concatenate([r0.errors.cpu().numpy()[idx[:5]], r1.errors.cpu().numpy()[idx[5:]]])
+    if solver == 'lsqml':
+        # LSQ-ML's per-position errors are finished from the rank-summed float64 sums:
+        # after finish every rank holds all of the group's errors
+        err_s = r0.errors.cpu().numpy()[idx]
+    else:   # ePIE writes each rank's rows' errors in its own step
+        err_s = numpy.concatenate([r0.errors.cpu().numpy()[idx[:5]], r1.errors.cpu().numpy()[idx[5:]]])
     assert numpy.allclose(err_s, err_f, rtol=1e-5)
     assert int(r0.status.cpu()[0]) == -1
 
