@@ -46,6 +46,10 @@ namespace cg = cooperative_groups;
 #ifndef PHB_BACK_CHUNK
 #define PHB_BACK_CHUNK 8
 #endif
+// 1: prefetch part of the next phase's object cutout into L1 during the inverse transform
+#ifndef PHB_L1_PREFETCH
+#define PHB_L1_PREFETCH 0
+#endif
 
 namespace phb {
 
@@ -408,6 +412,19 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             return;
         }
         if (!(resume && step == 0)) {
+#if PHB_L1_PREFETCH
+            // the phase after this inverse transform reads the object cutout of slice s:
+            // pull the first half of this warp's rows into L1 while the transform runs
+            // (a warp's elements 0..15 span 8 rows x 2 column blocks of 32 pixels: one
+            // 128-byte line per lane)
+            if (!fwd && (phase == PH_START || phase == PH_BACK) && N == 128) {
+                const int l = tid & 31, row = I::row(0, 0) + 16 * (l >> 2), col = I::col(0, 0) - (tid & 31) +
+                                                                                     32 * ((l >> 1) & 1) + 16 * (l & 1);
+                const int64_t y = ci.y0 + row, x = ci.x0 + col;
+                if (y >= 0 && y < a.H && x >= 0 && x + 15 < a.W)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.object + ((size_t)s * a.H + y) * a.W + x));
+            }
+#endif
             if (fwd) fft2_r2k<N>(v, xb, twid);
             else ifft2_k2r<N>(v, xb, twid);
         }
