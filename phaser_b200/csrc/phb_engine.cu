@@ -47,8 +47,9 @@ namespace cg = cooperative_groups;
 #define PHB_BACK_CHUNK 8
 #endif
 // 1: prefetch part of the next phase's object cutout into L1 during the inverse transform
+// (measured +0.65% on the 128^2 x 4-mode LSQ-ML step; 0 builds the kernel without it)
 #ifndef PHB_L1_PREFETCH
-#define PHB_L1_PREFETCH 0
+#define PHB_L1_PREFETCH 1
 #endif
 
 namespace phb {
