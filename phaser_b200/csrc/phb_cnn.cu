@@ -285,8 +285,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// named barrier `id` over `nthreads` threads (a multiple of 32) that also ANDs `v` over them
+__device__ __forceinline__ bool bar_and(int id, int nthreads, bool v) {
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}\n" : "=r"(r) : "r"((uint32_t)v), "r"(id), "r"(nthreads) : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
     return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// split 8 float32 values into bf16 hi and lo rows
+__device__ __forceinline__ void split_row(const float (&vals)[8], uint4 &hi, uint4 &lo) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(vals[2 * j]), h1 = __float2bfloat16_rn(vals[2 * j + 1]);
+        h[j] = pack_bf16(h0, h1);
+        l[j] = pack_bf16(__float2bfloat16_rn(vals[2 * j] - __bfloat162float(h0)),
+                         __float2bfloat16_rn(vals[2 * j + 1] - __bfloat162float(h1)));
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 // src (Nb, Cr, Hs, Ws) -> out (Nb, Ncol, Ho, Wo); tiles of 128 padded-grid rows, T per image
@@ -361,17 +383,10 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
                 const int ch = ch0 + 8 * half + j;
                 vals[j] = (in && ch < Cr) ? __ldg(srcn + ((size_t)ch * Hs + sy) * Ws + sx) : 0.f;
             }
-            uint32_t hi[4], lo[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const __nv_bfloat16 h0 = __float2bfloat16_rn(vals[2 * j]), h1 = __float2bfloat16_rn(vals[2 * j + 1]);
-                const __nv_bfloat16 l0 = __float2bfloat16_rn(vals[2 * j] - __bfloat162float(h0));
-                const __nv_bfloat16 l1 = __float2bfloat16_rn(vals[2 * j + 1] - __bfloat162float(h1));
-                hi[j] = pack_bf16(h0, h1);
-                lo[j] = pack_bf16(l0, l1);
-            }
-            *reinterpret_cast<uint4 *>(ah + L * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4 *>(al + L * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            uint4 hi, lo;
+            split_row(vals, hi, lo);
+            *reinterpret_cast<uint4 *>(ah + L * 16) = hi;
+            *reinterpret_cast<uint4 *>(al + L * 16) = lo;
         }
         // B: per tap, NT rows x two 8-channel halves; unit (tap, half, col) at ((tap * 2 + half) * NT + col) * 16
         unsigned char *bsb = Bs + sb * B_<NT>::BYTES;
@@ -470,6 +485,243 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"((uint32_t)NT) : "memory");
+    }
+}
+
+// ------------------------------- weight gradient on the tensor cores (stride 1)
+// dw[co][ci][ky][kx] = sum_{n,y,x} dout[n][co][y][x] in[n][ci][y + ky - 1][x + kx - 1]
+// as GEMMs that reduce over pixels: for tap t = (ky, kx)
+//   D_t[r][co] = sum_k X[k + off_t][r] G[k][co],
+// k running over the rows of the padded pixel grid of pitch Wp = W + 2 (halo rows of G are
+// zero, so only real output pixels contribute), X the input activations on the same grid
+// (zero outside the image), off_t = (ky - 1) Wp + (kx - 1).  Both operands are staged
+// MN-major (a 16-byte row holds 8 channels of one pixel; consecutive pixels are
+// consecutive rows), so the tap shift is again only the start address of the A
+// descriptor: one staged chunk serves all three taps of a kernel row.
+//
+// Precision: the UMMA M = 128 rows of D are the input channels twice, r = c from the bf16
+// hi part of X and r = 64 + c from its lo part (the two halves of the A operand's 16
+// channel blocks); G is split the same way and both parts are multiplied (two MMAs per
+// tap and K step).  D[c] + D[64 + c] is then (X_hi + X_lo)(G_hi + G_lo), the float32
+// product to ~2^-17, accumulated in float32 tensor memory.
+//
+// A CTA runs the three taps of one kernel row ky = blockIdx.y (3 NT tensor-memory columns,
+// NT = 32 or 64 output channels) and stages only the 130 rows they read.  CTAs stride over
+// the (image, 128-row tile) chunks, double buffered, and add their D to dw once at the end.
+// (Layers with at most 16 output channels stay on the FP32 kernel k_conv_bwd_w: the
+// narrowest MMA, N = 16, would carry at most 16 useful columns per tap.)
+namespace wg {
+constexpr int BM = 128;            // padded-grid rows (the K extent) per chunk
+constexpr int THREADS = 256;
+constexpr int MB = 16;             // 8-channel blocks of A: 8 hi (channels 0..63), 8 lo
+constexpr int ROWS = BM + 2;        // staged rows of X: the 128 + 2 that three kx taps read
+constexpr int A_BYTES = MB * ROWS * 16;
+__host__ __device__ constexpr int b_bytes(int NT) { return 2 * (NT / 8) * BM * 16; }
+__host__ __device__ constexpr int tmem_cols(int c) { return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512; }
+__host__ __device__ constexpr int smem_bytes(int NT) { return 2 * A_BYTES + 2 * b_bytes(NT) + 64; }
+}  // namespace wg
+
+// shared-memory matrix descriptor with both strides given: no swizzle, sm_100 version 1
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+// kind::f16 instruction descriptor with A and B MN-major (transpose bits 15 and 16)
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int M, int N) {
+    return umma_idesc_bf16(M, N) | (1u << 15) | (1u << 16);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(wg::THREADS) k_conv_wgrad_tc(const float *in, const float *dout, float *dw, int Ci,
+                                                              int Co, int H, int W, int chunks) {
+    using namespace wg;
+    constexpr int TAPS = 3;
+    constexpr int NB = NT / 8;                              // 8-channel blocks of B (per part)
+    constexpr uint32_t TCOLS = (uint32_t)tmem_cols(TAPS * NT);
+    static_assert(TAPS * NT <= 256, "two CTAs per SM must fit the 512 tensor-memory columns");
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    const int Wp = W + 2, Hp = H + 2, R = ROWS;
+    const int T = (Hp * Wp + BM - 1) / BM;                  // chunks per image
+    constexpr int ABYTES = A_BYTES;
+    constexpr int BBYTES = b_bytes(NT);
+    unsigned char *As = tsm, *Bs = tsm + 2 * ABYTES;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * BBYTES);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ky_cta = (int)blockIdx.y;
+    const int row_off = (ky_cta - 1) * Wp - 1;   // padded row of staged row 0, minus q0
+    const int cbi = (Ci + 7) / 8, cbo = (Co + 7) / 8;               // live channel blocks of X and G
+
+    // channel blocks beyond Ci / Co stay zero in both stages (never staged)
+    for (int L = tid; L < 2 * MB * R; L += THREADS) {
+        const int blk = (L % (MB * R)) / R;
+        if ((blk & 7) >= cbi) *reinterpret_cast<uint4 *>(As + (size_t)L * 16) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int L = tid; L < 2 * 2 * NB * BM; L += THREADS) {
+        const int blk = (L % (2 * NB * BM)) / BM;
+        if ((blk % NB) >= cbo) *reinterpret_cast<uint4 *>(Bs + (size_t)L * 16) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"(TCOLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    constexpr uint32_t IDESC = umma_idesc_bf16_mn(BM, NT);
+    bool ok = true;
+    int it = 0;
+
+    // Warp 0 issues the MMAs of chunk `it` while warps 1..7 stage chunk it + 1 into the
+    // other buffer: the staging warps wait (bounded) on that buffer's mbarrier, agree on
+    // the outcome at a named barrier, and meet warp 0 at the block barrier after staging.
+    constexpr int PRODUCERS = THREADS - 32;
+    for (int c = blockIdx.x; c < chunks; c += gridDim.x, ++it) {
+        const int sb = it & 1;
+        const int n = c / T, q0 = (c % T) * BM;
+        unsigned char *a = As + sb * ABYTES, *bsb = Bs + sb * BBYTES;
+        bool good = true;
+        if (warp != 0) {
+            if (it >= 2) good = mbar_wait(&mbar[sb], (uint32_t)(((it >> 1) - 1) & 1));   // chunk it - 2 left it
+            good = bar_and(1, PRODUCERS, good);
+        }
+        if (warp != 0 && good) {
+            const int p = tid - 32;
+            const float *inn = in + (size_t)n * Ci * H * W;
+            const float *gn = dout + (size_t)n * Co * H * W;
+            // A: unit (block, row) at (block * R + row) * 16 (hi) and ((block + 8) * R + row) * 16 (lo)
+            for (int L = p; L < cbi * R; L += PRODUCERS) {
+                const int row = L % R, blk = L / R;
+                const int qg = q0 + row_off + row;
+                const int qy = qg >= 0 ? qg / Wp : -1, qx = qg - qy * Wp;
+                const bool inb = qg >= 0 && qy >= 1 && qy <= H && qx >= 1 && qx <= W;
+                float vals[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int ch = 8 * blk + j;
+                    vals[j] = (inb && ch < Ci) ? __ldg(inn + ((size_t)ch * H + (qy - 1)) * W + (qx - 1)) : 0.f;
+                }
+                uint4 hi, lo;
+                split_row(vals, hi, lo);
+                *reinterpret_cast<uint4 *>(a + (size_t)(blk * R + row) * 16) = hi;
+                *reinterpret_cast<uint4 *>(a + (size_t)((blk + 8) * R + row) * 16) = lo;
+            }
+            // B: unit (block, row) at (block * BM + row) * 16 (hi) and ((block + NB) * BM + row) * 16 (lo)
+            for (int L = p; L < cbo * BM; L += PRODUCERS) {
+                const int row = L % BM, blk = L / BM;
+                const int qg = q0 + row, qy = qg / Wp, qx = qg - qy * Wp;
+                const bool inb = qy >= 1 && qy <= H && qx >= 1 && qx <= W;
+                float vals[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int ch = 8 * blk + j;
+                    vals[j] = (inb && ch < Co) ? __ldg(gn + ((size_t)ch * H + (qy - 1)) * W + (qx - 1)) : 0.f;
+                }
+                uint4 hi, lo;
+                split_row(vals, hi, lo);
+                *reinterpret_cast<uint4 *>(bsb + (size_t)(blk * BM + row) * 16) = hi;
+                *reinterpret_cast<uint4 *>(bsb + (size_t)((blk + NB) * BM + row) * 16) = lo;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        if (!__syncthreads_and(good)) {
+            ok = false;
+            break;
+        }
+        if (tid == 0) {
+            tc_fence_after();
+            // descriptors advance by 16 staged rows (256 bytes, 16 in the address field) per K step
+            const uint32_t sbo_a = (uint32_t)R * 16, sbo_b = (uint32_t)BM * 16;
+            const uint64_t dbh = umma_desc_mn(smem_u32(bsb), 128u, sbo_b);
+            const uint64_t dbl = umma_desc_mn(smem_u32(bsb) + (uint32_t)(NB * BM * 16), 128u, sbo_b);
+#pragma unroll 1
+            for (int tap = 0; tap < TAPS; ++tap) {
+                const int start = tap;   // staged row of k = 0 (tap = kx)
+                const uint64_t da = umma_desc_mn(smem_u32(a) + (uint32_t)(start * 16), 128u, sbo_a);
+                const uint32_t d = tmem + (uint32_t)(tap * NT);
+#pragma unroll
+                for (int ks = 0; ks < BM / 16; ++ks) {
+                    umma_bf16(d, da + (uint64_t)(16 * ks), dbh + (uint64_t)(16 * ks), IDESC, (it > 0 || ks > 0) ? 1u : 0u);
+                    umma_bf16(d, da + (uint64_t)(16 * ks), dbl + (uint64_t)(16 * ks), IDESC, 1u);
+                }
+            }
+            umma_commit(&mbar[sb]);
+        }
+    }
+    if (ok && it > 0) ok = mbar_wait(&mbar[(it - 1) & 1], (uint32_t)(((it - 1) >> 1) & 1));   // all MMAs done
+    ok = __syncthreads_and(ok);
+    if (!ok) {   // a wait gave up: let issued MMAs drain (bounded) before the memory is reused
+        mbar_wait(&mbar[0], 0);
+        mbar_wait(&mbar[1], 0);
+        __syncthreads();
+    }
+    tc_fence_after();
+    // D -> shared scratch [128 rows][TAPS][NT] (the operand buffers are free now): warp w reads
+    // lanes 32 (w % 4) .. +31, column half w / 4 of every tap
+    float *scr = reinterpret_cast<float *>(tsm);
+    if (it > 0) {
+        const int qd = warp & 3, halfc = warp >> 2;
+        const int r = 32 * qd + lane;
+        constexpr int HC = NT / 2;
+#pragma unroll 1
+        for (int tap = 0; tap < TAPS; ++tap) {
+#pragma unroll
+            for (int c8 = 0; c8 < HC / 8; ++c8) {
+                const uint32_t taddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(tap * NT + halfc * HC + 8 * c8);
+                uint32_t d[8];
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                             : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
+                               "=r"(d[7])
+                             : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    scr[((size_t)r * TAPS + tap) * NT + halfc * HC + 8 * c8 + j] = __uint_as_float(d[j]);
+            }
+        }
+    }
+    __syncthreads();
+    if (it > 0) {
+        // dw[co][ci][ky][kx] += D[ci] + D[64 + ci]; consecutive threads take consecutive taps
+        const int tap0 = 3 * ky_cta;
+        for (int L = tid; L < Co * Ci * TAPS; L += THREADS) {
+            const int tap = L % TAPS, ci = (L / TAPS) % Ci, co = L / (TAPS * Ci);
+            const float v = ok ? scr[((size_t)ci * TAPS + tap) * NT + co] + scr[((size_t)(64 + ci) * TAPS + tap) * NT + co]
+                               : __int_as_float(0x7fc00000);
+            atomicAdd(dw + ((size_t)co * Ci + ci) * 9 + tap0 + tap, v);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TCOLS) : "memory");
+    }
+}
+
+// db[co] += sum_{n, pixel} dout[n][co][pixel]: one CTA per (channel, batch slice)
+__global__ void __launch_bounds__(256) k_bias_grad(const float *dout, float *db, int Nb, int Co, int P, int n_per) {
+    __shared__ float red[8];
+    const int co = blockIdx.x, n0 = blockIdx.y * n_per, n1 = min(Nb, n0 + n_per);
+    float s = 0.f;
+    for (int n = n0; n < n1; ++n) {
+        const float *g = dout + ((size_t)n * Co + co) * P;
+        for (int p = threadIdx.x; p < P; p += blockDim.x) s += g[p];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int k = 0; k < 8; ++k) t += red[k];
+        atomicAdd(db + co, t);
     }
 }
 
@@ -648,6 +900,33 @@ static int launch_conv_tc(const float *src, const __nv_bfloat16 *w, const float 
 
 static bool tc_width(int n) { return n == 32 || n == 64; }
 
+// tensor-core weight gradient (stride 1, Ci <= 64, 17 <= Co <= 64): 3 CTAs (kernel rows)
+// per group of chunks, one wave of resident CTAs striding over the (image, 128-row tile) chunks
+template <int NT>
+static int launch_wgrad_tc(const float *in, const float *dout, float *dw, int Nb, int Ci, int Co, int H, int W,
+                           cudaStream_t st) {
+    const int Wp = W + 2, Hp = H + 2;
+    constexpr int smem = wg::smem_bytes(NT);
+    constexpr int scratch = wg::BM * 3 * NT * (int)sizeof(float);   // epilogue, over the operand buffers
+    static_assert(scratch <= smem - 64, "epilogue scratch must fit the operand buffers");
+    const long long chunks = (long long)Nb * ((Hp * Wp + wg::BM - 1) / wg::BM);
+    if (chunks > 0x7fffffffll) return PHB_ERR_UNSUPPORTED;
+    int dev = 0, sms = 0;
+    int rc = record_cuda(cudaGetDevice(&dev));
+    if (!rc) rc = record_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (rc) return rc;
+    const int per_sm = 2 * (smem + 1024) <= 227 * 1024 ? 2 : 1;
+    const int groups = 3;
+    long long gk = (long long)sms * per_sm / groups;   // one wave: every CTA resident at once
+    if (gk > chunks) gk = chunks;
+    if (gk < 1) gk = 1;
+    auto k = k_conv_wgrad_tc<NT>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return record_cuda(cudaGetLastError());
+    k<<<dim3((unsigned)gk, (unsigned)groups), wg::THREADS, smem, st>>>(in, dout, dw, Ci, Co, H, W, (int)chunks);
+    return check_launch();
+}
+
 extern "C" {
 
 int phb_conv3x3_fwd(const float *in, const void *w_bf16, const float *bias, float *out, int32_t Nb, int32_t Ci,
@@ -695,8 +974,15 @@ int phb_conv3x3_bwd_weight(const float *in, const float *dout, float *dw, float 
     if (Ci > 65535 || (stride == 2 && ((Hi | Wi) & 1))) return PHB_ERR_UNSUPPORTED;
     const int Ho = Hi / stride, Wo = Wi / stride;
     const int per = 8;
-    dim3 grid((unsigned)((Co + 7) / 8), (unsigned)Ci, (unsigned)((Nb + per - 1) / per));
     cudaStream_t st = (cudaStream_t)stream;
+    if (stride == 1 && Ci <= 64 && Co > 16 && Co <= 64) {   // tensor cores (tcgen05), bias gradient beside
+        k_bias_grad<<<dim3((unsigned)Co, (unsigned)((Nb + 15) / 16)), 256, 0, st>>>(dout, db, Nb, Co, Ho * Wo, 16);
+        int rc = check_launch();
+        if (rc) return rc;
+        return Co <= 32 ? launch_wgrad_tc<32>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st)
+                        : launch_wgrad_tc<64>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st);
+    }
+    dim3 grid((unsigned)((Co + 7) / 8), (unsigned)Ci, (unsigned)((Nb + per - 1) / per));
     if (stride == 1) k_conv_bwd_w<1><<<grid, 256, 0, st>>>(in, dout, dw, db, Nb, Ci, Hi, Wi, Co, Ho, Wo, per);
     else k_conv_bwd_w<2><<<grid, 256, 0, st>>>(in, dout, dw, db, Nb, Ci, Hi, Wi, Co, Ho, Wo, per);
     return check_launch();
