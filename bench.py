@@ -817,7 +817,8 @@ def extra_configs(dev, stream):
         at 5 px), probe 128^2 x 2 modes, Poisson negative log-likelihood, Adam on object
         and probe, grouping 64, 2 timed iterations after 1 warm-up;
       large multislice (detector binned 2x2 to 128^2, see large_multislice_config):
-        LSQ-ML and the gradient engine, 1 timed iteration each after 1 warm-up."""
+        LSQ-ML and the gradient engine, 1 timed iteration each after 1 warm-up;
+      large multislice as specified (256^2 probe and detector): large_spec_rate."""
     import torch
     from phaser_b200.synthetic import (epie_single_slice_config, gradient_multislice_config,
                                        large_multislice_config, simulate_patterns)
@@ -920,6 +921,9 @@ def extra_configs(dev, stream):
     out['large_multislice_binned'] = large
     del pats16
     torch.cuda.empty_cache()
+    # and as specified: 256^2 probe and detector x 8 modes (4-CTA cluster tiles), a sample of
+    # 4 mini-batches of 256 after 1 (python bench.py --large-rate times 8 after 2)
+    out['large_multislice_spec'] = large_spec_rate(dev, stream, steps=4, warmup=1)
     return out
 
 

@@ -24,13 +24,13 @@
 //   per-thread base plus a compile-time offset.
 //
 // N = 256 (a cluster of 4 CTAs per tile, each holding one 128 x 128 part):
-//   real space: CTA rank q = 2 a + b holds the quadrant x[128 a + y', 128 b + x'] in the
-//   N = 128 R layout of (y', x');  Fourier space: it holds the polyphase component
-//   X[2 ky' + a, 2 kx' + b] in the N = 128 K layout of (ky', kx').  The forward transform
-//   is one radix-2 x 2 decimation-in-frequency stage across the cluster -- two pairwise
-//   radix-2 exchanges through distributed shared memory (signs (-1)^(ac + bd)) and the
-//   twiddle W256^(c y' + d x') -- followed by the CTA's own 128 x 128 transform; the
-//   inverse runs the same steps in reverse order with conjugate twiddles.
+//   real space: CTA rank r = 2 a + b holds the polyphase component x[2 y' + a, 2 x' + b] in
+//   the N = 128 R layout of (y', x');  Fourier space: it holds a quarter of the spectrum,
+//   the points of N = 128 K-layout slots 8r .. 8r + 7, each at its four (ky' + 128p,
+//   kx' + 128q).  The forward transform is the CTA's own 128 x 128 transform followed by one
+//   radix-2 x 2 decimation-in-time stage across the cluster (an all-to-all through
+//   distributed shared memory, twiddles W256^(a ky' + b kx')); the inverse runs the same
+//   steps in reverse order with conjugate twiddles.
 //
 // N = 64 (8 values per thread, three exchanges): a line FFT of length
 // N = E * NT runs as a radix-E DFT in registers (elements strided by NT) ->
@@ -363,74 +363,103 @@ __device__ __forceinline__ void fft128_k2r(float2 (&v)[1][32], float2 *xb, const
 }
 
 // ------------------------------------------------- N = 256: 4-CTA cluster form
-// Radix-2 x 2 stage across the cluster at every register slot: this CTA (rank
-// 2 c + d) gets sum over ranks 2 a + b of (-1)^(a c + b d) x_ab.  It runs as two
-// pairwise radix-2 steps (partner rank q ^ 2, then q ^ 1), so a CTA reads 2 x 128 KB of
-// its partners' shared memory instead of 3 x 128 KB, in 16-byte loads.  Each step: every
-// CTA publishes its values (two register slots per float4), a cluster barrier, the
-// partner's values are read at the same slots, and a second barrier keeps each buffer
-// intact until its partner has read it.
-__device__ __forceinline__ void quad_pair_step(float2 (&v)[1][32], float2 *xb, int partner, bool upper) {
+// Decimation in time across the cluster.  In real space the CTA of rank r = 2a + b holds
+// the polyphase component x[2y' + a][2x' + b] in the N = 128 R layout of (y', x'), and its
+// own 128 x 128 transform gives Y_ab[ky'][kx'] in the N = 128 K layout.  Then
+//   X[ky' + 128p][kx' + 128q] = sum_ab (-1)^(ap + bq) W256^(a ky' + b kx') Y_ab[ky'][kx'],
+// so one output point needs the four CTAs' values at the same (ky', kx').  Rank r takes the
+// points of register slots 8r .. 8r + 7 (a quarter of the spectrum) from all four CTAs --
+// one all-to-all through distributed shared memory, 3 x 32 KB of remote reads per CTA --
+// and keeps the four outputs: slot 8 (2p + q) + j of thread t holds X[ky' + 128p][kx' + 128q]
+// for (ky', kx') = the N = 128 K-layout point of slot 8r + j.  The inverse runs the
+// butterflies first (conjugate twiddles), the all-to-all back, then the 128 x 128 inverse.
+// Each exchange: publish (two register slots per float4), cluster barrier, read, cluster
+// barrier (no CTA rewrites its buffer before the others have read it).
+__device__ __forceinline__ void quad_a2a_fwd(float2 (&v)[1][32], float2 *xb, const float2 *tw256) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, r = cluster_rank() & 3;
     float2 *x = v[0];
     float4 *mine = reinterpret_cast<float4 *>(xb);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) mine[j * 512 + t] = make_float4(x[2 * j].x, x[2 * j].y, x[2 * j + 1].x, x[2 * j + 1].y);
+    for (int i = 0; i < 16; ++i) mine[i * 512 + t] = make_float4(x[2 * i].x, x[2 * i].y, x[2 * i + 1].x, x[2 * i + 1].y);
     cl.sync();
-    const float4 *theirs = cl.map_shared_rank(mine, partner) + t;
-    // lower rank of the pair: x_own + x_partner; upper: x_partner - x_own
-    const float so = upper ? -1.f : 1.f;
+    float2 y[4][8];   // [source rank ab][point j]
 #pragma unroll
-    for (int j0 = 0; j0 < 16; j0 += 4) {
-        float4 p[4];
+    for (int ab = 0; ab < 4; ++ab) {
+        const float4 *src = cl.map_shared_rank(mine, ab) + 4 * r * 512 + t;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) p[j] = theirs[(j0 + j) * 512];
+        for (int i = 0; i < 4; ++i) {
+            const float4 p = src[i * 512];
+            y[ab][2 * i] = make_float2(p.x, p.y);
+            y[ab][2 * i + 1] = make_float2(p.z, p.w);
+        }
+    }
+    cl.sync();
+    const int ky0 = (t >> 6) + 64 * (r & 1), kx = (t & 63) + 64 * (r >> 1);   // point j: ky' = ky0 + 8 j
+    const float2 wx = tw256[kx];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            float2 &e0 = x[2 * (j0 + j)], &e1 = x[2 * (j0 + j) + 1];
-            e0 = make_float2(fmaf(so, e0.x, p[j].x), fmaf(so, e0.y, p[j].y));
-            e1 = make_float2(fmaf(so, e1.x, p[j].z), fmaf(so, e1.y, p[j].w));
+    for (int j = 0; j < 8; ++j) {
+        const int ky = ky0 + 8 * j;
+        const float2 y0 = y[0][j], y1 = cmul(y[1][j], wx), y2 = cmul(y[2][j], tw256[ky]),
+                     y3 = cmul(y[3][j], tw256[ky + kx]);   // ky + kx <= 254
+        const float2 s02 = cadd(y0, y2), d02 = csub(y0, y2), s13 = cadd(y1, y3), d13 = csub(y1, y3);
+        x[j] = cadd(s02, s13);        // (p, q) = (0, 0)
+        x[8 + j] = csub(s02, s13);    // (0, 1)
+        x[16 + j] = cadd(d02, d13);   // (1, 0)
+        x[24 + j] = csub(d02, d13);   // (1, 1)
+    }
+}
+
+__device__ __forceinline__ void quad_a2a_inv(float2 (&v)[1][32], float2 *xb, const float2 *tw256) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int t = threadIdx.x, r = cluster_rank() & 3;
+    float2 *x = v[0];
+    const int ky0 = (t >> 6) + 64 * (r & 1), kx = (t & 63) + 64 * (r >> 1);
+    const float2 wx = tw256[kx];
+    float2 y[4][8];   // [destination rank ab][point j]
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int ky = ky0 + 8 * j;
+        const float2 X0 = x[j], X1 = x[8 + j], X2 = x[16 + j], X3 = x[24 + j];
+        const float2 s02 = cadd(X0, X2), d02 = csub(X0, X2), s13 = cadd(X1, X3), d13 = csub(X1, X3);
+        y[0][j] = cadd(s02, s13);
+        y[1][j] = cmulc(csub(s02, s13), wx);
+        y[2][j] = cmulc(cadd(d02, d13), tw256[ky]);
+        y[3][j] = cmulc(csub(d02, d13), tw256[ky + kx]);
+    }
+    float4 *mine = reinterpret_cast<float4 *>(xb);
+#pragma unroll
+    for (int ab = 0; ab < 4; ++ab)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            mine[(4 * ab + i) * 512 + t] = make_float4(y[ab][2 * i].x, y[ab][2 * i].y, y[ab][2 * i + 1].x,
+                                                       y[ab][2 * i + 1].y);
+    cl.sync();
+#pragma unroll
+    for (int src_r = 0; src_r < 4; ++src_r) {
+        const float4 *src = cl.map_shared_rank(mine, src_r) + 4 * r * 512 + t;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float4 p = src[i * 512];
+            x[8 * src_r + 2 * i] = make_float2(p.x, p.y);
+            x[8 * src_r + 2 * i + 1] = make_float2(p.z, p.w);
         }
     }
     cl.sync();
 }
 
-__device__ __forceinline__ void quad_butterfly(float2 (&v)[1][32], float2 *xb) {
-    const int q = cluster_rank() & 3;
-    quad_pair_step(v, xb, q ^ 2, (q & 2) != 0);   // rows: a <-> c
-    quad_pair_step(v, xb, q ^ 1, (q & 1) != 0);   // columns: b <-> d
-}
-
-// multiply slot i (real-space position (y', x') of the N = 128 R layout) by
-// W256^(c y' + d x') (CONJ: its conjugate); c, d = the CTA's rank bits
-template <bool CONJ>
-__device__ __forceinline__ void quad_twiddle(float2 (&v)[1][32], const float2 *tw256) {
-    const int q = cluster_rank() & 3;
-    if (q == 0) return;   // uniform over the CTA
-    const int c = q >> 1, d = q & 1, t = threadIdx.x;
-    const int base = c * (t >> 5) + d * (t & 31);
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        const int e = (base + c * 16 * (i & 7) + d * 32 * (i >> 3)) & 255;
-        const float2 w = tw256[e];
-        v[0][i] = CONJ ? cmulc(v[0][i], w) : cmul(v[0][i], w);
-    }
-}
-
-// Forward 256 x 256 (cluster of 4): quadrant in R layout -> polyphase component in K layout.
+// Forward 256 x 256 (cluster of 4): polyphase component in R layout -> spectrum quarter.
 __device__ __forceinline__ void fft256_r2k(float2 (&v)[1][32], float2 *xb, const float2 *twid) {
-    quad_butterfly(v, xb);
-    quad_twiddle<false>(v, twid + 128);
     fft128_r2k(v, xb, twid);
+    quad_a2a_fwd(v, xb, twid + 128);
 }
 
-// Inverse (unnormalised): polyphase component in K layout -> quadrant in R layout.
+// Inverse (unnormalised): spectrum quarter -> polyphase component in R layout.
 __device__ __forceinline__ void ifft256_k2r(float2 (&v)[1][32], float2 *xb, const float2 *twid) {
+    quad_a2a_inv(v, xb, twid + 128);
     fft128_k2r(v, xb, twid);
-    quad_twiddle<true>(v, twid + 128);
-    quad_butterfly(v, xb);
 }
 
 // ----------------------------------------------------------------- line passes
@@ -648,20 +677,30 @@ struct Idx<64> {
     }
 };
 
-// N = 256: the CTA of cluster rank q = 2 a + b holds the quadrant (a, b) in real space
-// and the polyphase component (a, b) in Fourier space, each in the N = 128 layouts;
-// register-order flat indices are CTA-major (q * 16384 + the N = 128 flat index).
+// N = 256: the CTA of cluster rank r = 2 a + b holds the polyphase component (a, b) in real
+// space (pixel (2 y' + a, 2 x' + b) where the N = 128 R layout has (y', x')) and a quarter of
+// the spectrum in Fourier space (slot 8 (2p + q) + j: (ky' + 128 p, kx' + 128 q) where the
+// N = 128 K layout has (ky', kx') at slot 8 r + j); register-order flat indices are CTA-major
+// (r * 16384 + the N = 128 flat index).
 template <>
 struct Idx<256> {
     using B = Idx<128>;
     static constexpr int U = 1, E = 32;
     static __device__ __forceinline__ int quad() { return cluster_rank() & 3; }
-    static __device__ __forceinline__ int row(int u, int q) { return B::row(u, q) + ((quad() >> 1) << 7); }
-    static __device__ __forceinline__ int col(int u, int q) { return B::col(u, q) + ((quad() & 1) << 7); }
-    static __host__ __device__ __forceinline__ constexpr int drow(int q) { return B::drow(q); }
-    static __host__ __device__ __forceinline__ constexpr int dcol(int q) { return B::dcol(q); }
-    static __device__ __forceinline__ int kx(int u, int e) { return 2 * B::kx(u, e) + (quad() & 1); }
-    static __device__ __forceinline__ int ky(int u, int e) { return 2 * B::ky(u, e) + (quad() >> 1); }
+    static __device__ __forceinline__ int row(int u, int q) { return 2 * B::row(u, q) + (quad() >> 1); }
+    static __device__ __forceinline__ int col(int u, int q) { return 2 * B::col(u, q) + (quad() & 1); }
+    static __host__ __device__ __forceinline__ constexpr int drow(int q) { return 2 * B::drow(q); }
+    static __host__ __device__ __forceinline__ constexpr int dcol(int q) { return 2 * B::dcol(q); }
+    static __host__ __device__ __forceinline__ void k_of(int t, int r, int e, int &ky_, int &kx_) {
+        ky_ = (t >> 6) + 64 * (r & 1) + 8 * (e & 7) + 128 * (e >> 4);
+        kx_ = (t & 63) + 64 * (r >> 1) + 128 * ((e >> 3) & 1);
+    }
+    static __device__ __forceinline__ int ky(int, int e) {
+        return (threadIdx.x >> 6) + 64 * (quad() & 1) + 8 * (e & 7) + 128 * (e >> 4);
+    }
+    static __device__ __forceinline__ int kx(int, int e) {
+        return (threadIdx.x & 63) + 64 * (quad() >> 1) + 128 * ((e >> 3) & 1);
+    }
     static __device__ __forceinline__ int flat(int u, int e) { return (quad() << 14) + B::flat(u, e); }
 };
 
@@ -671,8 +710,8 @@ __device__ __forceinline__ void flat_to_rc(int f, int &r, int &c) {
     if constexpr (N == 256) {
         const int q = f >> 14;
         flat_to_rc<128>(f & 16383, r, c);
-        r += (q >> 1) << 7;
-        c += (q & 1) << 7;
+        r = 2 * r + (q >> 1);
+        c = 2 * c + (q & 1);
     } else {
         const int t = f % FFT_THREADS, s = f / FFT_THREADS;   // s = u*E + q
         Idx<N>::rc_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, r, c);
@@ -682,10 +721,8 @@ __device__ __forceinline__ void flat_to_rc(int f, int &r, int &c) {
 template <int N>
 __device__ __forceinline__ void flat_to_k(int f, int &ky, int &kx) {
     if constexpr (N == 256) {
-        const int q = f >> 14;
-        flat_to_k<128>(f & 16383, ky, kx);
-        ky = 2 * ky + (q >> 1);
-        kx = 2 * kx + (q & 1);
+        const int g = f & 16383;
+        Idx<256>::k_of(g % FFT_THREADS, f >> 14, g / FFT_THREADS, ky, kx);
     } else {
         const int t = f % FFT_THREADS, s = f / FFT_THREADS;
         Idx<N>::k_of(t, s / FFTCfg<N>::E, s % FFTCfg<N>::E, ky, kx);
