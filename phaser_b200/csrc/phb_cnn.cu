@@ -236,6 +236,11 @@ __global__ void __launch_bounds__(256) k_conv_bwd_w(const float *in, const float
 // MODE 0: forward, stride 1 or 2 (out = conv(in, w) + bias, optional ReLU).
 // MODE 1: data gradient at stride 1 (din[ci][Y][X] = sum w[co][ci][ky][kx] dout[co][Y+1-ky][X+1-kx]:
 //         the tap offsets mirrored and the channel roles exchanged).
+// MODE 2: data gradient at stride 2, one output parity class (py, px) per CTA (blockIdx.x % 4):
+//         din[ci][2Y + py][2X + px] = sum over the class's taps of w[co][ci][ky][kx]
+//         dout[co][Y + dy][X + dx], ky = 1 (dy = 0) for py = 0 and ky = 0 (dy = 1) or 2 (dy = 0)
+//         for py = 1, the same for x: a convolution of dout with 1, 2 or 4 taps on the
+//         dout grid (pitch Wo + 1, halo row and column after the image).
 namespace tc {
 constexpr int BM = 128;                 // output pixels (padded-grid rows) per CTA
 constexpr int CC = 16;                  // reduction channels per chunk (one MMA K)
@@ -244,10 +249,10 @@ constexpr long long WAIT_LIMIT = 1ll << 22;   // try_wait attempts before a wait
 __host__ __device__ constexpr int pitch(int S, int Wo) { return S == 1 ? Wo + 2 : Wo + 1; }
 // staged rows per phase
 __host__ __device__ constexpr int rows(int S, int Wp) { return S == 1 ? BM + 2 * Wp + 2 : BM + Wp + 1; }
-__host__ __device__ constexpr int phases(int S) { return S == 1 ? 1 : 4; }
+__host__ __device__ constexpr int phases(int S, int MODE = 0) { return S == 2 && MODE == 0 ? 4 : 1; }
 template <int NT> struct B_ { static constexpr int BYTES = 9 * NT * CC * 2; };
 // bytes of one stage: A (phases x rows x 16 channels x bf16, hi and lo) + B (9 taps x NT x 16)
-__host__ __device__ constexpr int a_bytes(int S, int Wp) { return phases(S) * rows(S, Wp) * CC * 2; }
+__host__ __device__ constexpr int a_bytes(int S, int Wp, int MODE = 0) { return phases(S, MODE) * rows(S, Wp) * CC * 2; }
 }  // namespace tc
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -317,17 +322,20 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
                                                          float *out, int Cr, int Ncol, int Hs, int Ws, int Ho, int Wo,
                                                          int Ci_w, int relu) {
     using namespace tc;
-    static_assert(MODE == 0 || S == 1, "the data gradient runs at stride 1 only");
+    static_assert(MODE == 0 || (MODE == 1 && S == 1) || (MODE == 2 && S == 2), "mode / stride");
     extern __shared__ __align__(1024) unsigned char tsm[];
     const int Wp = pitch(S, Wo), Hp = Ho + (S == 1 ? 2 : 1), R = rows(S, Wp);
-    const int ABYTES = a_bytes(S, Wp);                 // per stage, one part (hi or lo)
+    const int ABYTES = a_bytes(S, Wp, MODE);           // per stage, one part (hi or lo)
     unsigned char *Ahi = tsm, *Alo = tsm + 2 * ABYTES, *Bs = tsm + 4 * ABYTES;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * B_<NT>::BYTES);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int T = (Hp * Wp + BM - 1) / BM;             // tiles per image
-    const int n = blockIdx.x / T, q0 = (blockIdx.x % T) * BM;
-    const int lo_row = q0 - (Wp + 1);                  // padded-grid row of staged row 0
+    const int tile = MODE == 2 ? (int)(blockIdx.x >> 2) : (int)blockIdx.x;
+    const int cls = MODE == 2 ? (int)(blockIdx.x & 3) : 0, cpy = cls >> 1, cpx = cls & 1;   // MODE 2 parity class
+    const int ntaps = MODE == 2 ? (1 + cpy) * (1 + cpx) : 9;
+    const int n = tile / T, q0 = (tile % T) * BM;
+    const int lo_row = MODE == 2 ? q0 : q0 - (Wp + 1);   // padded-grid row of staged row 0
 
     if (warp == 0) {   // tensor-memory accumulator: NT columns x 128 lanes of float32
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -361,14 +369,18 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
         // A: per phase, R rows x two 8-channel halves; unit (phase, half, row) at
         // ((phase * 2 + half) * R + row) * 16 bytes.  Consecutive threads take consecutive
         // rows, so every channel plane is read in coalesced runs.
-        const int units = phases(S) * 2 * R;
+        const int units = phases(S, MODE) * 2 * R;
         for (int L = tid; L < units; L += THREADS) {
             const int row = L % R, ph_half = L / R, half = ph_half & 1, ph = ph_half >> 1;
             const int qg = lo_row + row, qy = qg / Wp, qx = qg - qy * Wp;   // qg may be negative: then outside
             // source pixel of this staged row
             int sy, sx;
             bool in;
-            if constexpr (S == 1) {
+            if constexpr (MODE == 2) {   // the dout grid itself, halo after the image
+                sy = qy;
+                sx = qx;
+                in = qy < Hs && qx < Ws;
+            } else if constexpr (S == 1) {
                 sy = qy - 1;
                 sx = qx - 1;
                 in = qg >= 0 && qy >= 1 && qy <= Hs && qx >= 1 && qx <= Ws;
@@ -390,8 +402,11 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
         }
         // B: per tap, NT rows x two 8-channel halves; unit (tap, half, col) at ((tap * 2 + half) * NT + col) * 16
         unsigned char *bsb = Bs + sb * B_<NT>::BYTES;
-        for (int L = tid; L < 9 * 2 * NT; L += THREADS) {
-            const int col = L % NT, tap_half = L / NT, half = tap_half & 1, tap = tap_half >> 1;
+        for (int L = tid; L < ntaps * 2 * NT; L += THREADS) {
+            const int col = L % NT, tap_half = L / NT, half = tap_half & 1, slot = tap_half >> 1;
+            // MODE 2: slot -> the class's (ky, kx): ky = 1 for py = 0, 0 / 2 for py = 1
+            const int tap = MODE == 2 ? (cpy ? 2 * (slot / (1 + cpx)) : 1) * 3 + (cpx ? 2 * (slot % (1 + cpx)) : 1)
+                                      : slot;
             uint32_t wv[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -418,10 +433,14 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
             const uint32_t a_hi = smem_u32(ah), a_lo = smem_u32(al), b0 = smem_u32(bsb);
             const uint32_t lbo_a = (uint32_t)R * 16, lbo_b = (uint32_t)NT * 16;
 #pragma unroll 1
-            for (int tap = 0; tap < 9; ++tap) {
+            for (int tap = 0; tap < ntaps; ++tap) {
                 const int ky = tap / 3, kx = tap % 3;
                 int ph = 0, start;
-                if constexpr (S == 1) {
+                if constexpr (MODE == 2) {
+                    // class slot `tap`: (ky, kx) as staged in B; dout row Y + (ky == 0), column X + (kx == 0)
+                    const int kyc = cpy ? 2 * (tap / (1 + cpx)) : 1, kxc = cpx ? 2 * (tap % (1 + cpx)) : 1;
+                    start = (kyc == 0 ? Wp : 0) + (kxc == 0 ? 1 : 0);
+                } else if constexpr (S == 1) {
                     // output row m reads padded row q0 + m + (ky - 1) Wp + (kx - 1) (mirrored for the data gradient)
                     const int dy = MODE == 0 ? ky - 1 : 1 - ky, dx = MODE == 0 ? kx - 1 : 1 - kx;
                     start = Wp + 1 + dy * Wp + dx;
@@ -451,7 +470,8 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
     {
         const int qd = warp & 3, halfc = warp >> 2;
         const int m = 32 * qd + lane, qg = q0 + m, qy = qg / Wp, qx = qg - qy * Wp;
-        const int y = qy - 1, x = qx - 1;   // the padded grid's first row and column are halo
+        // the padded grid's first row and column are halo (MODE 2: its last ones)
+        const int y = MODE == 2 ? qy : qy - 1, x = MODE == 2 ? qx : qx - 1;
         constexpr int COLS = NT / 2;
         uint32_t r[COLS];
 #pragma unroll
@@ -476,7 +496,10 @@ __global__ void __launch_bounds__(tc::THREADS) k_conv_tc(const float *src, const
                     v += bias[col];
                     if (relu) v = fmaxf(v, 0.f);
                 }
-                out[(((size_t)n * Ncol + col) * Ho + y) * Wo + x] = v;
+                if constexpr (MODE == 2)   // din is (2 Ho) x (2 Wo): pixel (2y + py, 2x + px)
+                    out[(((size_t)n * Ncol + col) * (2 * Ho) + 2 * y + cpy) * (2 * Wo) + 2 * x + cpx] = v;
+                else
+                    out[(((size_t)n * Ncol + col) * Ho + y) * Wo + x] = v;
             }
         }
     }
@@ -514,11 +537,14 @@ namespace wg {
 constexpr int BM = 128;            // padded-grid rows (the K extent) per chunk
 constexpr int THREADS = 256;
 constexpr int MB = 16;             // 8-channel blocks of A: 8 hi (channels 0..63), 8 lo
-constexpr int ROWS = BM + 2;        // staged rows of X: the 128 + 2 that three kx taps read
-constexpr int A_BYTES = MB * ROWS * 16;
+constexpr int ROWS = BM + 2;        // staged rows of X per plane: the 128 + 2 that three kx taps read
+constexpr int PLANE = MB * ROWS * 16;
+// X planes per stage: stride 1 one; stride 2 the two column parities of the kernel row's input rows
+__host__ __device__ constexpr int planes(int S) { return S == 1 ? 1 : 2; }
+__host__ __device__ constexpr int a_bytes(int S) { return planes(S) * PLANE; }
 __host__ __device__ constexpr int b_bytes(int NT) { return 2 * (NT / 8) * BM * 16; }
 __host__ __device__ constexpr int tmem_cols(int c) { return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512; }
-__host__ __device__ constexpr int smem_bytes(int NT) { return 2 * A_BYTES + 2 * b_bytes(NT) + 64; }
+__host__ __device__ constexpr int smem_bytes(int NT, int S) { return 2 * a_bytes(S) + 2 * b_bytes(NT) + 64; }
 }  // namespace wg
 
 // shared-memory matrix descriptor with both strides given: no swizzle, sm_100 version 1
@@ -531,29 +557,33 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int M, int N) {
     return umma_idesc_bf16(M, N) | (1u << 15) | (1u << 16);
 }
 
-template <int NT>
+template <int NT, int S>
 __global__ void __launch_bounds__(wg::THREADS) k_conv_wgrad_tc(const float *in, const float *dout, float *dw, int Ci,
-                                                              int Co, int H, int W, int chunks) {
+                                                              int Co, int Hi, int Wi, int Ho, int Wo, int chunks) {
     using namespace wg;
     constexpr int TAPS = 3;
     constexpr int NB = NT / 8;                              // 8-channel blocks of B (per part)
     constexpr uint32_t TCOLS = (uint32_t)tmem_cols(TAPS * NT);
     static_assert(TAPS * NT <= 256, "two CTAs per SM must fit the 512 tensor-memory columns");
     extern __shared__ __align__(1024) unsigned char tsm[];
-    const int Wp = W + 2, Hp = H + 2, R = ROWS;
+    // output pixel (y, x) is padded-grid row (y + 1) Wp + (x + 1) (halo first; stride 1 also last)
+    const int Wp = S == 1 ? Wo + 2 : Wo + 1, Hp = S == 1 ? Ho + 2 : Ho + 1, R = ROWS;
     const int T = (Hp * Wp + BM - 1) / BM;                  // chunks per image
-    constexpr int ABYTES = A_BYTES;
+    constexpr int PL = planes(S), ABYTES = a_bytes(S);
     constexpr int BBYTES = b_bytes(NT);
     unsigned char *As = tsm, *Bs = tsm + 2 * ABYTES;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * BBYTES);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ky_cta = (int)blockIdx.y;
-    const int row_off = (ky_cta - 1) * Wp - 1;   // padded row of staged row 0, minus q0
+    // stride 1: input row y + ky - 1 is padded row q + (ky - 1) Wp; stride 2: input row 2y + ky - 1
+    // is row y - (ky == 0) of the input's row-parity plane rp = (ky + 1) & 1
+    const int rp = (ky_cta + 1) & 1;
+    const int row_off = (S == 1 ? ky_cta - 1 : (ky_cta == 0 ? -1 : 0)) * Wp - 1;   // staged row 0, minus q0
     const int cbi = (Ci + 7) / 8, cbo = (Co + 7) / 8;               // live channel blocks of X and G
 
     // channel blocks beyond Ci / Co stay zero in both stages (never staged)
-    for (int L = tid; L < 2 * MB * R; L += THREADS) {
+    for (int L = tid; L < 2 * PL * MB * R; L += THREADS) {
         const int blk = (L % (MB * R)) / R;
         if ((blk & 7) >= cbi) *reinterpret_cast<uint4 *>(As + (size_t)L * 16) = make_uint4(0u, 0u, 0u, 0u);
     }
@@ -593,35 +623,37 @@ __global__ void __launch_bounds__(wg::THREADS) k_conv_wgrad_tc(const float *in, 
         }
         if (warp != 0 && good) {
             const int p = tid - 32;
-            const float *inn = in + (size_t)n * Ci * H * W;
-            const float *gn = dout + (size_t)n * Co * H * W;
-            // A: unit (block, row) at (block * R + row) * 16 (hi) and ((block + 8) * R + row) * 16 (lo)
-            for (int L = p; L < cbi * R; L += PRODUCERS) {
-                const int row = L % R, blk = L / R;
+            const float *inn = in + (size_t)n * Ci * Hi * Wi;
+            const float *gn = dout + (size_t)n * Co * Ho * Wo;
+            // A: unit (plane, block, row) at plane * PLANE + (block * R + row) * 16 (hi) and
+            // plane * PLANE + ((block + 8) * R + row) * 16 (lo)
+            for (int L = p; L < PL * cbi * R; L += PRODUCERS) {
+                const int pl = L / (cbi * R), rem = L - pl * (cbi * R), row = rem % R, blk = rem / R;
                 const int qg = q0 + row_off + row;
                 const int qy = qg >= 0 ? qg / Wp : -1, qx = qg - qy * Wp;
-                const bool inb = qg >= 0 && qy >= 1 && qy <= H && qx >= 1 && qx <= W;
+                const int sy = S == 1 ? qy - 1 : 2 * (qy - 1) + rp, sx = S == 1 ? qx - 1 : 2 * (qx - 1) + pl;
+                const bool inb = qg >= 0 && qy >= 1 && qx >= 1 && sy < Hi && sx < Wi;
                 float vals[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int ch = 8 * blk + j;
-                    vals[j] = (inb && ch < Ci) ? __ldg(inn + ((size_t)ch * H + (qy - 1)) * W + (qx - 1)) : 0.f;
+                    vals[j] = (inb && ch < Ci) ? __ldg(inn + ((size_t)ch * Hi + sy) * Wi + sx) : 0.f;
                 }
                 uint4 hi, lo;
                 split_row(vals, hi, lo);
-                *reinterpret_cast<uint4 *>(a + (size_t)(blk * R + row) * 16) = hi;
-                *reinterpret_cast<uint4 *>(a + (size_t)((blk + 8) * R + row) * 16) = lo;
+                *reinterpret_cast<uint4 *>(a + (size_t)pl * PLANE + (size_t)(blk * R + row) * 16) = hi;
+                *reinterpret_cast<uint4 *>(a + (size_t)pl * PLANE + (size_t)((blk + 8) * R + row) * 16) = lo;
             }
             // B: unit (block, row) at (block * BM + row) * 16 (hi) and ((block + NB) * BM + row) * 16 (lo)
             for (int L = p; L < cbo * BM; L += PRODUCERS) {
                 const int row = L % BM, blk = L / BM;
                 const int qg = q0 + row, qy = qg / Wp, qx = qg - qy * Wp;
-                const bool inb = qy >= 1 && qy <= H && qx >= 1 && qx <= W;
+                const bool inb = qy >= 1 && qy <= Ho && qx >= 1 && qx <= Wo;
                 float vals[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int ch = 8 * blk + j;
-                    vals[j] = (inb && ch < Co) ? __ldg(gn + ((size_t)ch * H + (qy - 1)) * W + (qx - 1)) : 0.f;
+                    vals[j] = (inb && ch < Co) ? __ldg(gn + ((size_t)ch * Ho + (qy - 1)) * Wo + (qx - 1)) : 0.f;
                 }
                 uint4 hi, lo;
                 split_row(vals, hi, lo);
@@ -642,8 +674,10 @@ __global__ void __launch_bounds__(wg::THREADS) k_conv_wgrad_tc(const float *in, 
             const uint64_t dbl = umma_desc_mn(smem_u32(bsb) + (uint32_t)(NB * BM * 16), 128u, sbo_b);
 #pragma unroll 1
             for (int tap = 0; tap < TAPS; ++tap) {
-                const int start = tap;   // staged row of k = 0 (tap = kx)
-                const uint64_t da = umma_desc_mn(smem_u32(a) + (uint32_t)(start * 16), 128u, sbo_a);
+                // staged row of k = 0 for tap kx: stride 1 row kx; stride 2 column x - (kx == 0) of the
+                // column-parity plane (kx + 1) & 1
+                const int pl = S == 1 ? 0 : (tap + 1) & 1, start = S == 1 ? tap : (tap == 0 ? 0 : 1);
+                const uint64_t da = umma_desc_mn(smem_u32(a) + (uint32_t)(pl * PLANE + start * 16), 128u, sbo_a);
                 const uint32_t d = tmem + (uint32_t)(tap * NT);
 #pragma unroll
                 for (int ks = 0; ks < BM / 16; ++ks) {
@@ -880,9 +914,9 @@ template <int NT, int S, int MODE>
 static int launch_conv_tc_n(const float *src, const __nv_bfloat16 *w, const float *bias, float *out, int Nb, int Cr,
                             int Ncol, int Hs, int Ws, int Ho, int Wo, int Ci_w, int relu, cudaStream_t st) {
     const int Wp = tc::pitch(S, Wo), Hp = Ho + (S == 1 ? 2 : 1);
-    const int smem = 4 * tc::a_bytes(S, Wp) + 2 * tc::B_<NT>::BYTES + 64;
+    const int smem = 4 * tc::a_bytes(S, Wp, MODE) + 2 * tc::B_<NT>::BYTES + 64;
     if (smem > 200 * 1024) return PHB_ERR_UNSUPPORTED;   // wider images than this network uses
-    const long long tiles = (long long)Nb * ((Hp * Wp + tc::BM - 1) / tc::BM);
+    const long long tiles = (long long)Nb * ((Hp * Wp + tc::BM - 1) / tc::BM) * (MODE == 2 ? 4 : 1);
     if (tiles > 0x7fffffffll) return PHB_ERR_UNSUPPORTED;
     auto k = k_conv_tc<NT, S, MODE>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
@@ -900,15 +934,17 @@ static int launch_conv_tc(const float *src, const __nv_bfloat16 *w, const float 
 
 static bool tc_width(int n) { return n == 32 || n == 64; }
 
-// tensor-core weight gradient (stride 1, Ci <= 64, 17 <= Co <= 64): 3 CTAs (kernel rows)
+// tensor-core weight gradient (stride 1 or 2, Ci <= 64, 17 <= Co <= 64): 3 CTAs (kernel rows)
 // per group of chunks, one wave of resident CTAs striding over the (image, 128-row tile) chunks
-template <int NT>
-static int launch_wgrad_tc(const float *in, const float *dout, float *dw, int Nb, int Ci, int Co, int H, int W,
+template <int NT, int S>
+static int launch_wgrad_tc(const float *in, const float *dout, float *dw, int Nb, int Ci, int Co, int Hi, int Wi,
                            cudaStream_t st) {
-    const int Wp = W + 2, Hp = H + 2;
-    constexpr int smem = wg::smem_bytes(NT);
+    const int Ho = Hi / S, Wo = Wi / S;
+    const int Wp = S == 1 ? Wo + 2 : Wo + 1, Hp = S == 1 ? Ho + 2 : Ho + 1;
+    constexpr int smem = wg::smem_bytes(NT, S);
     constexpr int scratch = wg::BM * 3 * NT * (int)sizeof(float);   // epilogue, over the operand buffers
     static_assert(scratch <= smem - 64, "epilogue scratch must fit the operand buffers");
+    static_assert(smem <= 227 * 1024, "shared memory per CTA");
     const long long chunks = (long long)Nb * ((Hp * Wp + wg::BM - 1) / wg::BM);
     if (chunks > 0x7fffffffll) return PHB_ERR_UNSUPPORTED;
     int dev = 0, sms = 0;
@@ -920,10 +956,11 @@ static int launch_wgrad_tc(const float *in, const float *dout, float *dw, int Nb
     long long gk = (long long)sms * per_sm / groups;   // one wave: every CTA resident at once
     if (gk > chunks) gk = chunks;
     if (gk < 1) gk = 1;
-    auto k = k_conv_wgrad_tc<NT>;
+    auto k = k_conv_wgrad_tc<NT, S>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
         return record_cuda(cudaGetLastError());
-    k<<<dim3((unsigned)gk, (unsigned)groups), wg::THREADS, smem, st>>>(in, dout, dw, Ci, Co, H, W, (int)chunks);
+    k<<<dim3((unsigned)gk, (unsigned)groups), wg::THREADS, smem, st>>>(in, dout, dw, Ci, Co, Hi, Wi, Ho, Wo,
+                                                                         (int)chunks);
     return check_launch();
 }
 
@@ -959,8 +996,10 @@ int phb_conv3x3_bwd_data(const float *dout, const void *w_bf16, float *din, int3
     const int Ho = Hi / stride, Wo = Wi / stride;
     const __nv_bfloat16 *w = (const __nv_bfloat16 *)w_bf16;
     cudaStream_t st = (cudaStream_t)stream;
-    if (tc_width(Ci) && stride == 1 && Wi <= 64) {   // tensor cores: the GEMM width is the input-channel count
-        return launch_conv_tc<1, 1>(dout, w, nullptr, din, Nb, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st);
+    if (tc_width(Ci) && Wi <= 64) {   // tensor cores: the GEMM width is the input-channel count
+        if (stride == 1) return launch_conv_tc<1, 1>(dout, w, nullptr, din, Nb, Co, Ci, Ho, Wo, Hi, Wi, Ci, 0, st);
+        // stride 2: four parity classes on the dout grid (Ho x Wo)
+        return launch_conv_tc<2, 2>(dout, w, nullptr, din, Nb, Co, Ci, Ho, Wo, Ho, Wo, Ci, 0, st);
     }
     if (stride == 1) launch_bwd_data<16, 1>(dout, w, din, Nb, Ci, Hi, Wi, Co, Ho, Wo, st);
     else launch_bwd_data<16, 2>(dout, w, din, Nb, Ci, Hi, Wi, Co, Ho, Wo, st);
@@ -975,12 +1014,15 @@ int phb_conv3x3_bwd_weight(const float *in, const float *dout, float *dw, float 
     const int Ho = Hi / stride, Wo = Wi / stride;
     const int per = 8;
     cudaStream_t st = (cudaStream_t)stream;
-    if (stride == 1 && Ci <= 64 && Co > 16 && Co <= 64) {   // tensor cores (tcgen05), bias gradient beside
+    if (Ci <= 64 && Co > 16 && Co <= 64) {   // tensor cores (tcgen05), bias gradient beside
         k_bias_grad<<<dim3((unsigned)Co, (unsigned)((Nb + 15) / 16)), 256, 0, st>>>(dout, db, Nb, Co, Ho * Wo, 16);
         int rc = check_launch();
         if (rc) return rc;
-        return Co <= 32 ? launch_wgrad_tc<32>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st)
-                        : launch_wgrad_tc<64>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st);
+        if (stride == 1)
+            return Co <= 32 ? launch_wgrad_tc<32, 1>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st)
+                            : launch_wgrad_tc<64, 1>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st);
+        return Co <= 32 ? launch_wgrad_tc<32, 2>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st)
+                        : launch_wgrad_tc<64, 2>(in, dout, dw, Nb, Ci, Co, Hi, Wi, st);
     }
     dim3 grid((unsigned)((Co + 7) / 8), (unsigned)Ci, (unsigned)((Nb + per - 1) / per));
     if (stride == 1) k_conv_bwd_w<1><<<grid, 256, 0, st>>>(in, dout, dw, db, Nb, Ci, Hi, Wi, Co, Ho, Wo, per);

@@ -28,11 +28,11 @@ def bf16_tensor(w):
     return q
 
 
-# 32 / 64 output (forward) or input (data gradient) channels run on the tensor cores
-# (tcgen05 implicit GEMM, 128-pixel tiles, 16-channel reduction chunks), and so does the
-# stride-1 weight gradient with 17..64 output channels (a GEMM reducing over pixels); the
-# others on the FP32 pipe.  Partial pixel tiles (B H^2 not a multiple of 128) and partial /
-# several reduction chunks are included.
+# 32 / 64 output (forward) or input (data gradient, stride 1 and 2) channels run on the
+# tensor cores (tcgen05 implicit GEMM, 128-pixel tiles, 16-channel reduction chunks), and
+# so does the weight gradient with 17..64 output channels (a GEMM reducing over pixels);
+# the others on the FP32 pipe.  Partial pixel tiles (B H^2 not a multiple of 128) and
+# partial / several reduction chunks are included.
 @pytest.mark.parametrize('ci,co,stride,H', [(1, 32, 2, 64), (32, 64, 2, 32), (64, 64, 1, 16), (64, 32, 1, 32),
                                             (32, 2, 1, 32), (3, 5, 1, 20), (5, 17, 2, 18), (6, 20, 1, 40),
                                             (7, 33, 1, 34), (7, 32, 1, 10), (40, 64, 2, 14), (32, 48, 1, 12),
@@ -65,23 +65,25 @@ def test_conv_layer_matches_oracle(ci, co, stride, H):
     assert rel_l2(db.cpu().numpy(), rdb) < 1e-5
 
 
-# The stride-1 weight gradient with Ci <= 64 and 17..64 output channels runs on the tensor
-# cores, CTAs striding over (image, 128-row tile) chunks: batches large enough that every
-# CTA takes several chunks (both operand buffers reused); 2 and 9 output channels run the
-# FP32 kernel.
-@pytest.mark.parametrize('ci,co,H,B', [(64, 32, 32, 40), (32, 2, 64, 12), (64, 64, 16, 64), (20, 9, 24, 48),
-                                       (20, 17, 24, 48), (3, 40, 20, 40)])
-def test_weight_gradient_many_chunks(ci, co, H, B):
+# The weight gradient with Ci <= 64 and 17..64 output channels runs on the tensor cores at
+# stride 1 and 2, CTAs striding over (image, 128-row tile) chunks: batches large enough that
+# every CTA takes several chunks (both operand buffers reused); 2 and 9 output channels run
+# the FP32 kernel.
+@pytest.mark.parametrize('ci,co,H,B,stride', [(64, 32, 32, 40, 1), (32, 2, 64, 12, 1), (64, 64, 16, 64, 1),
+                                              (20, 9, 24, 48, 1), (20, 17, 24, 48, 1), (3, 40, 20, 40, 1),
+                                              (32, 64, 32, 64, 2), (1, 32, 64, 24, 2), (24, 20, 30, 48, 2)])
+def test_weight_gradient_many_chunks(ci, co, H, B, stride):
     rng = numpy.random.default_rng(ci * 7 + co)
     x = rng.normal(size=(B, ci, H, H)).astype(numpy.float32)
-    dy = rng.normal(size=(B, co, H, H)).astype(numpy.float32)
+    dy = rng.normal(size=(B, co, H // stride, H // stride)).astype(numpy.float32)
     w = C.bf16(rng.normal(0, 0.3, (co, ci, 3, 3)).astype(numpy.float32))
     xd, dyd = torch.from_numpy(x).cuda(), torch.from_numpy(dy).cuda()
     dw = torch.zeros((co, ci, 3, 3), device='cuda')
     db = torch.zeros((co,), device='cuda')
     _lib.call('phb_conv3x3_bwd_weight', xd.data_ptr(), dyd.data_ptr(), dw.data_ptr(), db.data_ptr(), B, ci, H, H, co,
-              1, st())
-    _, rdw, rdb = C.conv3x3_backward(x.astype(numpy.float64), w.astype(numpy.float64), dy.astype(numpy.float64), 1)
+              stride, st())
+    _, rdw, rdb = C.conv3x3_backward(x.astype(numpy.float64), w.astype(numpy.float64), dy.astype(numpy.float64),
+                                     stride)
     assert rel_l2(dw.cpu().numpy(), rdw) < 1e-5
     assert rel_l2(db.cpu().numpy(), rdb) < 1e-5
 
