@@ -743,11 +743,13 @@ def run_large_race(args):
                       "nrmse": res}), flush=True)
 
 
-def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3):
+def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3, scan: int = 256,
+                    batch: int = 256):
     """The large configuration as specified (32 x 1033^2 slices, 256^2 probe and detector
     x 8 modes, 65536 positions at 3 px, uint16 counts resident): LSQ-ML and gradient-engine
-    throughput over `steps` of the first iteration's mini-batches of 256 (after `warmup`),
-    device time of the group steps (fused launches + update kernels)."""
+    throughput over `steps` of the first iteration's mini-batches of `batch` (after
+    `warmup`), device time of the group steps (fused launches + update kernels).  A smaller
+    `scan` / `batch` is the reduced case of the profiling commands."""
     import torch
     from phaser_b200.synthetic import large_multislice_config, simulate_patterns
     from phaser_b200.engines.conventional import ConventionalEngine
@@ -756,7 +758,7 @@ def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3)
     from phaser_b200.sampling import Sampling
     from phaser_b200 import plan as PL
     t0 = time.perf_counter()
-    ds = large_multislice_config(seed=seed, binned=False)
+    ds = large_multislice_config(seed=seed, scan=scan, binned=False)
     t_obj = time.perf_counter() - t0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -768,9 +770,9 @@ def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3)
     n_pos = int(numpy.prod(ds.scan.shape[:-1]))
     out = {"workload": f"large multislice as specified: {S} x {ds.obj_sampling.shape[0]}^2 slices, probe and "
                        f"detector {N}^2 x 8 modes, 256x256 scan @ 3 px, 5e5 e-/pattern as uint16 counts resident "
-                       f"({pats16.numel() * 2 / 1e9:.1f} GB), batch 256",
+                       f"({pats16.numel() * 2 / 1e9:.1f} GB), batch {batch}",
            "unit": UNIT, "positions": n_pos, "object_setup_seconds": t_obj, "simulation_seconds": t_sim,
-           "sample": f"{steps} of the {-(-n_pos // 256)} mini-batches of one iteration, after {warmup}"}
+           "sample": f"{steps} of the {-(-n_pos // batch)} mini-batches of one iteration, after {warmup}"}
 
     def state_of():
         return ReconsState(iter=IterState(), wavelength=ds.wavelength,
@@ -783,14 +785,14 @@ def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3)
             props = PL.ConventionalEnginePlan(
                 noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
                 position_solver={'type': 'momentum', 'step_size': 1e-3, 'max_step_size': 0.2, 'momentum': 0.9},
-                niter=10 ** 6, grouping=256, update_positions=True)
+                niter=10 ** 6, grouping=batch, update_positions=True)
             eng = ConventionalEngine({'data': Patterns(None, ds.mask), 'state': state_of(), 'dtype': numpy.float32,
                                       'seed': 'bench-c5', 'recons_name': 'c5'}, props, patterns_on_device=pats16)
         else:
             props = PL.GradientEnginePlan(
                 solvers={'object': {'type': 'adam', 'learning_rate': 1e-2},
                          'probe': {'type': 'adam', 'learning_rate': 1e-3}},
-                noise_model={'type': 'amplitude'}, niter=10 ** 6, grouping=256)
+                noise_model={'type': 'amplitude'}, niter=10 ** 6, grouping=batch)
             eng = GradientEngine({'data': Patterns(None, ds.mask), 'state': state_of(), 'dtype': numpy.float32,
                                   'seed': 'bench-c5', 'recons_name': 'c5-grad'}, props, patterns_on_device=pats16)
         e0.record(stream)
@@ -799,7 +801,7 @@ def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3)
         e1.synchronize()
         t_pre = e0.elapsed_time(e1) / 1e3
         secs = eng.time_group_steps(1, warmup, steps, stream)
-        out[kind] = {"value": steps * 256 * S / secs, "ms_per_mini_batch": secs / steps * 1e3,
+        out[kind] = {"value": steps * batch * S / secs, "ms_per_mini_batch": secs / steps * 1e3,
                      "presolve_seconds": t_pre}
         del eng
         torch.cuda.empty_cache()
@@ -1000,6 +1002,9 @@ def main():
                     help='only the learned warm start as the benchmark describes it (single-slice optics)')
     ap.add_argument('--large-rate', action='store_true',
                     help='only the large configuration at the stated size: LSQ-ML / gradient-engine throughput')
+    ap.add_argument('--large-scan', type=int, default=256,
+                    help='--large-rate on a smaller square scan (the reduced case of the profiling commands)')
+    ap.add_argument('--large-batch', type=int, default=256, help='--large-rate mini-batch size')
     ap.add_argument('--cnn', type=int, default=0, metavar='PATTERNS',
                     help='only time the warm-start network on this many patterns (training step and inference)')
     args = ap.parse_args()
@@ -1019,7 +1024,9 @@ def main():
         torch.cuda.set_device(dev)
         print(json.dumps({"metric": "large configuration as specified, pos*slice/s",
                           "large_multislice_spec": large_spec_rate(dev, torch.cuda.current_stream(), args.steps,
-                                                                   args.warmup)}), flush=True)
+                                                                   args.warmup, scan=args.large_scan,
+                                                                   batch=args.large_batch)}),
+              flush=True)
         return
     if args.impl == 'reference':
         run_reference(args, world, rank)
