@@ -769,7 +769,7 @@ def large_spec_rate(dev, stream, steps: int = 8, warmup: int = 2, seed: int = 3,
     N, S = ds.probe.shape[-1], ds.true_object.shape[0]
     n_pos = int(numpy.prod(ds.scan.shape[:-1]))
     out = {"workload": f"large multislice as specified: {S} x {ds.obj_sampling.shape[0]}^2 slices, probe and "
-                       f"detector {N}^2 x 8 modes, 256x256 scan @ 3 px, 5e5 e-/pattern as uint16 counts resident "
+                       f"detector {N}^2 x 8 modes, {scan}x{scan} scan @ 3 px, 5e5 e-/pattern as uint16 counts resident "
                        f"({pats16.numel() * 2 / 1e9:.1f} GB), batch {batch}",
            "unit": UNIT, "positions": n_pos, "object_setup_seconds": t_obj, "simulation_seconds": t_sim,
            "sample": f"{steps} of the {-(-n_pos // batch)} mini-batches of one iteration, after {warmup}"}

@@ -18,9 +18,17 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// complex add / subtract / real scale as one packed FP32 instruction each (sm_100
+// FADD2 / FMUL2: two round-to-nearest float32 operations, the same results as two scalar
+// ones; the compiler does not pair scalar float2 arithmetic by itself)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+    unsigned long long ra = *reinterpret_cast<unsigned long long *>(&a), rb = *reinterpret_cast<unsigned long long *>(&b),
+                       rd;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+    return *reinterpret_cast<float2 *>(&rd);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
 
 // numpy.maximum(x, 0) semantics: NaN propagates (CUDA's fmaxf would drop it).
