@@ -429,8 +429,11 @@ def run_b200(args, world, rank, local):
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     traffic = ncu_traffic_per_launch(args.engine)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic if (args.scan == 64 and args.batch == 256) else None, "traffic_unit": "GB per launch (ncu)", "kernel": ("k_group<128> (fused gradient-engine mini-batch: loss + adjoint)" if args.engine == 'gradient'
+            "traffic": traffic if (args.scan == 64 and args.batch == 256) else None,
+            "traffic_unit": "GB per launch (ncu)",
+            "kernel": ("k_group<128> (fused gradient-engine mini-batch: loss + adjoint)" if args.engine == 'gradient'
                        else "k_group<128> (fused LSQ-ML mini-batch)"),
+            "launch": "one mini-batch = the forward launch and the launch resumed at the detector, timed together",
             "launch_ms": avg_ms, "launches_timed": len(fused), "bytes_per_launch": bytes_launch,
             "peak_source": f"{peak_kind} hbm_gbs", "share_of_step": sum(fused) / t_ms if t_ms else None}
     # the kernel's other bound: FP32 FFT work (5 N^2 log2 N^2 per transform, M (4 + 4/S) transforms
