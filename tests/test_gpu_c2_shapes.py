@@ -6,6 +6,8 @@ at 1e6 e- per pattern.
   * one LSQ-ML and one ePIE mini-batch of 64 positions on the full benchmark
     object grid (518^2, scan 64 x 64), from a partly reconstructed object, against
     the numpy oracle (complex64) and the float64 oracle;
+  * one gradient-engine loss + adjoint on the same group against the oracle's
+    hand-written adjoint (complex64 and float64);
   * three whole LSQ-ML iterations at batch 256 (momentum position correction)
     on a 16 x 16 scan of the same optics, compared after EVERY iteration with
     the complex64 oracle and the float64 oracle (phaser/engines/conventional/
@@ -17,11 +19,12 @@ position steps within 2e-3; whole iterations within 1e-4.  The float64 figures
 are printed (pytest -s) and bounded by the same limits."""
 import numpy
 import pytest
+import torch
 
 from oracle import phaser_np as P
 from phaser_b200 import _lib
 from phaser_b200 import plan as PL
-from phaser_b200.device import DeviceEngine
+from phaser_b200.device import DeviceEngine, NoiseSpec
 from phaser_b200.engines.conventional import ConventionalEngine
 from phaser_b200.sampling import Sampling
 from phaser_b200.state import ReconsState, ProbeState, ObjectState, IterState, Patterns
@@ -128,6 +131,48 @@ def test_c2_group_matches_oracle_and_float64(c2_group, solver):
     assert numpy.allclose(err_gpu, ref['errors'], rtol=1e-4)
     assert rel_l2(pos_gpu, ref['pos_update']) < 2e-3
     assert p64 < 2e-3
+
+
+def test_c2_gradient_group_matches_oracle_and_float64(c2_group):
+    """The gradient engine's fused loss + adjoint on the same 64 positions of the benchmark
+    dataset (amplitude noise model): loss, object / probe / position gradients against the
+    oracle's hand-written adjoint in complex64 and float64."""
+    ds, idx, pats, probe, est = c2_group
+    N = ds.probe.shape[-1]
+    n = int(numpy.prod(ds.scan.shape[:-1]))
+    full = numpy.zeros((n, N, N), numpy.float32)
+    full[idx] = pats
+    eng = DeviceEngine(probe=probe, obj=est, scan=ds.scan, patterns=full, mask=ds.mask,
+                       probe_sampling=ds.probe_sampling, obj_sampling=ds.obj_sampling,
+                       thicknesses=ds.thicknesses, wavelength=ds.wavelength, group_max=len(idx),
+                       noise=NoiseSpec('amplitude', 1e-2, 0.0, 0.1))
+    gt, sizes = eng.group_tensor([idx])
+    g_obj, g_probe, g_pos = torch.zeros_like(eng.object), torch.zeros_like(eng.probe), torch.zeros_like(eng.scan)
+    total = torch.zeros((1,), dtype=torch.float64, device=eng.device)
+    eng.status.fill_(-1)
+    eng.step('grad', gt[0], sizes[0],
+             flags=_lib.PHB_FLAG_UPDATE_OBJECT | _lib.PHB_FLAG_UPDATE_PROBE | _lib.PHB_FLAG_UPDATE_POSITION,
+             grad_object=g_obj, grad_probe=g_probe, grad_pos=g_pos, group_loss=total)
+    torch.cuda.synchronize()
+    assert int(eng.status.cpu()[0]) == -1
+    scan = ds.scan.reshape(-1, 2)[idx]
+    g32, props32 = geometry(ds, numpy.float32)
+    L, r_obj, r_probe, r_pos = P.grad_model_grads(g32, probe, est, scan, pats, ds.mask, props32, None,
+                                                 P.NoiseModel(eps=1e-2))
+    g64, props64 = geometry(ds, numpy.float64)
+    L64, f_obj, f_probe, f_pos = P.grad_model_grads(
+        g64, probe.astype(numpy.complex128), est.astype(numpy.complex128), scan.astype(numpy.float64),
+        pats.astype(numpy.float64), ds.mask.astype(numpy.float64), props64, None, P.NoiseModel(eps=1e-2))
+    go, gp, gs = g_obj.cpu().numpy(), g_probe.cpu().numpy(), g_pos.cpu().numpy()[idx]
+    print(f"\ngradient 64 positions, N=128 M=4 S=8: loss {float(total.cpu()[0]):.6e} vs oracle {float(L):.6e} "
+          f"vs float64 {float(L64):.6e}; object gradient vs oracle {rel_l2(go, r_obj):.2e}, vs float64 "
+          f"{rel_l2(go, f_obj):.2e}; probe {rel_l2(gp, r_probe):.2e} / {rel_l2(gp, f_probe):.2e}; "
+          f"positions {rel_l2(gs, r_pos):.2e} / {rel_l2(gs, f_pos):.2e}")
+    assert float(total.cpu()[0]) == pytest.approx(float(L), rel=1e-5)
+    assert float(total.cpu()[0]) == pytest.approx(float(L64), rel=1e-5)
+    assert rel_l2(go, r_obj) < 1e-4 and rel_l2(go, f_obj) < 1e-4
+    assert rel_l2(gp, r_probe) < 1e-4 and rel_l2(gp, f_probe) < 1e-4
+    assert rel_l2(gs, r_pos) < 2e-3 and rel_l2(gs, f_pos) < 2e-3
 
 
 def test_c2_lsqml_iterations_match_oracle_and_float64():

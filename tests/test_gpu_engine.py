@@ -175,6 +175,33 @@ def test_run_engine_matches_oracle(solver):
     assert numpy.allclose(state.progress.detector_errors, errors, rtol=1e-3)
 
 
+def test_run_engine_matches_oracle_n256():
+    """Two whole LSQ-ML iterations at a 256^2 probe and detector (4-CTA cluster tiles): sparse
+    shuffled groups, presolve, momentum position correction, per-iteration errors."""
+    c = make_case(seed=43, N=256, M=4, S=2, scan_shape=(3, 3))
+    props = PL.ConventionalEnginePlan(
+        noise_model={'type': 'amplitude', 'eps': 1e-2},
+        solver={'type': 'lsqml', 'beta_object': 0.9, 'beta_probe': 0.8, 'gamma': 1e-3},
+        position_solver={'type': 'momentum', 'step_size': 10.0, 'max_step_size': 0.2, 'momentum': 0.9},
+        niter=2, grouping=5, update_positions=True, calc_error_fraction=1.0)
+    state = run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                        'seed': 'engine-seed-256', 'recons_name': 't'}, props)
+    run = P.ConventionalRun(solver='lsqml', niter=2, grouping=5, seed='engine-seed-256', noise=P.NoiseModel(eps=1e-2),
+                            lsqml=P.LSQMLParams(0.9, 0.8, 1e-2, 1e-2, 1e-3), update_positions=True,
+                            position_solver='momentum', pos_step_size=10.0, pos_max_step=0.2, pos_momentum=0.9,
+                            calc_error_fraction=1.0)
+    probe, obj, scan, errors = P.run_conventional(
+        run, probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+        probe_sampling=c.probe_sampling, corner=c.osamp.corner, obj_sampling=c.osamp.sampling,
+        thicknesses=c.thick, wavelength=c.wavelength)
+    assert rel_l2(state.object.data, obj) < 1e-4
+    assert rel_l2(state.probe.data, probe) < 1e-4
+    # the positions move by ~3.5e-3 A over the two iterations: agree to ~3% of that
+    assert numpy.max(numpy.abs(scan - c.scan)) > 1e-3
+    assert numpy.max(numpy.abs(state.scan - scan)) < 1e-4
+    assert numpy.allclose(state.progress.detector_errors, errors, rtol=1e-3)
+
+
 def test_nonfinite_pattern_raises_value_error():
     c = make_case(seed=51, N=64, M=1, S=1, scan_shape=(4, 4))
     c.patterns[1, 2, 5, 5] = numpy.inf
@@ -202,14 +229,14 @@ def test_unsupported_shapes_fail_loudly():
         eng.step('epie', gt[0], sizes[0], flags=_lib.PHB_FLAG_UPDATE_OBJECT)
 
 
-@pytest.mark.parametrize('solver', ['lsqml', 'epie', 'grad'])
-def test_uint16_resident_patterns_match_float32(solver):
+@pytest.mark.parametrize('solver,N', [('lsqml', 64), ('epie', 64), ('grad', 64), ('lsqml', 256), ('grad', 256)])
+def test_uint16_resident_patterns_match_float32(solver, N):
     """Patterns held as uint16 counts give the float32 results (the kernels convert
     each count exactly): presolve rescale, one group step, errors / loss."""
-    c = make_case(seed=55, N=64, M=2, S=3)
+    c = make_case(seed=55, N=N, M=2, S=3) if N == 64 else make_case(seed=56, N=N, M=2, S=2, scan_shape=(3, 3))
     n = c.scan.shape[0] * c.scan.shape[1]
     counts = numpy.round(c.patterns * (4000.0 / c.patterns.max())).astype(numpy.uint16)
-    idx = numpy.random.default_rng(3).permutation(n)[:10].astype(numpy.int64)
+    idx = numpy.random.default_rng(3).permutation(n)[:min(10, n)].astype(numpy.int64)
     spec = NoiseSpec('poisson', 1e-3, 0.0, 0.1) if solver == 'grad' else NoiseSpec()
     out = []
     for pats in (counts, counts.astype(numpy.float32)):

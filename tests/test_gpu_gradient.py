@@ -180,6 +180,30 @@ def test_run_engine_matches_oracle_gradient_loop(name, solvers, noise):
     assert numpy.max(numpy.abs(state.scan - scan)) < 1e-4
 
 
+def test_run_engine_matches_oracle_gradient_loop_n256():
+    """Two gradient-engine iterations at a 256^2 probe and detector: Adam on object and
+    probe, SGD on positions, Poisson noise model."""
+    c = make_case(seed=92, N=256, M=2, S=2, scan_shape=(3, 3))
+    solvers = {'object': ('adam', dict(learning_rate=1e-2)), 'probe': ('adam', dict(learning_rate=1e-3)),
+               'positions': ('sgd', dict(learning_rate=5.0, momentum=0.5, nesterov=False))}
+    onoise, _ = NOISES['poisson']
+    props = PL.GradientEnginePlan(solvers={k: dict(type=kind, **sp) for (k, (kind, sp)) in solvers.items()},
+                                  noise_model={'type': 'poisson', 'eps': onoise.eps}, niter=2, grouping=5,
+                                  update_positions=True)
+    state = run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                        'seed': 'grad-seed-256', 'recons_name': 't'}, props)
+    run = P.GradientRun(solvers={(k,): v for (k, v) in solvers.items()}, niter=2, grouping=5, seed='grad-seed-256',
+                        noise=onoise, update_positions=True)
+    probe, obj, scan, losses = P.run_gradient(
+        run, probe=c.probe, obj=c.obj, scan=c.scan, patterns=c.patterns, mask=c.mask,
+        probe_sampling=c.probe_sampling, corner=c.osamp.corner, obj_sampling=c.osamp.sampling,
+        thicknesses=c.thick, wavelength=c.wavelength)
+    assert numpy.allclose(state.progress.detector_errors, losses, rtol=1e-4)
+    assert rel_l2(state.object.data, obj) < 1e-4
+    assert rel_l2(state.probe.data, probe) < 1e-4
+    assert numpy.max(numpy.abs(state.scan - scan)) < 1e-4
+
+
 def test_autograd_function_matches_oracle_adjoint():
     """torch.autograd through the hand-written adjoint: loss, and the gradients of
     2 * loss with respect to object, probe and scan, against the oracle."""
