@@ -169,7 +169,9 @@ def test_c2_gradient_group_matches_oracle_and_float64(c2_group):
           f"{rel_l2(go, f_obj):.2e}; probe {rel_l2(gp, r_probe):.2e} / {rel_l2(gp, f_probe):.2e}; "
           f"positions {rel_l2(gs, r_pos):.2e} / {rel_l2(gs, f_pos):.2e}")
     assert float(total.cpu()[0]) == pytest.approx(float(L), rel=1e-5)
-    assert float(total.cpu()[0]) == pytest.approx(float(L64), rel=1e-5)
+    # the loss is a float32 sum of 64 x 128^2 terms: numpy's complex64 evaluation is 9e-6 from
+    # float64 itself
+    assert float(total.cpu()[0]) == pytest.approx(float(L64), rel=5e-5)
     assert rel_l2(go, r_obj) < 1e-4 and rel_l2(go, f_obj) < 1e-4
     assert rel_l2(gp, r_probe) < 1e-4 and rel_l2(gp, f_probe) < 1e-4
     assert rel_l2(gs, r_pos) < 2e-3 and rel_l2(gs, f_pos) < 2e-3
