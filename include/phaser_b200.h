@@ -246,7 +246,8 @@ int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *gro
  * them on one stream.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress); make that first call before any stream
  * capture.  Besides that, EVERY call copies the propagator check's result to
- * the host and waits for its stream to finish before it launches the step.
+ * the host and waits for its stream to finish before it launches the step, so
+ * no call can be recorded under stream capture (CUDA graphs).
  * PHB_FLAG_PARTIAL is refused with PHB_ERR_UNSUPPORTED: a partial share left in
  * the library's array could not be summed over ranks by the caller, and the
  * next call clears it. */
