@@ -430,6 +430,13 @@ int phb_position_update(float *scan, float *pos_update, float *momentum_state, i
                         float momentum, double obj_min_y, double obj_min_x,
                         double obj_max_y, double obj_max_x, int32_t *n_outside, void *stream);
 
+/* Count positions completely outside the object (-> *n_outside, device int): the
+ * check of phaser/utils/object.py:288-289 on the device, for the gradient engine's
+ * position updates (phaser/engines/gradient/run.py:330-349), so an iteration needs no
+ * host copy of the scan. */
+int phb_count_outside(const float *scan, int64_t n_pos, double obj_min_y, double obj_min_x, double obj_max_y,
+                      double obj_max_x, int32_t *n_outside, void *stream);
+
 /* Start of an iteration: *status = -1, errors[0:n] = NaN. */
 int phb_iteration_reset(int32_t *status, float *errors, int64_t n, void *stream);
 

@@ -182,6 +182,7 @@ _SIGNATURES = {
                                     c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_nanmean': (c_i32, [c_void_p, c_i64, c_void_p, c_void_p, c_void_p]),
     'phb_iteration_reset': (c_i32, [c_void_p, c_void_p, c_i64, c_void_p]),
+    'phb_count_outside': (c_i32, [c_void_p, c_i64, c_f64, c_f64, c_f64, c_f64, c_void_p, c_void_p]),
     'phb_iteration_report': (c_i32, [c_void_p, c_void_p, c_void_p, c_i64, c_void_p, c_void_p]),
     'phb_kernel_launches': (c_i64, []),
     'phb_fp32_peak': (c_i32, [c_i32, ctypes.POINTER(c_f64), ctypes.POINTER(c_f32), c_void_p]),

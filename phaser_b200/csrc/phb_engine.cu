@@ -1313,6 +1313,19 @@ __global__ void __launch_bounds__(1024) k_nanmean(const float *v, int64_t n, dou
     }
 }
 
+// positions completely outside the object (the reference's check in utils/object.py:288-289)
+__global__ void __launch_bounds__(1024) k_count_outside(const float *scan, int64_t n, double y0, double x0,
+                                                        double y1, double x1, int32_t *n_out) {
+    __shared__ double red[32];
+    int outside = 0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double py = scan[2 * i], px = scan[2 * i + 1];
+        outside += (py < y0) || (py > y1) || (px < x0) || (px > x1);
+    }
+    const double tot = block_sum1<1024>((double)outside, red);
+    if (threadIdx.x == 0) *n_out = (int32_t)tot;
+}
+
 __global__ void k_iteration_reset(int32_t *status, float *errors, int64_t n) {
     const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i0 == 0) *status = -1;
@@ -1834,6 +1847,14 @@ int phb_position_update(float *scan, float *pos_update, float *momentum_state, i
     k_position_update<<<1, 1024, 0, (cudaStream_t)stream>>>(scan, pos_update, momentum_state, n_pos, use_momentum,
                                                             step_size, max_step, momentum, obj_min_y, obj_min_x,
                                                             obj_max_y, obj_max_x, n_outside);
+    return check_launch();
+}
+
+int phb_count_outside(const float *scan, int64_t n_pos, double obj_min_y, double obj_min_x, double obj_max_y,
+                      double obj_max_x, int32_t *n_outside, void *stream) {
+    if (!scan || !n_outside || n_pos < 1) return PHB_ERR_INVALID_ARG;
+    k_count_outside<<<1, 1024, 0, (cudaStream_t)stream>>>(scan, n_pos, obj_min_y, obj_min_x, obj_max_y, obj_max_x,
+                                                          n_outside);
     return check_launch();
 }
 

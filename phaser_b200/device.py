@@ -283,6 +283,13 @@ class DeviceEngine:
                   float(max_step) if max_step is not None else -1.0, float(momentum),
                   float(lo[0]), float(lo[1]), float(hi[0]), float(hi[1]), self.n_outside.data_ptr(), _stream())
 
+    def count_outside(self) -> None:
+        """Positions completely outside the object -> self.n_outside (device), the bounds
+        of position_update."""
+        lo, hi = self.obj_sampling.check_bounds(numpy.asarray(self.probe_extent()) / 2.)
+        _lib.call('phb_count_outside', self.scan.data_ptr(), self.n_pos, float(lo[0]), float(lo[1]), float(hi[0]),
+                  float(hi[1]), self.n_outside.data_ptr(), _stream())
+
     def probe_extent(self) -> numpy.ndarray:
         return self.probe_sampling * self.N
 

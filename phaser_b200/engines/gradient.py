@@ -313,8 +313,10 @@ class GradientEngine:
         self.pos_step = torch.zeros_like(eng.scan)
         self.losses = torch.zeros((len(self.groups),), dtype=torch.float64, device=dev)
         self.loss_mean = torch.zeros((1,), dtype=torch.float64, device=dev)
-        self.loss_host = torch.zeros((2,), dtype=torch.float64).pin_memory()
-        self.status_host = torch.zeros((1,), dtype=torch.int32).pin_memory()
+        # per iteration parity (iteration i reads what iteration i wrote while i + 1 runs):
+        # mean loss; status and the count of positions outside the object
+        self.loss_hosts = [torch.zeros((2,), dtype=torch.float64).pin_memory() for _ in range(2)]
+        self.status_hosts = [torch.zeros((2,), dtype=torch.int32).pin_memory() for _ in range(2)]
         self.probe_int = 0.0
         self.start_i = int(state.iter.total_iter)
         self.fused_events: t.Optional[t.List[t.Tuple[int, int]]] = None
@@ -411,12 +413,17 @@ class GradientEngine:
                 eng.tilt.add_(self.tilt_step)
         for con in self.iter_cons:
             con.apply_iter()
-        self.loss_host[:1].copy_(self.loss_mean, non_blocking=True)
-        self.status_host.copy_(eng.status, non_blocking=True)
+        it_pos = 'positions' in iter_vars
+        if it_pos:   # positions outside the object, counted on the device
+            eng.count_outside()
+        self.loss_hosts[i % 2][:1].copy_(self.loss_mean, non_blocking=True)
+        self.status_hosts[i % 2][:1].copy_(eng.status, non_blocking=True)
+        if it_pos:
+            self.status_hosts[i % 2][1:].copy_(eng.n_outside, non_blocking=True)
         if not sync:
             return None
         torch.cuda.current_stream().synchronize()
-        return self.check(i, 'positions' in iter_vars)
+        return self.check(i, it_pos)
 
     def _grad_step(self, group: torch.Tensor, B: int, flags: int, gi: int, events, iter_vars, group_loss,
                    probe_int: float) -> None:
@@ -433,19 +440,18 @@ class GradientEngine:
                     grad_tilt_scale=-1.0 / (probe_int * B))
 
     def check(self, i: int, it_pos: bool = True) -> float:
+        """Read iteration i's report (after the device has finished iteration i)."""
         state, eng = self.state, self.eng
-        bad_group = int(self.status_host[0])
+        rep = self.status_hosts[i % 2]
+        bad_group = int(rep[0])
         if bad_group >= _lib.PHB_STATUS_INTERNAL:
             raise RuntimeError(f"internal error: fused kernel aborted in group {bad_group - _lib.PHB_STATUS_INTERNAL}")
         if bad_group >= 0:
             raise ValueError(f"NaN or inf encountered in object or probe, group {bad_group}")
-        if it_pos:
-            scan = eng.scan.cpu().numpy()
-            lo, hi = eng.obj_sampling.check_bounds(numpy.asarray(eng.probe_extent()) / 2.)
-            outside = numpy.any((scan < lo) | (scan > hi), axis=-1)
-            if numpy.any(outside):
-                raise ValueError(f"{int(numpy.sum(outside))}/{eng.n_pos} probe positions completely outside object")
-        loss = float(self.loss_host[0])
+        n_out = int(rep[1])
+        if it_pos and n_out > 0:
+            raise ValueError(f"{n_out}/{eng.n_pos} probe positions completely outside object")
+        loss = float(self.loss_hosts[i % 2][0])
         state.progress.iters = numpy.concatenate([state.progress.iters, [i + self.start_i]])
         state.progress.detector_errors = numpy.concatenate([state.progress.detector_errors, [loss]])
         _call(self.observer, 'update_iteration', state, i, self.niter, loss)

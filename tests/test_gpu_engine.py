@@ -202,6 +202,19 @@ def test_run_engine_matches_oracle_n256():
     assert numpy.allclose(state.progress.detector_errors, errors, rtol=1e-3)
 
 
+def test_positions_leaving_the_object_raise_value_error():
+    """An unclipped position step that throws the probe off the object ends the run with
+    the reference's error (utils/object.py:288-289), counted on the device."""
+    c = make_case(seed=44, N=64, M=1, S=1, scan_shape=(4, 4))
+    props = PL.ConventionalEnginePlan(
+        noise_model={'type': 'amplitude'}, solver={'type': 'lsqml'},
+        position_solver={'type': 'momentum', 'step_size': 1e9, 'max_step_size': None, 'momentum': 0.0},
+        niter=2, grouping=8, update_positions=True)
+    with pytest.raises(ValueError, match='probe positions completely outside object'):
+        run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                    'seed': 'outside', 'recons_name': 't'}, props)
+
+
 def test_nonfinite_pattern_raises_value_error():
     c = make_case(seed=51, N=64, M=1, S=1, scan_shape=(4, 4))
     c.patterns[1, 2, 5, 5] = numpy.inf

@@ -204,6 +204,18 @@ def test_run_engine_matches_oracle_gradient_loop_n256():
     assert numpy.max(numpy.abs(state.scan - scan)) < 1e-4
 
 
+def test_positions_leaving_the_object_raise_value_error():
+    """A position step that throws the probe off the object ends the run with the
+    reference's error (utils/object.py:288-289), counted on the device."""
+    c = make_case(seed=93, N=64, M=1, S=1, scan_shape=(4, 4))
+    props = PL.GradientEnginePlan(
+        solvers={'object': {'type': 'sgd', 'learning_rate': 1.0}, 'positions': {'type': 'sgd', 'learning_rate': 1e9}},
+        noise_model={'type': 'amplitude'}, niter=2, grouping=8, update_positions=True)
+    with pytest.raises(ValueError, match='probe positions completely outside object'):
+        run_engine({'data': Patterns(c.patterns, c.mask), 'state': make_state(c), 'dtype': numpy.float32,
+                    'seed': 'outside', 'recons_name': 't'}, props)
+
+
 def test_autograd_function_matches_oracle_adjoint():
     """torch.autograd through the hand-written adjoint: loss, and the gradients of
     2 * loss with respect to object, probe and scan, against the oracle."""
