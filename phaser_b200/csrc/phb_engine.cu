@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             // ------------------------------------------- incident wave of slice s (R layout)
             const CutView<N> cv = load_cv();
             const float2 *Os = a.object + (size_t)s * a.H * a.W;
-            if (s == 0 && upd_pos) {
+            if (s == 0 && upd_pos && !grad) {
                 float n0 = 0.f;
 #pragma unroll
                 for (int u = 0; u < U; ++u)
@@ -712,7 +712,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                                     t4[2] += c2 * o2;
                                     t4[3] += (c2 * o2) * o2;
                                 }
-                                if (upd_pos) ps[f] = c;   // exit-wave update of slice 0 for the position step
+                                if (upd_pos && !grad) ps[f] = c;   // exit-wave update of slice 0 for the position step
                             }
                             v[u][q] = cmulc(c, o);
                         }
@@ -804,7 +804,7 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
                 load_prop(s - 1);
                 fwd = true;
                 phase = PH_BPROP;
-            } else if (upd_probe) {
+            } else if (upd_probe || (grad && upd_pos)) {   // gradient engine: positions from this spectrum
                 fwd = true;
                 phase = PH_PROBE;
             } else if (upd_pos) {
@@ -882,14 +882,40 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
             --s;
         } else if (phase == PH_PROBE) {
             // ------------------------------------------- sum_b fft2(dP) conj(H_b) (solvers.py:265, 484)
-            float2 *ap = a.acc_probe + (size_t)m * NN;
+            if (upd_probe) {
+                float2 *ap = a.acc_probe + (size_t)m * NN;
 #pragma unroll
-            for (int u = 0; u < U; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const float2 h = cmul(hy[I::ky(u, e)], hx[I::kx(u, e)]);
-                    atomic_add_c(ap + I::flat(u, e), cscale(cmulc(v[u][e], h), inv_n));
+                    for (int e = 0; e < E; ++e) {
+                        const float2 h = cmul(hy[I::ky(u, e)], hx[I::kx(u, e)]);
+                        atomic_add_c(ap + I::flat(u, e), cscale(cmulc(v[u][e], h), inv_n));
+                    }
+            }
+            if constexpr (grad) {
+                if (upd_pos) {
+                    // The gradient engine's position gradient is sum_r Re(conj(chi) D_dir O_0) alone (no
+                    // step-size denominator), D_dir = ifft2(DFT(P_m)/N^2 H_b (-2 pi i k_dir)).  By Parseval
+                    // it is sum_k 2 pi k_dir Im(conj(F) g), F = fft2(chi conj(O_0)) (this spectrum),
+                    // g = DFT(P_m)/N^2 H_b: no inverse transforms and no real-space pass.
+                    const float2 *pk = a.probe_k + (size_t)m * NN;
+                    const float twopi = 6.283185307179586f;
+                    float t2[2] = {0.f, 0.f};
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int e = 0; e < E; ++e) {
+                            const int ky = I::ky(u, e), kx = I::kx(u, e);
+                            const float2 g = cmul(__ldg(pk + I::flat(u, e)), cmul(hy[ky], hx[kx]));
+                            const float im = v[u][e].x * g.y - v[u][e].y * g.x;   // Im(conj(F) g)
+                            t2[0] += (twopi * a.fy[ky]) * im;
+                            t2[1] += (twopi * a.fx[kx]) * im;
+                        }
+                    warp_atomic_sum(sums + a.o_pnum + 2 * b, (double)t2[0]);
+                    warp_atomic_sum(sums + a.o_pnum + 2 * b + 1, (double)t2[1]);
                 }
+                return;
+            }
             if (!upd_pos) return;
             load_probe_spectrum(0);
             fwd = false;
