@@ -17,8 +17,8 @@
 //    into a per-position intensity buffer with float32 atomics; the second launch
 //    resumes at the detector with the summed intensity and runs the constraint and
 //    the adjoint.  The CTAs of a launch are independent, so they run without
-//    clusters on every SM (a 4-CTA cluster fits only 4 of a GPC's SMs per 4: 132
-//    of 148 SMs).  ePIE keeps the M CTAs of a position in one cluster: its far
+//    clusters on every SM (4-CTA clusters of these 157 KB CTAs placed only 33 clusters,
+//    132 of the 148 SMs).  ePIE keeps the M CTAs of a position in one cluster: its far
 //    field and its per-slice maximum over the modes go through distributed shared
 //    memory;
 //  * object / probe updates are accumulated during the pass and applied by
@@ -28,8 +28,11 @@
 //  * step-size numerators / denominators and the position-gradient sums are
 //    accumulated in float64 (block reduce, then one float64 atomic per CTA);
 //  * N = 256: a tile needs four SMs (512 KB of complex64), so a cluster of 4 CTAs
-//    holds one (position, mode), one quadrant / polyphase component each (the
-//    4-CTA transform of phb_fft.cuh), with the same two-launch far field.
+//    holds one (position, mode), one 128 x 128 polyphase part each in real space and
+//    a quarter of the spectrum in Fourier space (the 4-CTA transform of phb_fft.cuh),
+//    with the same two-launch far field.  The gradient engine's position gradient
+//    needs no step-size denominator, so it is formed from the probe-gradient spectrum
+//    by Parseval (PH_PROBE) instead of by two more transforms.
 #include <cooperative_groups.h>
 
 #include "phb_fft.cuh"
@@ -266,8 +269,8 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     constexpr bool lsqml = mode == MODE_LSQML, epie = mode == MODE_EPIE, grad = mode == MODE_GRAD;
     constexpr bool QUAD = N == 256;   // 4 CTAs per (position, mode)
     // Far field through global memory (two launches): the modes of a position are then
-    // independent CTAs, launched without clusters, and every SM takes work (a cluster of 4
-    // fits only 4 of a GPC's SMs per 4).  ePIE keeps its modes in one cluster: its
+    // independent CTAs, launched without clusters, and every SM takes work (4-CTA clusters
+    // occupied only 132 of the 148 SMs).  ePIE keeps its modes in one cluster: its
     // per-slice maximum over the modes goes through distributed shared memory.
     constexpr bool SPLIT = mode != MODE_EPIE;
     static_assert(!QUAD || (mode != MODE_EPIE && mode != MODE_PRE_EPIE), "ePIE needs the modes in one cluster");
@@ -1499,7 +1502,7 @@ static int launch_group_mode(const GroupArgs &a, cudaStream_t st) {
             return record_cuda(cudaGetLastError());
         configured = true;
     }
-    // N = 256: one cluster of 4 CTAs (the quadrants) per (position, mode); ePIE at N <= 128:
+    // N = 256: one cluster of 4 CTAs (the polyphase parts) per (position, mode); ePIE at N <= 128:
     // one cluster of M CTAs (the modes) per position; otherwise independent CTAs
     constexpr unsigned C = TileCfg<N>::CTAS;
     const unsigned cluster = C > 1 ? C : (MODE == MODE_EPIE ? (unsigned)a.M : 1u);
