@@ -996,15 +996,30 @@ __global__ void k_finalize(const FinArgs f) {
     __shared__ double red[2][32];
     const int tid = threadIdx.x;
     if (f.mode == MODE_LSQML) {
-        for (int s = tid; s < f.S; s += blockDim.x) {
+        // coef[k] for the S slices then the M modes: sum over the group's positions of the
+        // per-position numerators, split over the block (up to 64 k at a time, blockDim / n
+        // threads per k, each a contiguous run of positions) and combined in a fixed order
+        __shared__ double part[256];
+        const int K = f.S + f.M;
+        for (int k0 = 0; k0 < K; k0 += 64) {
+            const int n = min(64, K - k0), parts = (int)blockDim.x / n;
+            const int k = k0 + tid % n, pi = tid / n;
             double acc = 0.0;
-            for (int b = 0; b < f.B; ++b) acc += sums[SI.numO + (int64_t)b * f.S + s];
-            f.coef[s] = (double)f.beta_object * acc / (sums[SI.denO + s] + (double)f.gamma);
-        }
-        for (int m = tid; m < f.M; m += blockDim.x) {
-            double acc = 0.0;
-            for (int b = 0; b < f.B; ++b) acc += sums[SI.numP + (int64_t)b * f.M + m];
-            f.coef[f.S + m] = (double)f.beta_probe * acc / (sums[SI.denP] + (double)f.gamma);
+            if (pi < parts) {
+                const int b0 = (f.B * pi) / parts, b1 = (f.B * (pi + 1)) / parts;
+                for (int b = b0; b < b1; ++b)
+                    acc += k < f.S ? sums[SI.numO + (int64_t)b * f.S + k] : sums[SI.numP + (int64_t)b * f.M + (k - f.S)];
+            }
+            part[tid] = acc;
+            __syncthreads();
+            if (tid < n) {
+                double s = 0.0;
+                for (int q = 0; q < parts; ++q) s += part[q * n + tid];
+                const int kk = k0 + tid;
+                f.coef[kk] = kk < f.S ? (double)f.beta_object * s / (sums[SI.denO + kk] + (double)f.gamma)
+                                      : (double)f.beta_probe * s / (sums[SI.denP] + (double)f.gamma);
+            }
+            __syncthreads();
         }
     }
     const bool pos = (f.flags & PHB_FLAG_UPDATE_POSITION) && (f.mode <= MODE_GRAD);
