@@ -958,6 +958,9 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
 }
 
 // ---------------------------------------------------------------- group_obj_mag
+// positions split over gridDim.y: each thread walks B / GOM_SPLIT positions (its loads of
+// different positions are independent; more splits, more of them in flight per SM)
+constexpr int GOM_SPLIT = 32;
 // gom[r, c] += sum_b |prod_s O_s[y0_b + r, x0_b + c]|^2  (solvers.py:203)
 template <int N>
 __global__ void k_gom(const GroupArgs a, float *out) {
@@ -1630,7 +1633,7 @@ static int presolve(const phb_engine *e, const int64_t *group, int B, int solver
     a.pre_den = den;
     a.illum = (mode == MODE_PRE_LSQML) ? e->new_probe_mag : nullptr;
     if (mode == MODE_PRE_LSQML && e->new_obj_mag) {
-        k_gom<N><<<dim3((N * N + 255) / 256, 8), 256, 0, st>>>(a, e->new_obj_mag);
+        k_gom<N><<<dim3((N * N + 255) / 256, GOM_SPLIT), 256, 0, st>>>(a, e->new_obj_mag);
         if ((rc = check_launch())) return rc;
     }
     return launch_group<N>(a, st);
@@ -1681,7 +1684,7 @@ static int solver_group(const phb_engine *e, const phb_step *sp, const int64_t *
         if (!upd_obj && !e->new_probe_mag) a.illum = nullptr;
         if (upd_probe || e->new_obj_mag) {
             if ((rc = record_cuda(cudaMemsetAsync(w.gom, 0, (size_t)N * N * sizeof(float), st)))) return rc;
-            k_gom<N><<<dim3((N * N + 255) / 256, 8), 256, 0, st>>>(a, w.gom);
+            k_gom<N><<<dim3((N * N + 255) / 256, GOM_SPLIT), 256, 0, st>>>(a, w.gom);
             if ((rc = check_launch())) return rc;
         }
     } else {
