@@ -1095,11 +1095,11 @@ struct ObjApplyArgs {
     int update;
 };
 
-__global__ void k_obj_apply(const ObjApplyArgs a) {
+// blocks [0, nblocks) of a grid-stride loop over the S*H*W object values, this block = blk
+__device__ __forceinline__ void obj_apply_body(const ObjApplyArgs &a, int64_t blk, int64_t nblocks) {
     const int64_t total = (int64_t)a.S * a.HW;
     bool bad = false;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = blk * blockDim.x + threadIdx.x; i < total; i += nblocks * blockDim.x) {
         float2 o = a.object[i];
         if (a.update) {
             const float2 acc = a.acc[i];
@@ -1124,6 +1124,8 @@ __global__ void k_obj_apply(const ObjApplyArgs a) {
     if (bad && a.status) atomicCAS(a.status, -1, a.group_index);
 }
 
+__global__ void k_obj_apply(const ObjApplyArgs a) { obj_apply_body(a, blockIdx.x, gridDim.x); }
+
 // ---------------------------------------------------------------- probe apply / spectrum refresh
 struct ProbeApplyArgs {
     int mode, M, B;
@@ -1142,8 +1144,9 @@ struct ProbeApplyArgs {
 
 // One CTA per mode: P_m += update (LSQ-ML solvers.py:262-269, ePIE 483-485, or the gradient
 // output), then refresh the cached spectrum DFT(P_m)/N^2 in K order for the next group.
+// mode m's CTA (N = 256: the 4-CTA cluster of mode m); all threads of the CTA call it
 template <int N>
-__global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApplyArgs a) {
+__device__ __forceinline__ void probe_apply_body(const ProbeApplyArgs &a, int m) {
     using I = Idx<N>;
     constexpr int U = I::U, E = I::E, NN = N * N, CTAS = TileCfg<N>::CTAS;
     extern __shared__ float4 smem_raw[];
@@ -1152,7 +1155,6 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
     float *fred = reinterpret_cast<float *>(twid + TileCfg<N>::TW);
     fft_init_twiddles<N>(twid);
     __syncthreads();
-    const int m = blockIdx.x / CTAS;   // one CTA (N = 256: one 4-CTA cluster) per mode
     float2 *P = a.probe + (size_t)m * NN;
     float2 v[U][E];
     bool bad = false;
@@ -1210,6 +1212,26 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApply
         for (int e = 0; e < E; ++e) a.probe_k[(size_t)m * NN + I::flat(u, e)] = cscale(v[u][e], sc);
     if (bad && a.status) atomicCAS(a.status, -1, a.group_index);
     (void)fred;
+}
+
+template <int N>
+__global__ void __launch_bounds__(FFT_THREADS, 1) k_probe_apply(const ProbeApplyArgs a) {
+    probe_apply_body<N>(a, (int)(blockIdx.x / TileCfg<N>::CTAS));
+}
+
+// N <= 128: the probe and object updates of a mini-batch are independent, so one launch
+// runs both -- CTAs [0, M) the probe modes (one 128^2 transform pair each), the rest a
+// grid-stride pass over the object -- and the object work fills the SMs the M probe CTAs
+// leave idle instead of waiting in the stream for them.
+template <int N>
+__global__ void __launch_bounds__(FFT_THREADS, 1) k_apply(const ObjApplyArgs o, const ProbeApplyArgs p,
+                                                          int probe_ctas, int obj_on) {
+    static_assert(TileCfg<N>::CTAS == 1, "one CTA per probe mode");
+    if ((int)blockIdx.x < probe_ctas) {
+        probe_apply_body<N>(p, (int)blockIdx.x);
+        return;
+    }
+    if (obj_on) obj_apply_body(o, (int64_t)blockIdx.x - probe_ctas, (int64_t)gridDim.x - probe_ctas);
 }
 
 // ---------------------------------------------------------------- propagator factors
@@ -1434,6 +1456,11 @@ static int configure_kernels() {
     if (cudaFuncSetAttribute(k_probe_apply<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)fft_smem_bytes<N>()) != cudaSuccess)
         rc = record_cuda(cudaGetLastError());
+    if constexpr (TileCfg<N>::CTAS == 1) {
+        if (!rc && cudaFuncSetAttribute(k_apply<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)fft_smem_bytes<N>()) != cudaSuccess)
+            rc = record_cuda(cudaGetLastError());
+    }
     done = rc;
     return rc;
 }
@@ -1737,8 +1764,10 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
     k_finalize<<<1, 256, 0, st>>>(f);
     if ((rc = check_launch())) return rc;
 
-    if (mode != MODE_GRAD && (upd_obj || illum)) {
-        ObjApplyArgs o{};
+    const bool obj_on = mode != MODE_GRAD && (upd_obj || illum);
+    const bool probe_on = upd_probe || (mode == MODE_LSQML && e->new_obj_mag);
+    ObjApplyArgs o{};
+    if (obj_on) {
         o.mode = mode;
         o.S = e->S;
         o.HW = e->H * e->W;
@@ -1752,14 +1781,9 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
         o.status = sp->status;
         o.group_index = sp->group_index;
         o.update = upd_obj;
-        const int64_t total = (int64_t)e->S * e->H * e->W;
-        int64_t g = (total + 255) / 256;
-        if (g > 148 * 16) g = 148 * 16;
-        k_obj_apply<<<(unsigned)g, 256, 0, st>>>(o);
-        if ((rc = check_launch())) return rc;
     }
-    if (upd_probe || (mode == MODE_LSQML && e->new_obj_mag)) {
-        ProbeApplyArgs p{};
+    ProbeApplyArgs p{};
+    if (probe_on) {
         p.mode = mode;
         p.M = e->M;
         p.B = B;
@@ -1778,6 +1802,23 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
         p.group_index = sp->group_index;
         p.update = upd_probe;
         if (mode == MODE_GRAD && !sp->grad_probe) p.update = 0;
+    }
+    const int64_t total = (int64_t)e->S * e->H * e->W;
+    if constexpr (TileCfg<N>::CTAS == 1) {
+        if (obj_on && probe_on) {   // one launch: M probe CTAs + object CTAs on the other SMs
+            int64_t g = (total + FFT_THREADS - 1) / FFT_THREADS;
+            if (g > 148 - e->M) g = 148 - e->M > 1 ? 148 - e->M : 1;   // one wave beside the probe CTAs
+            k_apply<N><<<(unsigned)(e->M + g), FFT_THREADS, fft_smem_bytes<N>(), st>>>(o, p, e->M, 1);
+            return check_launch();
+        }
+    }
+    if (obj_on) {
+        int64_t g = (total + 255) / 256;
+        if (g > 148 * 16) g = 148 * 16;
+        k_obj_apply<<<(unsigned)g, 256, 0, st>>>(o);
+        if ((rc = check_launch())) return rc;
+    }
+    if (probe_on) {
         if ((rc = launch_probe_apply<N>(p, st))) return rc;
     }
     return PHB_OK;
