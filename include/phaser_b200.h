@@ -117,6 +117,10 @@ int phb_fourier_mask_c64(void *arr, int64_t batch, int64_t N, const float *mask,
 #define PHB_FLAG_CALC_ERROR      8
 
 #define PHB_STATUS_INTERNAL (1 << 30)   /* flag bit in phb_step.status: kernel aborted its program */
+/* flag bit in phb_step.status, set only by the bounds-checking build of the library
+ * (compiled with -DPHB_BOUNDS_CHECK=1: libphaser_b200_bounds.so): a group index outside
+ * [0, n_pos); the position is skipped instead of read or written out of bounds */
+#define PHB_STATUS_BOUNDS (1 << 29)
 
 typedef struct phb_engine {
     /* sizes */
@@ -167,7 +171,8 @@ typedef struct phb_step {
     void  *grad_probe;    /* gradient solver: (M, N, N) complex64 accumulator */
     float *grad_pos;      /* gradient solver: (n_pos, 2) float32 dL/d(y, x) */
     int32_t *status;      /* device int, sticky, -1 = fine: the first group index that produced NaN/inf,
-                             or PHB_STATUS_INTERNAL | group index if a kernel aborted (internal error) */
+                             or PHB_STATUS_INTERNAL | group index if a kernel aborted (internal error),
+                             or PHB_STATUS_BOUNDS | group index (bounds-checking build only) */
     int32_t group_index;  /* index of this group within the iteration (for `status`) */
     const float *group_patterns; /* optional (B, N, N): this group's patterns in group order, read
                                     instead of patterns[group[b]] (host-streamed data) */

@@ -2,6 +2,11 @@
 
 The library is built in-tree by `phaser_b200.build`.  There is no fallback:
 if the shared object is missing or a call fails, an exception is raised.
+
+With PHASER_B200_BOUNDS_CHECK=1 in the environment the bounds-checking build
+(libphaser_b200_bounds.so, same entry points) is loaded instead: its kernels
+report a position index outside [0, n_pos) as PHB_STATUS_BOUNDS in the step's
+status, which the engines raise as IndexError.
 """
 from __future__ import annotations
 
@@ -11,6 +16,7 @@ from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / 'libphaser_b200.so'
+BOUNDS_LIB_PATH = _PKG / 'libphaser_b200_bounds.so'
 
 PHB_OK = 0
 PHB_ERR_INVALID_ARG = 1
@@ -34,6 +40,7 @@ PHB_FLAG_CALC_ERROR = 8
 PHB_FLAG_PARTIAL = 16
 PHB_FLAG_UPDATE_TILT = 32
 PHB_STATUS_INTERNAL = 1 << 30
+PHB_STATUS_BOUNDS = 1 << 29
 
 c_void_p = ctypes.c_void_p
 c_i32 = ctypes.c_int32
@@ -213,7 +220,10 @@ def load(path: os.PathLike | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path is not None else LIB_PATH
+    if path is not None:
+        p = Path(path)
+    else:
+        p = BOUNDS_LIB_PATH if os.environ.get('PHASER_B200_BOUNDS_CHECK', '0') == '1' else LIB_PATH
     if not p.exists():
         raise ImportError(f"{p} is missing: build it with `python -m phaser_b200.build` "
                           "(the B200 backend has no CPU fallback)")
@@ -224,6 +234,19 @@ def load(path: os.PathLike | None = None) -> ctypes.CDLL:
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def raise_for_status(bad_group: int) -> None:
+    """Raise for a step status word read back from the device (-1: fine).  The
+    flag bits say what the group index beside them produced: an aborted kernel
+    program, a position index outside the scan (bounds-checking build), or NaN / inf
+    in the updated object or probe (run.py:281 check_finite)."""
+    if bad_group >= PHB_STATUS_INTERNAL:
+        raise RuntimeError(f"internal error: fused kernel aborted in group {bad_group - PHB_STATUS_INTERNAL}")
+    if bad_group >= PHB_STATUS_BOUNDS:
+        raise IndexError(f"position index outside [0, n_pos) in group {bad_group - PHB_STATUS_BOUNDS}")
+    if bad_group >= 0:
+        raise ValueError(f"NaN or inf encountered in object or probe, group {bad_group}")
 
 
 def call(name: str, *args) -> None:

@@ -71,8 +71,9 @@ class MultisliceLoss(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, grad_out: torch.Tensor):
-        if int(ctx.status.cpu()[0]) >= _lib.PHB_STATUS_INTERNAL:
-            raise RuntimeError("internal error: the fused kernel aborted")
+        status = int(ctx.status.cpu()[0])
+        if status >= _lib.PHB_STATUS_BOUNDS:   # an aborted kernel, or a position outside the scan
+            _lib.raise_for_status(status)
         saved = list(ctx.saved_tensors)
         out = []
         for need in ctx.which:

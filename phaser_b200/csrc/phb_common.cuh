@@ -36,6 +36,29 @@ __device__ __forceinline__ float np_max0(float x) { return (x != x) ? x : (x > 0
 
 __device__ __forceinline__ bool finite2(float2 a) { return isfinite(a.x) && isfinite(a.y); }
 
+// ------------------------------------------------------ bounds-checking build
+// Compiled with -DPHB_BOUNDS_CHECK=1 (libphaser_b200_bounds.so), every kernel that
+// dereferences a caller-supplied position index (a row of `group`) checks it against
+// n_pos first: an index outside [0, n_pos) is recorded (bit 2 of the workspace error
+// word, PHB_STATUS_BOUNDS | group index in the step's status) and the position is
+// skipped instead of read or written out of bounds.  The default build has no checks.
+#ifndef PHB_BOUNDS_CHECK
+#define PHB_BOUNDS_CHECK 0
+#endif
+__device__ __forceinline__ bool pos_ok(long long p, long long n_pos) {
+#if PHB_BOUNDS_CHECK
+    return p >= 0 && p < n_pos;
+#else
+    (void)p;
+    (void)n_pos;
+    return true;
+#endif
+}
+__device__ __forceinline__ void report_bounds(int32_t *err_word, int32_t *status, int32_t group_index) {
+    if (err_word) atomicOr(err_word, 2);
+    if (status) atomicCAS(status, -1, PHB_STATUS_BOUNDS | group_index);
+}
+
 // ------------------------------------------------------ exact cutout indices
 // (pos - corner) / sampling - (n - 1)/2, float64 with no contraction, then
 // round-half-to-even: the same IEEE operations, in the same order, as

@@ -306,6 +306,14 @@ __global__ void __launch_bounds__(FFT_THREADS, 1) k_group(const GroupArgs a) {
     double *sums = a.sums;
 
     const int64_t pos = a.group[b];
+#if PHB_BOUNDS_CHECK
+    // before any barrier and any access through pos; every CTA of a cluster has the same
+    // position, so a cluster returns whole and none of its CTAs waits on another
+    if (!pos_ok(pos, a.n_pos)) {
+        if (tid == 0) report_bounds(a.err_word, a.status, a.group_index);
+        return;
+    }
+#endif
     const CutoutIndex ci = cutout_index(a.scan, pos, a.cy, a.cx, a.sy, a.sx, N, N);
     {
         CutView<N> c0;
@@ -970,6 +978,7 @@ __global__ void k_gom(const GroupArgs a, float *out) {
     const int b0 = (a.B * blockIdx.y) / nsplit, b1 = (a.B * (blockIdx.y + 1)) / nsplit;
     float acc = 0.f;
     for (int b = b0; b < b1; ++b) {
+        if (!pos_ok(a.group[b], a.n_pos)) continue;   // recorded by the fused kernel of the group
         const CutoutIndex ci = cutout_index(a.scan, a.group[b], a.cy, a.cx, a.sy, a.sx, N, N);
         float2 prod = make_float2(1.f, 0.f);
         for (int s = 0; s < a.S; ++s)
@@ -991,6 +1000,7 @@ struct FinArgs {
     float *grad_tilt;
     float grad_tilt_scale;
     float *errors;   // N = 256: per-position errors, the root of the summed squares in `sums`
+    int64_t n_pos;   // bounds-checking build: group rows outside [0, n_pos) are skipped
 };
 
 __global__ void k_finalize(const FinArgs f) {
@@ -1029,6 +1039,7 @@ __global__ void k_finalize(const FinArgs f) {
     if (pos && f.mode != MODE_GRAD && f.pos_update) {
         double d[2] = {0.0, 0.0};
         for (int b = tid; b < f.B; b += blockDim.x) {
+            if (!pos_ok(f.group[b], f.n_pos)) continue;   // a skipped row's sums are 0 (0 / 0 here)
             const double n = sums[SI.pnorm + b];
             d[0] += sums[SI.pden + 2 * b] / (n * n);
             d[1] += sums[SI.pden + 2 * b + 1] / (n * n);
@@ -1050,6 +1061,7 @@ __global__ void k_finalize(const FinArgs f) {
         for (int b = tid; b < f.B; b += blockDim.x) {
             const double n = sums[SI.pnorm + b];
             const int64_t p = f.group[b];
+            if (!pos_ok(p, f.n_pos)) continue;
             f.pos_update[2 * p] = (float)(sums[SI.pnum + 2 * b] / n / red[0][0]);
             f.pos_update[2 * p + 1] = (float)(sums[SI.pnum + 2 * b + 1] / n / red[1][0]);
         }
@@ -1059,6 +1071,7 @@ __global__ void k_finalize(const FinArgs f) {
         double lsum = 0.0;
         for (int b = tid; b < f.B; b += blockDim.x) {
             const int64_t p = f.group[b];
+            if (!pos_ok(p, f.n_pos)) continue;
             if (pos && f.grad_pos) {
                 f.grad_pos[2 * p] = (float)(gs * sums[SI.pnum + 2 * b]);
                 f.grad_pos[2 * p + 1] = (float)(gs * sums[SI.pnum + 2 * b + 1]);
@@ -1077,7 +1090,8 @@ __global__ void k_finalize(const FinArgs f) {
         }
     }
     if (f.errors && (f.flags & PHB_FLAG_CALC_ERROR) && f.mode != MODE_GRAD)
-        for (int b = tid; b < f.B; b += blockDim.x) f.errors[f.group[b]] = (float)sqrt(sums[SI.err + b]);
+        for (int b = tid; b < f.B; b += blockDim.x)
+            if (pos_ok(f.group[b], f.n_pos)) f.errors[f.group[b]] = (float)sqrt(sums[SI.err + b]);
     __syncthreads();
     for (int64_t i = tid; i < SI.total; i += blockDim.x) sums[i] = 0.0;
 }
@@ -1746,6 +1760,7 @@ static int solver_finish(const phb_engine *e, const phb_step *sp, const int64_t 
     f.S = e->S;
     f.M = e->M;
     f.B = B;
+    f.n_pos = e->n_pos;
     f.B_max = e->B_max;
     f.beta_object = sp->beta_object;
     f.beta_probe = sp->beta_probe;
@@ -1851,6 +1866,7 @@ size_t phb_engine_workspace_bytes(int32_t N, int32_t M, int32_t S, int32_t B_max
     ((n) == 256 ? F<256>(__VA_ARGS__) : (n) == 128 ? F<128>(__VA_ARGS__) : F<64>(__VA_ARGS__))
 
 int phb_engine_init(const phb_engine *e, void *stream) {
+    const NvtxRange range("phb_engine_init");
     int rc = validate(e);
     if (rc) return rc;
     return PHB_DISPATCH_N(e->N, engine_init, e, (cudaStream_t)stream);
@@ -1867,6 +1883,7 @@ int phb_engine_probe_changed(const phb_engine *e, void *stream) {
 
 int phb_presolve_group(const phb_engine *e, const int64_t *group, int32_t B, int32_t solver, int32_t gradient_form,
                        double *rescale_num, double *rescale_den, void *stream) {
+    const NvtxRange range("phb_presolve_group");
     int rc = validate(e);
     if (rc) return rc;
     if (!group || !rescale_num || !rescale_den || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
@@ -1876,6 +1893,7 @@ int phb_presolve_group(const phb_engine *e, const int64_t *group, int32_t B, int
 }
 
 int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, float *intensity, void *stream) {
+    const NvtxRange range("phb_simulate_group");
     int rc = validate(e);
     if (rc) return rc;
     if (!group || !intensity || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
@@ -1884,6 +1902,7 @@ int phb_simulate_group(const phb_engine *e, const int64_t *group, int32_t B, flo
 }
 
 int phb_solver_group_finish(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B, void *stream) {
+    const NvtxRange range("phb_solver_group_finish");
     int rc = validate(e);
     if (rc) return rc;
     if (!st || !group || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
@@ -1905,6 +1924,7 @@ int phb_engine_reduce_layout(int32_t N, int32_t M, int32_t S, int32_t B_max, int
 }
 
 int phb_solver_group(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B, void *stream) {
+    const NvtxRange range("phb_solver_group");
     int rc = validate(e);
     if (rc) return rc;
     if (!st || !group || B < 1 || B > e->B_max) return PHB_ERR_INVALID_ARG;
@@ -1995,6 +2015,7 @@ static void *g_static_scratch_ptr[kMaxDevices] = {nullptr};   // device address 
 extern "C" int phb_solver_group_static(const phb_engine *e, const phb_step *st, const int64_t *group, int32_t B,
                                        void *stream) {
     using namespace phb;
+    const NvtxRange range("phb_solver_group_static");
     if (!e || !st || !group || B < 1) return PHB_ERR_INVALID_ARG;
     // a partial launch leaves its share in the accumulators for a later finish call, but
     // the next call here clears them (and the caller cannot reach this array): refuse it

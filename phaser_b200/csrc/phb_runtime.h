@@ -2,9 +2,20 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include "../../include/phaser_b200.h"
 
 namespace phb {
+
+// NVTX range over one host entry point: a timeline profiler (or ncu --nvtx
+// --nvtx-include "phb_solver_group/") shows the launches it issues under its name.
+// NVTX v3 is header-only; with no tool attached a push / pop is a null check.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Record and map the last CUDA error of a launch to a status code.
 int check_launch();

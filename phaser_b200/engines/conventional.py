@@ -272,10 +272,7 @@ class ConventionalEngine:
         state, eng = self.state, self.eng
         rep = self.status_hosts[i % 2]
         bad_group, n_out, err = int(rep[0]), int(rep[1]), float(rep[2])
-        if bad_group >= _lib.PHB_STATUS_INTERNAL:
-            raise RuntimeError(f"internal error: fused kernel aborted in group {bad_group - _lib.PHB_STATUS_INTERNAL}")
-        if bad_group >= 0:
-            raise ValueError(f"NaN or inf encountered in object or probe, group {bad_group}")
+        _lib.raise_for_status(bad_group)
         if it_pos and n_out > 0:
             raise ValueError(f"{n_out}/{eng.n_pos} probe positions completely outside object")
         error = err if it_err else None

@@ -4,6 +4,9 @@ import ctypes
 import os
 import re
 import subprocess
+import sys
+
+import pytest
 
 from phaser_b200 import _lib
 
@@ -24,6 +27,44 @@ def test_library_loads_and_exports_header_symbols():
         assert hasattr(lib, name), f"{name} declared in the header but not exported"
     # the Python binding covers every declared entry point
     assert set(declared) <= set(_lib.EXPORTED), set(declared) - set(_lib.EXPORTED)
+
+
+def test_header_constants_match_the_binding():
+    text = open(os.path.join(ROOT, 'include', 'phaser_b200.h')).read()
+    found = 0
+    for name, val in re.findall(r'^#define (PHB_[A-Z0-9_]+)\s+(\d+|\(1 << \d+\))', text, flags=re.M):
+        want = 1 << int(val[6:-1]) if val.startswith('(') else int(val)
+        if hasattr(_lib, name):
+            assert getattr(_lib, name) == want, name
+            found += 1
+    assert found >= 18
+
+
+def test_bounds_checking_build_exports_the_same_entry_points():
+    """libphaser_b200_bounds.so (build(bounds_check=True): kernels compiled with
+    -DPHB_BOUNDS_CHECK=1) has every entry point of the header, and the loader picks
+    it when PHASER_B200_BOUNDS_CHECK=1."""
+    from phaser_b200 import build as B
+    path = B.build(bounds_check=True)   # nothing to do when it is newer than the sources
+    lib = ctypes.CDLL(str(path))
+    for name in header_functions():
+        assert hasattr(lib, name), f"{name} missing from the bounds-checking build"
+    code = "import os; from phaser_b200 import _lib; print(os.path.basename(_lib.load()._name))"
+    for flag, want in (('1', 'libphaser_b200_bounds.so'), ('0', 'libphaser_b200.so')):
+        env = dict(os.environ, PHASER_B200_BOUNDS_CHECK=flag)
+        got = subprocess.run([sys.executable, '-c', code], cwd=ROOT, env=env, capture_output=True, text=True,
+                             check=True).stdout.strip()
+        assert got == want
+
+
+def test_step_status_words_map_to_exceptions():
+    _lib.raise_for_status(-1)
+    with pytest.raises(ValueError, match='group 3'):
+        _lib.raise_for_status(3)
+    with pytest.raises(IndexError, match='group 4'):
+        _lib.raise_for_status(_lib.PHB_STATUS_BOUNDS | 4)
+    with pytest.raises(RuntimeError, match='group 5'):
+        _lib.raise_for_status(_lib.PHB_STATUS_INTERNAL | 5)
 
 
 def test_host_only_entry_points():
