@@ -373,6 +373,13 @@ int phb_object_recip_l1(const void *obj, int64_t S, int64_t H, int64_t W, float 
  * which accumulates into them. */
 int phb_conv3x3_fwd(const float *in, const void *w_bf16, const float *bias, float *out, int32_t Nb, int32_t Ci,
                     int32_t Hi, int32_t Wi, int32_t Co, int32_t stride, int32_t relu, void *stream);
+/* Failure-detection probe of the bounded mbarrier waits of the tensor-core kernels
+ * (each gives up after 2^22 attempts; the CTA then writes NaN outputs, drains its
+ * MMAs and frees its tensor memory).  One thread waits on a shared-memory mbarrier
+ * that nothing completes (arrive = 0) or that one arrival completes first
+ * (arrive = 1), for at most `limit` attempts (1 .. 2^22); out[0] (device int32) = 1 if
+ * the wait saw the phase complete, 0 if it gave up. */
+int phb_wait_probe(int32_t arrive, int64_t limit, int32_t *out, void *stream);
 int phb_conv3x3_bwd_data(const float *dout, const void *w_bf16, float *din, int32_t Nb, int32_t Ci, int32_t Hi,
                          int32_t Wi, int32_t Co, int32_t stride, void *stream);
 int phb_conv3x3_bwd_weight(const float *in, const float *dout, float *dw, float *db, int32_t Nb, int32_t Ci,

@@ -150,6 +150,7 @@ _SIGNATURES = {
                                           c_void_p]),
     'phb_object_regularizers': (c_i32, [c_void_p, c_i64, c_i64, c_i64, ctypes.POINTER(PhbObjReg), c_void_p,
                                         c_void_p, c_void_p]),
+    'phb_wait_probe': (c_i32, [c_i32, c_i64, c_void_p, c_void_p]),
     'phb_conv3x3_fwd': (c_i32, [c_void_p, c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32,
                                 c_i32, c_void_p]),
     'phb_conv3x3_bwd_data': (c_i32, [c_void_p, c_void_p, c_void_p, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32,

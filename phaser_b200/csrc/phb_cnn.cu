@@ -277,9 +277,9 @@ __device__ __forceinline__ void umma_commit(uint64_t *mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  :: "r"(smem_u32(mbar)) : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, long long limit = tc::WAIT_LIMIT) {
     const uint32_t addr = smem_u32(mbar);
-    for (long long i = 0; i < tc::WAIT_LIMIT; ++i) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(done) : "r"(addr), "r"(parity) : "memory");
@@ -287,6 +287,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
     }
     return false;
 }
+// Failure-detection probe of the bounded wait above: one thread waits on an mbarrier of
+// arrival count 1 that nothing completes (arrive == 0; the wait gives up after `limit`
+// attempts) or that its own arrival completed first (arrive == 1).  out[0] = 1 if the
+// wait saw phase 0 complete, 0 if it gave up.
+__global__ void k_wait_probe(int arrive, long long limit, int32_t *out) {
+    __shared__ uint64_t mbar;
+    const uint32_t addr = smem_u32(&mbar);
+    if (threadIdx.x == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(addr) : "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (arrive) {
+            uint64_t state;
+            asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(addr) : "memory");
+        }
+        out[0] = mbar_wait(&mbar, 0, limit) ? 1 : 0;
+    }
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -1097,6 +1115,12 @@ int phb_stitch_finish(const void *acc, const float *wgt, void *obj, int64_t n, v
 int phb_project_slices(const void *obj, int64_t S, int64_t HW, void *out, void *stream) {
     if (!obj || !out || S < 1 || HW < 1) return PHB_ERR_INVALID_ARG;
     k_project<<<ew_grid(HW), 256, 0, (cudaStream_t)stream>>>((const float2 *)obj, S, HW, (float2 *)out);
+    return check_launch();
+}
+
+int phb_wait_probe(int32_t arrive, int64_t limit, int32_t *out, void *stream) {
+    if (!out || (arrive != 0 && arrive != 1) || limit < 1 || limit > tc::WAIT_LIMIT) return PHB_ERR_INVALID_ARG;
+    k_wait_probe<<<1, 32, 0, (cudaStream_t)stream>>>(arrive, (long long)limit, out);
     return check_launch();
 }
 

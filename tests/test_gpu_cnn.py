@@ -109,6 +109,27 @@ def test_network_loss_and_gradients_match_oracle():
         assert rel_l2(gb.cpu().numpy(), rb) < 1e-4
 
 
+def test_bounded_wait_gives_up_and_the_context_stays_usable():
+    """The tensor-core kernels' mbarrier waits are bounded: on a barrier that nothing
+    completes the wait gives up after its limit and reports it (no hang, no fault); the
+    same wait sees a completed phase at once; a tensor-core layer runs afterwards."""
+    out = torch.full((1,), -1, dtype=torch.int32, device='cuda')
+    _lib.call('phb_wait_probe', 0, 4096, out.data_ptr(), st())
+    assert int(out.cpu()[0]) == 0
+    _lib.call('phb_wait_probe', 1, 4096, out.data_ptr(), st())
+    assert int(out.cpu()[0]) == 1
+    rng = numpy.random.default_rng(8)
+    x = rng.normal(size=(2, 64, 16, 16)).astype(numpy.float32)
+    w = rng.normal(0, 0.3, (64, 64, 3, 3)).astype(numpy.float32)
+    b = numpy.zeros(64, numpy.float32)
+    xd, bd = torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda()
+    y = torch.empty((2, 64, 16, 16), device='cuda')
+    _lib.call('phb_conv3x3_fwd', xd.data_ptr(), bf16_tensor(w).data_ptr(), bd.data_ptr(), y.data_ptr(), 2, 64, 16, 16,
+              64, 1, 1, st())
+    ref = C.conv3x3(x.astype(numpy.float64), C.bf16(w).astype(numpy.float64), b.astype(numpy.float64), 1, relu=True)
+    assert rel_l2(y.cpu().numpy(), ref) < 1e-5
+
+
 def test_upsample_and_relu_kernels():
     rng = numpy.random.default_rng(6)
     x = torch.from_numpy(rng.normal(size=(2, 3, 5, 7)).astype(numpy.float32)).cuda()

@@ -119,6 +119,12 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     st.flags = _lib.PHB_FLAG_PARTIAL
     grp = (ctypes.c_int64 * 1)(0)
     assert lib.phb_solver_group_static(ctypes.byref(desc), ctypes.byref(st), grp, 1, None) == _lib.PHB_ERR_UNSUPPORTED
+    # the wait probe takes 1 .. 2^22 attempts (the limit of the tensor-core kernels' waits)
+    out = (ctypes.c_int32 * 1)(0)
+    assert lib.phb_wait_probe(0, 16, None, None) == _lib.PHB_ERR_INVALID_ARG
+    assert lib.phb_wait_probe(0, 0, out, None) == _lib.PHB_ERR_INVALID_ARG
+    assert lib.phb_wait_probe(0, (1 << 22) + 1, out, None) == _lib.PHB_ERR_INVALID_ARG
+    assert lib.phb_wait_probe(2, 16, out, None) == _lib.PHB_ERR_INVALID_ARG
 
 
 def test_argument_checks_return_status_without_touching_a_gpu():
