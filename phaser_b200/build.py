@@ -1,7 +1,7 @@
 """Build libphaser_b200.so in-tree with nvcc for sm_100a.
 
     python -m phaser_b200.build                  # or phaser_b200.build.build()
-    python -m phaser_b200.build --bounds-check   # libphaser_b200_bounds.so
+    python -m phaser_b200.build --bounds-check   # also libphaser_b200_bounds.so
 
 The library is a plain C ABI (include/phaser_b200.h); nothing here depends on
 torch.  Objects are rebuilt when a source or header is newer than the .so.
@@ -10,6 +10,9 @@ The bounds-checking build (-DPHB_BOUNDS_CHECK=1) has the same entry points; its
 kernels check every caller-supplied position index against n_pos and report one
 outside [0, n_pos) as PHB_STATUS_BOUNDS in the step's status instead of reading or
 writing out of bounds.  `phaser_b200._lib` loads it when PHASER_B200_BOUNDS_CHECK=1.
+Only the translation units in CHECKED carry checks: the bounds library links their
+checked objects with the default build's objects of the others, and its compiles run
+beside the default build's.
 """
 from __future__ import annotations
 
@@ -26,7 +29,10 @@ LIB = PKG / 'libphaser_b200.so'
 BOUNDS_LIB = PKG / 'libphaser_b200_bounds.so'
 SOURCES = ['phb_runtime.cu', 'phb_ops.cu', 'phb_engine.cu', 'phb_optim.cu', 'phb_constraints.cu', 'phb_cnn.cu',
            'phb_prepare.cu']
+CHECKED = ['phb_engine.cu']   # the sources whose kernels dereference caller-supplied position indices
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+OBJ_DIR = PKG / '_build'
+BOUNDS_OBJ_DIR = PKG / '_build_bounds'
 
 
 def nvcc() -> str:
@@ -45,32 +51,51 @@ def _stale(lib: Path) -> bool:
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False, bounds_check: bool = False) -> Path:
-    lib = BOUNDS_LIB if bounds_check else LIB
-    if not force and not _stale(lib):
-        return lib
-    out_dir = PKG / ('_build_bounds' if bounds_check else '_build')
+def _obj(out_dir: Path, src: str) -> Path:
+    return out_dir / (Path(src).stem + '.o')
+
+
+def _compile(sources, out_dir: Path, verbose: bool, defines=()):
+    """Start one nvcc per translation unit; returns (source, process) pairs."""
     out_dir.mkdir(exist_ok=True)
     flags = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC',
-             '-Xptxas', '-v' if verbose else '-O3', *ARCH, f'-I{ROOT / "include"}']
-    if bounds_check:
-        flags.append('-DPHB_BOUNDS_CHECK=1')
-    objs = [str(out_dir / (Path(src).stem + '.o')) for src in SOURCES]
-    procs = [subprocess.Popen([nvcc(), '-c', str(CSRC / src), '-o', obj, *flags], stdout=subprocess.PIPE,
-                              stderr=subprocess.PIPE, text=True) for src, obj in zip(SOURCES, objs)]
-    for src, proc in zip(SOURCES, procs):   # the translation units compile in parallel
+             '-Xptxas', '-v' if verbose else '-O3', *ARCH, f'-I{ROOT / "include"}', *defines]
+    return [(src, subprocess.Popen([nvcc(), '-c', str(CSRC / src), '-o', str(_obj(out_dir, src)), *flags],
+                                   stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)) for src in sources]
+
+
+def _wait(jobs, verbose: bool) -> None:
+    for src, proc in jobs:
         _, err = proc.communicate()
         if proc.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{err}")
         if verbose:
             sys.stderr.write(err)
+
+
+def _link(lib: Path, objs) -> None:
     tmp = lib.with_suffix('.so.tmp')
-    cmd = [nvcc(), '-shared', '-o', str(tmp), *objs, *ARCH, '-lcudart']
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    res = subprocess.run([nvcc(), '-shared', '-o', str(tmp), *map(str, objs), *ARCH, '-lcudart'],
+                         capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stderr}")
     os.replace(tmp, lib)
-    return lib
+
+
+def build(force: bool = False, verbose: bool = False, bounds_check: bool = False) -> Path:
+    """Build libphaser_b200.so when it is stale (or `force`); with `bounds_check` also
+    libphaser_b200_bounds.so, compiled at the same time.  Returns the library asked for."""
+    main = force or _stale(LIB) or not all(_obj(OBJ_DIR, s).exists() for s in SOURCES)
+    bounds = bounds_check and (main or _stale(BOUNDS_LIB))
+    jobs = _compile(SOURCES, OBJ_DIR, verbose) if main else []
+    checked = _compile(CHECKED, BOUNDS_OBJ_DIR, verbose, ['-DPHB_BOUNDS_CHECK=1']) if bounds else []
+    _wait(jobs, verbose)   # the translation units of both libraries compile in parallel
+    if main:
+        _link(LIB, [_obj(OBJ_DIR, s) for s in SOURCES])
+    if bounds:
+        _wait(checked, verbose)
+        _link(BOUNDS_LIB, [_obj(BOUNDS_OBJ_DIR if s in CHECKED else OBJ_DIR, s) for s in SOURCES])
+    return BOUNDS_LIB if bounds_check else LIB
 
 
 if __name__ == '__main__':
