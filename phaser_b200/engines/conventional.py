@@ -258,6 +258,8 @@ class ConventionalEngine:
         if not sync:
             return None
         torch.cuda.current_stream().synchronize()
+        if self.observer is not None:   # observers get the state as it is after iteration i
+            self._refresh_host_state()
         return self.check(i, it_pos, it_err)
 
     def _group_step(self, group: torch.Tensor, B: int, flags: int, gi: int, events, sched) -> None:
@@ -282,11 +284,18 @@ class ConventionalEngine:
         _call(self.observer, 'update_iteration', state, i, self.niter, error)
         return error
 
-    def finish(self):
+    def _refresh_host_state(self) -> None:
+        """Copy the device's probe, object and positions into the host state: the one the
+        engine returns and the observers are given.  The reference's state is current
+        whenever an observer sees it; SaveObserver writes it out at an iteration
+        (observer.py:224-233), the web worker sends it (web/worker.py:84-85)."""
         probe, obj, scan = self.eng.host_state()
         self.state.probe.data = probe
         self.state.object.data = obj
         self.state.scan = scan.astype(self.scan0.dtype)
+
+    def finish(self):
+        self._refresh_host_state()
         _call(self.observer, 'finish_engine', self.state)
         return self.state
 

@@ -265,6 +265,7 @@ class GradientEngine:
         self.noise = _noise(props)
         self.all_vars, group_specs, iter_specs = process_solvers(props)
         self.niter = int(P.get(props, 'niter', 10))
+        self.send_every_group = bool(P.get(props, 'send_every_group', False))
         grouping = int(P.get(props, 'grouping', None) or 64)
         self.compact = bool(P.get(props, 'compact', False))
         self.flags = {
@@ -396,6 +397,13 @@ class GradientEngine:
                 eng.probe_changed()
             for con in self.group_cons:
                 con.apply_group()
+            if sync and self.observer is not None:
+                # run.py:262: after every group, with `force` = send_every_group; a forced
+                # update gets the device's current arrays (one wait per group, opted into
+                # by the plan), otherwise the state as of the end of the last iteration
+                if self.send_every_group:
+                    self._refresh_host_state()
+                _call(self.observer, 'update_group', state, self.send_every_group)
         torch.mean(losses, dim=0, keepdim=True, out=self.loss_mean)
         for sol in self.iter_solvers:
             d = {}
@@ -423,6 +431,8 @@ class GradientEngine:
         if not sync:
             return None
         torch.cuda.current_stream().synchronize()
+        if self.observer is not None:   # observers get the state as it is after iteration i
+            self._refresh_host_state()
         return self.check(i, it_pos)
 
     def _grad_step(self, group: torch.Tensor, B: int, flags: int, gi: int, events, iter_vars, group_loss,
@@ -454,13 +464,20 @@ class GradientEngine:
         _call(self.observer, 'update_iteration', state, i, self.niter, loss)
         return loss
 
-    def finish(self):
+    def _refresh_host_state(self) -> None:
+        """Copy the device's probe, object, positions and tilt into the host state: the
+        one the engine returns and the observers are given.  The reference's state is
+        current whenever an observer sees it; SaveObserver writes it out at an iteration
+        (observer.py:224-233), the web worker sends it (web/worker.py:79-85)."""
         probe, obj, scan = self.eng.host_state()
         self.state.probe.data = probe
         self.state.object.data = obj
         self.state.scan = scan.astype(self.scan0.dtype)
         if self.eng.tilt is not None and 'tilt' in self.all_vars:
             self.state.tilt = self.eng.tilt.cpu().numpy().reshape(self.scan0.shape).astype(self.scan0.dtype)
+
+    def finish(self):
+        self._refresh_host_state()
         _call(self.observer, 'finish_engine', self.state)
         return self.state
 
