@@ -81,3 +81,40 @@ def test_gradient_engine_reports_every_group(every):
         assert all(numpy.array_equal(o, c.obj) for o in objs[:n_groups])
         assert all(numpy.array_equal(o, rec.iters[0][2]) for o in objs[n_groups:])
     assert numpy.array_equal(rec.iters[-1][2], state.object.data)
+
+
+class Stop(Exception):
+    """Stands for the reference's EarlyTermination(state, continue_next_engine)."""
+
+    def __init__(self, state):
+        super().__init__('stop')
+        self.state = state
+
+
+class StopAt:
+    """Ends the run at iteration k, as PatienceObserver does (observer.py:162-180)."""
+
+    def __init__(self, k):
+        self.k = k
+
+    def update_iteration(self, state, i, n, error=None):
+        if i == self.k:
+            raise Stop(state)
+
+
+def test_early_termination_hands_on_the_state_of_that_iteration():
+    """execute_engine takes the state out of the exception (execute.py:83-89): it must be
+    the state after the iteration that ended the run, not the one the engine started from."""
+    c = make_case(seed=63, N=64, M=2, S=2, scan_shape=(5, 5))
+    props = PL.ConventionalEnginePlan(
+        noise_model={'type': 'amplitude', 'eps': 1e-2},
+        solver={'type': 'lsqml', 'beta_object': 0.9, 'beta_probe': 0.8, 'gamma': 1e-3},
+        niter=5, grouping=10, calc_error_fraction=1.0)
+    with pytest.raises(Stop) as stop:
+        run_conventional(run_args(c, StopAt(2), 'observer-seed'), props)
+    state = stop.value.state
+    assert state.iter.engine_iter == 2
+    assert len(state.progress.detector_errors) == 2
+    assert not numpy.array_equal(state.object.data, c.obj)
+    assert not numpy.array_equal(state.probe.data, c.probe)
+    assert numpy.isfinite(state.object.data).all()
