@@ -164,6 +164,7 @@ class ConventionalEngine:
         h = host_inputs(args, props, patterns_on_device=patterns_on_device)
         state = self.state = h.state
         self.observer = h.observer
+        self.send_every_group = bool(P.get(props, 'send_every_group', False))
         self.noise = h.noise
         self.solver_kind = h.solver_kind
         self.solver = SOLVERS[self.solver_kind](props, h.solver_props)
@@ -241,6 +242,13 @@ class ConventionalEngine:
             self._group_step(gt[gi], B, f, gi, ev, sched)
             for con in self.group_cons:
                 con.apply_group()
+            if sync and self.observer is not None:
+                # solvers.py:119, 377: after every group, with `force` = send_every_group; a
+                # forced update gets the device's current arrays (one wait per group, opted
+                # into by the plan), otherwise the state as of the end of the last iteration
+                if self.send_every_group:
+                    self._refresh_host_state()
+                _call(self.observer, 'update_group', state, self.send_every_group)
         for con in self.iter_cons:
             con.apply_iter()
         if it_pos:

@@ -1,8 +1,9 @@
 """Observers see the state the reference's engines show them (phaser/observer.py):
 after every iteration the probe, object and positions as they are after that
-iteration (SaveObserver writes them out then, observer.py:224-233), and in the
-gradient engine an update_group call after every group (gradient/run.py:262) whose
-state carries the device's arrays when the plan's send_every_group forces the update."""
+iteration (SaveObserver writes them out then, observer.py:224-233), and an
+update_group call after every group (conventional/solvers.py:119, 377;
+gradient/run.py:262) whose state carries the device's arrays when the plan's
+send_every_group forces the update."""
 import numpy
 import pytest
 
@@ -56,7 +57,12 @@ def test_conventional_engine_observers_see_every_iteration():
     assert numpy.array_equal(probe, state.probe.data)
     assert numpy.array_equal(scan, state.scan)
     assert numpy.array_equal(rec.finished, state.object.data)
-    assert rec.groups == []   # the conventional engines report iterations only (run.py:93-122)
+    # one unforced update_group per group, with the state of the last iteration boundary
+    n_groups = len(rec.groups) // 3
+    assert n_groups >= 2 and len(rec.groups) == 3 * n_groups
+    assert all(force is False for (force, _) in rec.groups)
+    assert all(numpy.array_equal(o, c.obj) for (_, o) in rec.groups[:n_groups])
+    assert all(numpy.array_equal(o, rec.iters[0][2]) for (_, o) in rec.groups[n_groups:2 * n_groups])
 
 
 @pytest.mark.parametrize('every', [False, True])
