@@ -200,6 +200,8 @@ class ConventionalEngine:
         logger.info(f"Rescaling initial probe intensity by {rescale:.2e}")
         self.eng.probe.mul_(float(numpy.sqrt(rescale)))
         self.eng.probe_changed()
+        if self.observer is not None:   # the reference's state holds the rescaled probe here
+            self._refresh_host_state()
         _call(self.observer, 'start_engine', self.state)
         return rescale
 

@@ -333,6 +333,8 @@ class GradientEngine:
         self.eng.probe.mul_(float(numpy.sqrt(rescale)))
         self.eng.probe_changed()
         self.probe_int = float(torch.sum(torch.view_as_real(self.eng.probe).double() ** 2))
+        if self.observer is not None:   # the reference's state holds the rescaled probe here
+            self._refresh_host_state()
         _call(self.observer, 'start_engine', self.state)
         return rescale
 

@@ -22,7 +22,10 @@ class Recorder:
     """Keeps copies of what each observer call was shown."""
 
     def __init__(self):
-        self.iters, self.groups, self.finished = [], [], None
+        self.iters, self.groups, self.start, self.finished = [], [], None, None
+
+    def start_engine(self, state):
+        self.start = (state.object.data.copy(), state.probe.data.copy())
 
     def update_iteration(self, state, i, n, error=None):
         self.iters.append((i, n, state.object.data.copy(), state.probe.data.copy(), numpy.array(state.scan)))
@@ -61,7 +64,7 @@ def test_conventional_engine_observers_see_every_iteration():
     n_groups = len(rec.groups) // 3
     assert n_groups >= 2 and len(rec.groups) == 3 * n_groups
     assert all(force is False for (force, _) in rec.groups)
-    assert all(numpy.array_equal(o, c.obj) for (_, o) in rec.groups[:n_groups])
+    assert all(numpy.array_equal(o, rec.start[0]) for (_, o) in rec.groups[:n_groups])
     assert all(numpy.array_equal(o, rec.iters[0][2]) for (_, o) in rec.groups[n_groups:2 * n_groups])
 
 
@@ -84,7 +87,7 @@ def test_gradient_engine_reports_every_group(every):
         assert numpy.array_equal(objs[n_groups - 1], rec.iters[0][2])
         assert numpy.array_equal(objs[-1], state.object.data)
     else:   # otherwise the state as of the last iteration boundary
-        assert all(numpy.array_equal(o, c.obj) for o in objs[:n_groups])
+        assert all(numpy.array_equal(o, rec.start[0]) for o in objs[:n_groups])
         assert all(numpy.array_equal(o, rec.iters[0][2]) for o in objs[n_groups:])
     assert numpy.array_equal(rec.iters[-1][2], state.object.data)
 
