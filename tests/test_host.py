@@ -109,3 +109,42 @@ def test_schedule_hooks_in_plan_form():
     assert P.process_schedule({'type': 'expr', 'expr': '0.5 ** i / niter'})(args) == pytest.approx(0.025)
     with pytest.raises(NotImplementedError):
         P.process_schedule({'type': 'cosine'})
+
+
+def test_defocus_and_propagation_signs_agree():
+    """Known answer of the reference's test_propagator_sign (tests/test_optics.py:43-57),
+    restated A against B instead of against its image fixture: a probe 200 A underfocused,
+    propagated 200 A, is the focused probe; with either sign flipped it is not."""
+    samp = Sampling((256, 256), extent=(25., 25.))
+    ky, kx = samp.recip_grid(dtype=numpy.float32)
+
+    def propagate(probe, dz):
+        k = numpy.fft.fft2(numpy.fft.ifftshift(probe, axes=(-2, -1)), norm='ortho')
+        k = k * optics.fresnel_propagator(ky, kx, 0.0251, dz)
+        return numpy.fft.fftshift(numpy.fft.ifft2(k, norm='ortho'), axes=(-2, -1))
+
+    focused = optics.make_focused_probe(ky, kx, 0.0251, 10., defocus=0.)
+    under = optics.make_focused_probe(ky, kx, 0.0251, 10., defocus=-200.)
+    scale = numpy.abs(focused).max()
+    assert numpy.abs(numpy.abs(propagate(under, 200.)) - numpy.abs(focused)).max() < 1e-5 * scale
+    assert numpy.abs(numpy.abs(propagate(under, -200.)) - numpy.abs(focused)).max() > 1e-2 * scale
+    over = optics.make_focused_probe(ky, kx, 0.0251, 10., defocus=200.)
+    assert numpy.abs(numpy.abs(propagate(over, 200.)) - numpy.abs(focused)).max() > 1e-2 * scale
+
+
+def test_object_slicing_rounding():
+    """Known answers of the reference's test_object_slicing (tests/test_object.py:105-143):
+    an exact pixel position maps to that pixel, a shift under half a sample keeps it, and odd
+    (2n + 1) and even (2n) cutouts n and n - 1/2 samples away start at the same pixel."""
+    samp = ObjectSampling((40, 31), (0.5, 2.0))
+    yy = samp.corner[0] + samp.sampling[0] * numpy.arange(40)
+    xx = samp.corner[1] + samp.sampling[1] * numpy.arange(31)
+    yp, xp = samp.cutout_starts(numpy.array((-1.25, 12.0)), (1, 1))
+    assert yy[yp] == pytest.approx(-1.25) and xx[xp] == pytest.approx(12.0)
+    assert_array_equal(samp.cutout_starts(numpy.array((-1.25 + 0.24, 12.0 - 0.99)), (1, 1)), (yp, xp))
+    n = 2
+    pos = numpy.array((-1.25 - 0.24 + 0.5 * n, 12.0 - 0.99 + 2.0 * n))
+    assert_array_equal(samp.cutout_starts(pos, (2 * n + 1, 2 * n + 1)), (yp, xp))
+    n = 6
+    pos = numpy.array((-1.25 - 0.24 + 0.5 * (n - 0.5), 12.0 - 0.99 + 2.0 * (n - 0.5)))
+    assert_array_equal(samp.cutout_starts(pos, (2 * n, 2 * n)), (yp, xp))
