@@ -161,3 +161,20 @@ def test_engine_run_matches_reference(solver):
     assert rel_l2(probe, g['out_probe']) < 1e-5
     assert_allclose(scan, g['out_scan'], rtol=0, atol=1e-6)
     assert_allclose(errors, g['errors'], rtol=1e-5)
+
+
+def test_cutout_multidim_known_answers():
+    """Known answers of the reference's test_cutout_multidim (tests/test_object.py:265-295):
+    a 2 x 2 grid of (80, 100) cutouts from a 3 x 200^2 ramp object, corner of the default
+    centred grid, top-left values and unit ramps along x, 2 along y."""
+    sampling = numpy.array([1.0, 1.0])
+    corner = -numpy.array([200., 200.]) * sampling / 2. + sampling / 2.
+    zz, yy, xx = numpy.indices((3, 200, 200), dtype=numpy.float32)
+    obj = 1000. * zz + (2. * yy + xx)
+    pos = numpy.array([[[-50., -50.], [-50., 50.]], [[50., -50.], [50., 50.]]])
+    starts = P.cutout_starts(pos.reshape(-1, 2), corner, sampling, (80, 100))
+    cut = P.get_cutouts(obj, starts, (80, 100)).reshape(2, 2, 3, 80, 100)
+    assert_array_equal(cut[..., 0, 0], [[[20., 1020., 2020.], [120., 1120., 2120.]],
+                                        [[220., 1220., 2220.], [320., 1320., 2320.]]])
+    assert (numpy.diff(cut, axis=-1) == 1.).all()
+    assert (numpy.diff(cut, axis=-2) == 2.).all()
